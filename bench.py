@@ -1,0 +1,345 @@
+"""Throughput of the AnisoMPM substep on B200: particle-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 1,048,576-particle slab on a 128^3 grid (seeded synthetic
+scene: vMF fibers about x with kappa=20, log-normal E, sigma_c U(180,220),
+initial damage U(0,0.05), bottom clamped, top edge pulled at 1 m/s,
+dt = 5e-5).  A step is one substep of the whole scene.  The particle state
+(~290 MB with its grids) is larger than L2, so no flush is needed between
+steps.
+
+Arms:
+  ours       -- the sm_100a path.  ``value``: particle state resident in HBM,
+                K substeps timed with CUDA events.  ``e2e``: the same substeps
+                through the public API with the mutable state copied from
+                pinned host memory before and back after every substep.
+  reference  -- the reference algorithm on the host cores: the C oracle
+                (a restatement of anisompm.py's substep) with all threads, on
+                rank 0 only.
+
+Multi-GPU: one independent replica per rank (the substep couples every
+particle through the grid each step, so a single scene does not shard);
+``value`` is the sum over ranks, time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at 1M pts: plain vs batched vs fwd+adjoint on 1 B200, rel err ≤1e-4"
+UNIT = "particle-steps/s"
+# algorithmic bytes per particle-step: mutable state x v F C d lap D_hist read
+# and written (108 + 108 B) plus per-particle material read once (vol0 mass mu
+# lam sigma_c eta zeta l0 residual A0 allow: 73 B)
+BYTES_PER_PARTICLE = 216 + 73
+# per active grid node and substep: momentum accumulate/read/v write/v read
+# (16+16+12+12) + damage (8+8+4+4)
+BYTES_PER_NODE = 80
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (median SM clock, reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ helpers
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def build_sim(torch, device, seed):
+    import peel_mpm_b200 as pm
+    from peel_mpm_b200 import scenes
+    sc = scenes.plain_1m(seed=seed)
+    sim = pm.AnisoMPM(n_grid=sc.n_grid, grid_lim=sc.grid_lim, dt=sc.dt, gravity=tuple(sc.gravity),
+                      grid_damp=sc.grid_damp, f_clamp=sc.f_clamp, damage_every=sc.damage_every, device=device)
+
+    def mk_col(c):
+        raise AssertionError("scene has no colliders")
+
+    scenes.apply_scene(sim, sc, pm.grip_bc, mk_col, torch)
+    return sim, sc
+
+
+def time_kernels(torch, sim, steps, t0):
+    """Per-kernel device time (ms per launch) via events around each C-ABI piece."""
+    from peel_mpm_b200 import _lib
+    grips, _ = sim._descriptors()
+    prm = sim._build_params(grips)
+    P = sim._particles()
+    lib = sim._lib
+    s = torch.cuda.current_stream()
+    sp = s.cuda_stream
+    ws, nb = sim._ws.data_ptr(), sim._ws_bytes
+    names = ["bin", "p2g", "grid", "g2p"]
+    acc = {k: 0.0 for k in names}
+    for i in range(steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        clk = sim._clock(t0 + i * sim.dt, sim._step)
+        ev[0].record(s)
+        _lib.check(lib.pm_set_clock(C.byref(prm), ws, nb, sim.n, C.byref(clk), sp))
+        _lib.check(lib.pm_bin(C.byref(prm), C.byref(P), ws, nb, sp))
+        ev[1].record(s)
+        _lib.check(lib.pm_p2g(C.byref(prm), C.byref(P), ws, nb, sp))
+        ev[2].record(s)
+        _lib.check(lib.pm_grid_update(C.byref(prm), ws, nb, sim.n, sp))
+        ev[3].record(s)
+        _lib.check(lib.pm_g2p(C.byref(prm), C.byref(P), ws, nb, sp))
+        ev[4].record(s)
+        sim._step += 1
+        torch.cuda.synchronize()
+        for k in range(4):
+            acc[names[k]] += ev[k].elapsed_time(ev[k + 1])
+    return {k: v / steps for k, v in acc.items()}
+
+
+def cpu_baseline(sample_steps=3):
+    """The oracle port on the host cores: full 1M scene, a few substeps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from peel_mpm_b200 import scenes
+    sc = scenes.plain_1m()
+    cores = os.cpu_count() or 1
+    sim = orc.OracleSim(sc, np.float32, nthreads=cores, scatter_mode=1)
+    sim.substep(0.0)
+    t = time.perf_counter()
+    for i in range(sample_steps):
+        sim.substep((i + 1) * sc.dt)
+    dt = time.perf_counter() - t
+    return {"value": sc.n * sample_steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{sample_steps} substeps of the 1,048,576-particle scene after 1 warm-up, "
+                      f"C oracle with OpenMP on {cores} threads"}
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from peel_mpm_b200 import scenes
+    sc = scenes.plain_1m()
+    cores = os.cpu_count() or 1
+    sim = orc.OracleSim(sc, np.float32, nthreads=cores, scatter_mode=1)
+    for i in range(args.warmup):
+        sim.substep(i * sc.dt)
+    t = time.perf_counter()
+    for i in range(args.steps):
+        sim.substep((args.warmup + i) * sc.dt)
+    el = time.perf_counter() - t
+    value = sc.n * args.steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "plain AnisoMPM substep, 1,048,576 particles, 128^3 grid (seeded slab)",
+                       "particles": sc.n, "n_grid": sc.n_grid, "dt": sc.dt},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} substeps of the full scene, C oracle, {cores} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sim, sc = build_sim(torch, device, seed=rank)
+    n = sim.n
+    t0 = 0.0
+    for i in range(args.warmup):
+        sim.substep(t0 + i * sim.dt)
+    torch.cuda.synchronize()
+    barrier()
+
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(s)
+        for i in range(args.steps):
+            sim.substep(t0 + (args.warmup + i) * sim.dt)
+        e1.record(s)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    barrier()
+    ms_max = max_over_ranks(ms)
+    value = world * n * args.steps / (ms_max * 1e-3)
+    st = sim.status()
+    n_active = st["n_active_blocks"] * 64
+
+    # e2e: mutable state from pinned host memory in, back out, every substep
+    e2e = None
+    if not args.no_e2e:
+        k = min(args.steps, 20)
+        nplanes = 27
+        host = torch.empty((nplanes, sim._S.shape[1]), dtype=torch.float32, pin_memory=True)
+        host.copy_(sim._S[:nplanes])
+        torch.cuda.synchronize()
+        barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        step0 = sim._step
+        for i in range(k):
+            sim._S[:nplanes].copy_(host, non_blocking=True)
+            sim.substep((step0 + i) * sim.dt)
+            host.copy_(sim._S[:nplanes], non_blocking=True)
+        b.record(s)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(a.elapsed_time(b))
+        nbytes = nplanes * sim._S.shape[1] * 4
+        e2e = {"value": world * n * k / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": k,
+               "what": "AnisoMPM.substep with x,v,F,C,d,lap,D_hist copied from pinned host before and to "
+                       "pinned host after every substep"}
+
+    # per-kernel times for the roofline (separate pass, events around each piece)
+    kt = time_kernels(torch, sim, min(args.steps, 20), (sim._step) * sim.dt)
+    hbm, peak_kind = peaks()
+    p2g_bytes = n * (108 + 73 + 4 + 12) + n_active * 24
+    g2p_bytes = n * (4 + 48 + 100) + n_active * 20
+    dom = max(("p2g", "g2p"), key=lambda k: kt[k])
+    alg = p2g_bytes if dom == "p2g" else g2p_bytes
+    achieved = alg / (kt[dom] * 1e-3) / 1e9
+    step_bytes = n * BYTES_PER_PARTICLE + n_active * BYTES_PER_NODE
+    roof = {"bound": "hbm", "kernel": "k_p2g (fused constitutive + P2G)" if dom == "p2g" else "k_g2p",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+            "traffic": None, "algorithmic_bytes_per_launch": alg,
+            "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
+            "whole_step": {"achieved": step_bytes / (ms / args.steps * 1e-3) / 1e9,
+                           "frac": step_bytes / (ms / args.steps * 1e-3) / 1e9 / hbm,
+                           "bytes_per_step": step_bytes}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+
+    launches_per_step = 1 + 2 + 3 * sim_passes(sim) + 3
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "plain AnisoMPM substep, 1,048,576 particles, 128^3 grid (seeded slab)",
+                           "particles": n, "n_grid": sim.n_grid, "dt": sim.dt, "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2 (particle state ~290 MB)"},
+                "clocks": clocks.summary(), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches_per_step * args.steps, "status": st}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def sim_passes(sim):
+    from peel_mpm_b200 import _lib
+    return _lib.workspace_layout(sim.n, sim.n_grid).sort_passes
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

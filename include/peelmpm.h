@@ -1,0 +1,200 @@
+/*
+ * peelmpm.h -- C ABI of the B200 (sm_100a) AnisoMPM substep.
+ *
+ * Plain pointers and sizes only.  Every entry point:
+ *   - returns PM_OK (0) or a pm_status code; pm_last_error() describes the
+ *     last failure on the calling thread;
+ *   - enqueues work on the given CUDA stream (a cudaStream_t passed as
+ *     void*), never synchronises and never allocates device memory: the
+ *     caller provides every buffer, including the workspace, so every call
+ *     can be captured in a CUDA graph;
+ *   - reads and writes particle state in place.
+ *
+ * Particle state is structure-of-arrays: a field with c components is c
+ * planes of `plane_stride` floats, component k of particle p at
+ * ptr[k * plane_stride + p].  Matrices (F, C, A0, tau_last) are 9 planes in
+ * row-major component order (k = 3*i + j).  This is the layout a
+ * reference-shaped (N,3) / (N,3,3) tensor view with strides (1, stride) /
+ * (1, 3*stride, stride) aliases.
+ *
+ * Reference: anisompm_py/src/anisompm.py (class AnisoMPM).  The comment on
+ * each function names the reference code it replaces.
+ */
+#ifndef PEELMPM_H
+#define PEELMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PM_ABI_VERSION 1
+#define PM_MAX_GRIPS 32
+#define PM_MAX_COLLIDERS 8
+
+typedef enum pm_status {
+    PM_OK = 0,
+    PM_ERR_ARG = 1,          /* bad size, null required pointer, unsupported option */
+    PM_ERR_CUDA = 2,         /* a launch failed (pm_last_error has cudaGetErrorString) */
+    PM_ERR_WORKSPACE = 3,    /* workspace too small or not initialised for (n, n_grid) */
+    PM_ERR_UNSUPPORTED = 4   /* device is not sm_100 */
+} pm_status;
+
+/* Particle grip: particles tagged g get v = vel * min(t / ramp, 1) before P2G
+ * (ramp <= 0: no ramp).  Device form of the particle_bc hook
+ * (anisompm.py:601-602; idiom of test_block.py:109-113, peel_test.py:233-236). */
+typedef struct pm_grip {
+    double vel[3];
+    double ramp;
+} pm_grip;
+
+/* Grid collider (anisompm.py:811-867).  kind 0 = half-space (normal = unit
+ * outward normal of the material side), 1 = sphere (radius).  mode 0 = slip,
+ * 1 = sticky.  Origins are per-substep inputs (pm_clock). */
+typedef struct pm_collider {
+    int32_t kind;
+    int32_t mode;
+    double friction;
+    double radius;
+    double normal[3];
+} pm_collider;
+
+/* Static solver parameters (AnisoMPM.__init__, anisompm.py:304-347). */
+typedef struct pm_params {
+    int32_t n_grid;
+    int32_t damage_every;
+    double grid_lim;
+    double dx;
+    double inv_dx;
+    double dt;
+    double gravity[3];
+    double grid_damp;
+    int32_t use_f_clamp;
+    int32_t record_stress;      /* write tau_last / J_last diagnostics */
+    double f_clamp_lo;
+    double f_clamp_hi;
+    int32_t n_grips;
+    int32_t n_colliders;
+    pm_grip grips[PM_MAX_GRIPS];
+    pm_collider colliders[PM_MAX_COLLIDERS];
+} pm_params;
+
+/* Per-substep inputs: time, step counter (_step) and collider origins at t and
+ * t + 1e-4 (the collider velocity is their forward difference, as in
+ * sphere_collider / halfspace_collider). */
+typedef struct pm_clock {
+    double time;
+    int64_t step;
+    double col_origin[PM_MAX_COLLIDERS][3];
+    double col_origin_next[PM_MAX_COLLIDERS][3];
+} pm_clock;
+
+/* Particle arrays (device pointers), state of add_object/_append
+ * (anisompm.py:374-463). */
+typedef struct pm_particles {
+    int64_t n;
+    int64_t plane_stride;            /* >= n */
+    /* mutable state */
+    float *x, *v, *F, *C;            /* 3, 3, 9, 9 planes */
+    float *d, *lap, *D_hist;
+    /* material, read-only during a substep */
+    const float *vol0, *mass, *mu, *lam, *sigma_c, *eta, *zeta, *l0, *residual;
+    const float *A0;                 /* 9 planes */
+    const uint8_t *allow;            /* damage allowed (bool) */
+    /* optional (NULL = absent) */
+    const float *n_interface;        /* 3 planes; needed for phi_shear */
+    const uint8_t *interface_mask;   /* directional stress particles */
+    const int8_t *grip_tag;          /* grip index or -1 */
+    float *phi, *phi_shear;          /* written on damage steps */
+    float *tau_last;                 /* 9 planes, written when record_stress */
+    float *J_last;
+} pm_particles;
+
+/* Device-side status counters (a copy is read back by pm_read_status). */
+typedef struct pm_status_info {
+    uint32_t nonfinite;              /* particles whose new x or F is not finite (sticky) */
+    uint32_t tile_fallbacks;         /* P2G CTAs that scattered straight to global memory */
+    uint32_t n_active_blocks;        /* active 4^3 grid blocks in the last substep */
+    int32_t any_allow;               /* allow.any() seen by the last substep */
+} pm_status_info;
+
+/* ---------------------------------------------------------------- queries */
+int pm_abi_version(void);
+const char *pm_last_error(void);
+
+/* sizeof the ABI structs, for binding checks: 0 pm_params, 1 pm_particles,
+ * 2 pm_clock, 3 pm_status_info, 4 pm_ws_layout, 5 pm_grip, 6 pm_collider. */
+size_t pm_struct_size(int32_t which);
+
+/* Workspace for n particles on an n_grid^3 grid: grids, sort buffers, block
+ * lists and the control block.  Must be zeroed once by pm_workspace_init. */
+int pm_workspace_size(int64_t n, int32_t n_grid, size_t *bytes);
+int pm_workspace_init(void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, void *stream);
+
+/* Byte offsets of the workspace's views (for inspection and tests). */
+typedef struct pm_ws_layout {
+    size_t ctrl, keys_a, keys_b, vals_a, vals_b, hist, block_mask, block_list;
+    size_t g_mom, g_dmg, g_vel, g_gd, total;
+    int32_t sort_passes;             /* sorted keys/perm end in *_a if even, *_b if odd */
+    int32_t n_tiles;
+} pm_ws_layout;
+int pm_workspace_layout(int64_t n, int32_t n_grid, pm_ws_layout *out);
+
+/* ------------------------------------------------------------ the substep */
+
+/* Whole substep: clock, binning, P2G, grid update, G2P.
+ * Replaces AnisoMPM.substep(time) (anisompm.py:593-803). */
+int pm_substep(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes,
+               const pm_clock *clk, void *stream);
+
+/* Same, reading the clock from row `row` of a device array of pm_clock (so a
+ * captured graph replays with new times).  Replaces one iteration of
+ * AnisoMPM.run_frame (anisompm.py:805-807). */
+int pm_substep_dev_clock(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes,
+                         const pm_clock *dev_clocks, int32_t row, void *stream);
+
+/* The pieces of pm_substep, in order.  Each needs the previous ones of the
+ * same substep to have been enqueued. */
+int pm_set_clock(const pm_params *prm, void *ws, size_t ws_bytes, int64_t n, const pm_clock *clk,
+                 void *stream);
+/* Binning of the substep: the quadratic base cell of every particle
+ * (anisompm.py:544-548), numbered block-major (8^3-cell blocks, x-major;
+ * a bijection of _node_index, anisompm.py:586-590), stable LSD radix sort of
+ * (key, particle id), and the active 4^3 grid blocks.  No reference
+ * counterpart: the reference scatters in particle order. */
+int pm_bin(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, void *stream);
+/* Particle BCs, constitutive update, damage update, degradation, quadratic
+ * P2G and cubic damage scatter (anisompm.py:601-724, 768-776). */
+int pm_p2g(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, void *stream);
+/* Grid velocity update with gravity, damping, mask, colliders, and damage
+ * field normalisation (anisompm.py:727-746, 777-779). */
+int pm_grid_update(const pm_params *prm, void *ws, size_t ws_bytes, int64_t n, void *stream);
+/* Quadratic G2P (APIC), cubic damage Laplacian gather, advection, F update,
+ * domain clamp (anisompm.py:749-760, 781-803). */
+int pm_g2p(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, void *stream);
+
+/* Copies the status counters to host memory (synchronises `stream`). */
+int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, pm_status_info *out,
+                   void *stream);
+
+/* ---------------------------------------------------------------- helpers */
+
+/* Batched 3x3 symmetric eigendecomposition by 5-sweep cyclic Jacobi, A
+ * (n,3,3) row-major contiguous -> ascending evals (n,3), eigenvector columns
+ * evecs (n,3,3).  Replaces sym_eig (anisompm.py:48-95). */
+int pm_sym_eig(const float *A, int64_t n, int32_t sweeps, float *evals, float *evecs, void *stream);
+
+/* Binning only, in the reference's own numbering: keys_out = the sorted
+ * _node_index of every particle's quadratic base cell (anisompm.py:544-548,
+ * 586-590) and perm_out = the stable argsort of those keys, for positions x
+ * (3 planes of stride `plane_stride`).  Uses the workspace's sort buffers;
+ * keys_out / perm_out must not alias the workspace. */
+int pm_bin_sort(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid, double inv_dx,
+                uint32_t *keys_out, int32_t *perm_out, void *ws, size_t ws_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PEELMPM_H */

@@ -1,0 +1,226 @@
+// Particle binning: per-substep cell keys and a stable LSD radix sort of
+// (key, particle id), plus the list of active 4^3 grid blocks.
+//
+// Key = _node_index(base) of the quadratic base cell (anisompm.py:544-548,
+// 586-590), x-major with z fastest.  The permutation equals the stable
+// argsort of the keys, bit for bit.
+#include "pm_kernels.cuh"
+
+namespace pm {
+
+// Keys, identity ids, active-block marks and allow.any().  blocked = false
+// gives the reference's x-major cell index, true the block-major sort key.
+__global__ void __launch_bounds__(256) k_keys(const float *__restrict__ x, long long n, long long ps, int ng,
+                                              float inv_dx, bool blocked, unsigned *__restrict__ keys,
+                                              int *__restrict__ vals, unsigned char *__restrict__ block_mask,
+                                              int nbs, const unsigned char *__restrict__ allow, Ctrl *ctrl) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    bool any = false;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const float xp[3] = {x[p], x[ps + p], x[2 * ps + p]};
+        int qb[3], lo[3], hi[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float X = __fmul_rn(xp[a], inv_dx);
+            qb[a] = sat_base(floorf(__fsub_rn(X, 0.5f)), ng);
+            const int cb = sat_base(floorf(X), ng) - 1;
+            // nodes touched by the quadratic [qb, qb+2] and cubic [cb, cb+3] stencils
+            const int l = min(qb[a], cb), h = max(qb[a] + 2, cb + 3);
+            lo[a] = clampi(l, 0, ng - 1) / kBlockEdge;
+            hi[a] = clampi(h, 0, ng - 1) / kBlockEdge;
+        }
+        keys[p] = blocked ? blocked_key(qb, ng) : cell_key(qb, ng);
+        vals[p] = (int)p;
+        if (block_mask == nullptr) continue;
+        for (int bx = lo[0]; bx <= hi[0]; ++bx)
+            for (int by = lo[1]; by <= hi[1]; ++by)
+                for (int bz = lo[2]; bz <= hi[2]; ++bz)
+                    block_mask[((long long)bx * nbs + by) * nbs + bz] = 1;
+        if (allow != nullptr && allow[p]) any = true;
+    }
+    if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0 && ctrl != nullptr) ctrl->any_allow = 1;
+}
+
+// Compacts the marked blocks into block_list and clears the marks.
+__global__ void __launch_bounds__(256) k_compact_blocks(unsigned char *__restrict__ block_mask, long long nb,
+                                                        int *__restrict__ block_list, Ctrl *ctrl) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long start = (long long)blockIdx.x * blockDim.x;
+    for (long long base = start; base < nb; base += stride) {
+        const long long b = base + threadIdx.x;
+        const bool on = (b < nb) && block_mask[b];
+        const unsigned ball = __ballot_sync(0xffffffffu, on);
+        unsigned slot0 = 0;
+        if ((threadIdx.x & 31) == 0 && ball) slot0 = atomicAdd(&ctrl->n_active, (unsigned)__popc(ball));
+        slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+        if (on) {
+            const unsigned slot = slot0 + __popc(ball & lanemask_lt());
+            if (slot < (unsigned long long)nb) block_list[slot] = (int)b;   // bounded even without a clock reset
+            block_mask[b] = 0;
+        }
+    }
+}
+
+// ------------------------------------------------------------ radix sort
+// Per tile (kSortTile keys) digit histogram -> hist[digit * n_tiles + tile].
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const unsigned *__restrict__ keys, long long n,
+                                                             int shift, unsigned *__restrict__ hist, int n_tiles) {
+    __shared__ unsigned cnt[kRadix];
+    for (int i = threadIdx.x; i < kRadix; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    const long long t0 = (long long)blockIdx.x * kSortTile;
+    const int lane = threadIdx.x & 31;
+#pragma unroll 4
+    for (int it = 0; it < kSortItems; ++it) {
+        const long long i = t0 + (long long)it * kSortThreads + threadIdx.x;
+        const bool ok = i < n;
+        const unsigned dg = ok ? (keys[i] >> shift) & (kRadix - 1) : 0xffffffffu;
+        // warp-aggregate equal digits (sorted-ish input repeats digits a lot)
+        const unsigned peers = __match_any_sync(0xffffffffu, dg);
+        if (ok && lane == __ffs(peers) - 1) atomicAdd(&cnt[dg], (unsigned)__popc(peers));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kRadix; i += blockDim.x) hist[(long long)i * n_tiles + blockIdx.x] = cnt[i];
+}
+
+// Exclusive scan of each digit's row hist[d][0..n_tiles) in place; row totals
+// go to dtot[d].  One CTA per digit.
+__global__ void __launch_bounds__(256) k_radix_rowscan(unsigned *__restrict__ hist, int n_tiles,
+                                                       unsigned *__restrict__ dtot) {
+    __shared__ unsigned wsum[8];
+    __shared__ unsigned carry;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    unsigned *row = hist + (long long)blockIdx.x * n_tiles;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n_tiles; base += 256) {
+        const int i = base + tid;
+        const unsigned v = i < n_tiles ? row[i] : 0u;
+        unsigned incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[wid] = incl;
+        __syncthreads();
+        unsigned wpre = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) wpre += (w < wid) ? wsum[w] : 0u;
+        const unsigned c = carry;
+        if (i < n_tiles) row[i] = c + wpre + incl - v;
+        __syncthreads();
+        if (tid == 255) carry = c + wpre + incl;
+        __syncthreads();
+    }
+    if (tid == 0) dtot[blockIdx.x] = carry;
+}
+
+// Stable scatter of one digit pass.  Warp w of a tile owns keys
+// [w*512, w*512+512) of the tile and ranks them in 16 rounds of 32 in index
+// order; per-warp digit counters are then offset by the earlier warps.
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *__restrict__ kin,
+                                                                const int *__restrict__ vin,
+                                                                unsigned *__restrict__ kout, int *__restrict__ vout,
+                                                                long long n, int shift,
+                                                                const unsigned *__restrict__ offs, int n_tiles,
+                                                                const unsigned *__restrict__ dtot) {
+    constexpr int W = kSortThreads / 32;
+    __shared__ unsigned wcnt[W][kRadix];
+    __shared__ unsigned dbase[kRadix];
+    __shared__ unsigned wtot[W];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < W * kRadix; i += blockDim.x) (&wcnt[0][0])[i] = 0;
+    {   // exclusive scan of the digit totals (kRadix == kSortThreads)
+        const unsigned v = dtot[threadIdx.x];
+        unsigned incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wtot[wid] = incl;
+        __syncthreads();
+        unsigned wpre = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) wpre += (w < wid) ? wtot[w] : 0u;
+        dbase[threadIdx.x] = wpre + incl - v;
+    }
+    __syncthreads();
+    const long long t0 = (long long)blockIdx.x * kSortTile + (long long)wid * (32 * kSortItems);
+    unsigned key[kSortItems];
+    int val[kSortItems];
+    unsigned rank[kSortItems];
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const long long i = t0 + r * 32 + lane;
+        const bool ok = i < n;
+        key[r] = ok ? kin[i] : 0u;
+        val[r] = ok ? vin[i] : 0;
+        const unsigned dg = ok ? (key[r] >> shift) & (kRadix - 1) : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, dg);
+        const int leader = __ffs(peers) - 1;
+        unsigned before = 0;
+        if (ok && lane == leader) {
+            before = wcnt[wid][dg];
+            wcnt[wid][dg] = before + (unsigned)__popc(peers);
+        }
+        before = __shfl_sync(0xffffffffu, before, leader);
+        rank[r] = before + (unsigned)__popc(peers & lt);
+        __syncwarp();
+    }
+    __syncthreads();
+    // exclusive prefix over warps per digit, then add the global tile offset
+    for (int dg = threadIdx.x; dg < kRadix; dg += blockDim.x) {
+        unsigned run = dbase[dg] + offs[(long long)dg * n_tiles + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const unsigned c = wcnt[w][dg];
+            wcnt[w][dg] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const long long i = t0 + r * 32 + lane;
+        if (i < n) {
+            const unsigned dg = (key[r] >> shift) & (kRadix - 1);
+            const unsigned pos = wcnt[wid][dg] + rank[r];
+            kout[pos] = key[r];
+            vout[pos] = val[r];
+        }
+    }
+}
+
+void launch_sort(const WS &w, long long n, cudaStream_t s) {
+    const int tiles = w.n_tiles;
+    unsigned *kin = w.keys_a, *kout = w.keys_b;
+    int *vin = w.vals_a, *vout = w.vals_b;
+    for (int pass = 0; pass < w.passes; ++pass) {
+        const int shift = pass * kRadixBits;
+        k_radix_hist<<<tiles, kSortThreads, 0, s>>>(kin, n, shift, w.hist, tiles);
+        k_radix_rowscan<<<kRadix, 256, 0, s>>>(w.hist, tiles, w.dtot);
+        k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, w.hist, tiles, w.dtot);
+        unsigned *tk = kin; kin = kout; kout = tk;
+        int *tv = vin; vin = vout; vout = tv;
+    }
+}
+
+void launch_keys(const WS &w, const Parts &P, int ng, float inv_dx, cudaStream_t s) {
+    const int blocks = (int)std::min<long long>((P.n + 255) / 256, 148LL * 16);
+    k_keys<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(P.x, P.n, P.ps, ng, inv_dx, true, w.keys_a, w.vals_a,
+                                                  w.block_mask, w.nbs, P.allow, w.ctrl);
+    const int cb = (int)std::min<long long>((w.n_blocks + 255) / 256, 148LL * 8);
+    k_compact_blocks<<<cb > 0 ? cb : 1, 256, 0, s>>>(w.block_mask, w.n_blocks, w.block_list, w.ctrl);
+}
+
+void launch_keys_only(const float *x, long long n, long long ps, int ng, float inv_dx, bool blocked, const WS &w,
+                      cudaStream_t s) {
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_keys<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(x, n, ps, ng, inv_dx, blocked, w.keys_a, w.vals_a, nullptr, 0,
+                                                  nullptr, nullptr);
+}
+
+}  // namespace pm

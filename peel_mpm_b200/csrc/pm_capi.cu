@@ -1,0 +1,253 @@
+// C ABI of the AnisoMPM substep (declarations in include/peelmpm.h).
+// Validates arguments, carves the caller's workspace and enqueues kernels;
+// never allocates and never synchronises (except pm_read_status).
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "pm_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *msg) {
+    g_err = msg;
+    return code;
+}
+
+int cuda_check(const char *where) {
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return PM_OK;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "%s: %s", where, cudaGetErrorString(e));
+    g_err = buf;
+    return PM_ERR_CUDA;
+}
+
+// Device must be compute capability 10.x (the binary carries sm_100a code only).
+int check_device() {
+    static int ok_dev[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail(PM_ERR_CUDA, "no CUDA device");
+    if (ok_dev[dev] == 1) return PM_OK;
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) return fail(PM_ERR_UNSUPPORTED, "peelmpm kernels are built for sm_100a only");
+    ok_dev[dev] = 1;
+    return PM_OK;
+}
+
+int check_params(const pm_params *prm) {
+    if (!prm) return fail(PM_ERR_ARG, "params is NULL");
+    if (prm->n_grid < 4 || prm->n_grid > 1024) return fail(PM_ERR_ARG, "n_grid must be in [4, 1024]");
+    if (prm->damage_every < 1) return fail(PM_ERR_ARG, "damage_every must be >= 1");
+    if (prm->n_grips < 0 || prm->n_grips > PM_MAX_GRIPS) return fail(PM_ERR_ARG, "too many grips");
+    if (prm->n_colliders < 0 || prm->n_colliders > PM_MAX_COLLIDERS) return fail(PM_ERR_ARG, "too many colliders");
+    if (!(prm->dx > 0.0) || !(prm->inv_dx > 0.0)) return fail(PM_ERR_ARG, "dx must be positive");
+    return PM_OK;
+}
+
+int check_particles(const pm_particles *P, bool need_all) {
+    if (!P) return fail(PM_ERR_ARG, "particles is NULL");
+    if (P->n < 0 || P->n >= (1LL << 31)) return fail(PM_ERR_ARG, "particle count must be in [0, 2^31)");
+    if (P->plane_stride < P->n) return fail(PM_ERR_ARG, "plane_stride < n");
+    if (!P->x) return fail(PM_ERR_ARG, "x is NULL");
+    if (need_all) {
+        if (!P->v || !P->F || !P->C || !P->d || !P->lap || !P->D_hist || !P->vol0 || !P->mass || !P->mu ||
+            !P->lam || !P->sigma_c || !P->eta || !P->zeta || !P->l0 || !P->residual || !P->A0 || !P->allow)
+            return fail(PM_ERR_ARG, "a required particle array is NULL");
+        if (P->interface_mask && !P->n_interface) return fail(PM_ERR_ARG, "interface_mask needs n_interface");
+    }
+    return PM_OK;
+}
+
+int get_ws(void *ws, size_t bytes, long long n, int ng, pm::WS *out) {
+    if (!ws) return fail(PM_ERR_WORKSPACE, "workspace is NULL");
+    if (((uintptr_t)ws & 255) != 0) return fail(PM_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    const pm::Layout L = pm::make_layout(n, ng);
+    if (bytes < L.total) return fail(PM_ERR_WORKSPACE, "workspace too small for (n, n_grid)");
+    *out = pm::make_ws(ws, L);
+    return PM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pm_abi_version(void) { return PM_ABI_VERSION; }
+
+const char *pm_last_error(void) { return g_err.c_str(); }
+
+size_t pm_struct_size(int32_t which) {
+    switch (which) {
+        case 0: return sizeof(pm_params);
+        case 1: return sizeof(pm_particles);
+        case 2: return sizeof(pm_clock);
+        case 3: return sizeof(pm_status_info);
+        case 4: return sizeof(pm_ws_layout);
+        case 5: return sizeof(pm_grip);
+        case 6: return sizeof(pm_collider);
+        default: return 0;
+    }
+}
+
+int pm_workspace_size(int64_t n, int32_t n_grid, size_t *bytes) {
+    if (!bytes) return fail(PM_ERR_ARG, "bytes is NULL");
+    if (n < 0 || n_grid < 4 || n_grid > 1024) return fail(PM_ERR_ARG, "bad n or n_grid");
+    *bytes = pm::make_layout(n, n_grid).total;
+    return PM_OK;
+}
+
+int pm_workspace_layout(int64_t n, int32_t n_grid, pm_ws_layout *out) {
+    if (!out) return fail(PM_ERR_ARG, "out is NULL");
+    if (n < 0 || n_grid < 4 || n_grid > 1024) return fail(PM_ERR_ARG, "bad n or n_grid");
+    const pm::Layout L = pm::make_layout(n, n_grid);
+    out->ctrl = L.ctrl; out->keys_a = L.keys_a; out->keys_b = L.keys_b; out->vals_a = L.vals_a;
+    out->vals_b = L.vals_b; out->hist = L.hist; out->block_mask = L.block_mask; out->block_list = L.block_list;
+    out->g_mom = L.g_mom; out->g_dmg = L.g_dmg; out->g_vel = L.g_vel; out->g_gd = L.g_gd; out->total = L.total;
+    out->sort_passes = L.passes;
+    out->n_tiles = L.n_tiles;
+    return PM_OK;
+}
+
+int pm_workspace_init(void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, void *stream) {
+    int rc = check_device();
+    if (rc) return rc;
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, n, n_grid, &w))) return rc;
+    const pm::Layout L = pm::make_layout(n, n_grid);
+    if (cudaMemsetAsync(ws, 0, L.total, (cudaStream_t)stream) != cudaSuccess) return cuda_check("pm_workspace_init");
+    return cuda_check("pm_workspace_init");
+}
+
+int pm_set_clock(const pm_params *prm, void *ws, size_t ws_bytes, int64_t n, const pm_clock *clk, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_params(prm))) return rc;
+    if (!clk) return fail(PM_ERR_ARG, "clock is NULL");
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, n, prm->n_grid, &w))) return rc;
+    pm::launch_set_clock(*prm, w, *clk, (cudaStream_t)stream);
+    return cuda_check("pm_set_clock");
+}
+
+int pm_bin(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, false))) return rc;
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
+    const pm::Parts parts = pm::make_parts(P);
+    cudaStream_t s = (cudaStream_t)stream;
+    pm::launch_keys(w, parts, prm->n_grid, (float)prm->inv_dx, s);
+    pm::launch_sort(w, P->n, s);
+    return cuda_check("pm_bin");
+}
+
+int pm_p2g(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
+    pm::launch_p2g(*prm, pm::make_parts(P), w, (cudaStream_t)stream);
+    return cuda_check("pm_p2g");
+}
+
+int pm_grid_update(const pm_params *prm, void *ws, size_t ws_bytes, int64_t n, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_params(prm))) return rc;
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, n, prm->n_grid, &w))) return rc;
+    pm::launch_grid(*prm, w, (cudaStream_t)stream);
+    return cuda_check("pm_grid_update");
+}
+
+int pm_g2p(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
+    pm::launch_g2p(*prm, pm::make_parts(P), w, (cudaStream_t)stream);
+    return cuda_check("pm_g2p");
+}
+
+static int substep_common(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes,
+                          const pm_clock *clk, const pm_clock *dev_clocks, int32_t row, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
+    const pm::Parts parts = pm::make_parts(P);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (clk)
+        pm::launch_set_clock(*prm, w, *clk, s);
+    else
+        pm::launch_set_clock_dev(*prm, w, dev_clocks, row, s);
+    if (P->n > 0) {
+        pm::launch_keys(w, parts, prm->n_grid, (float)prm->inv_dx, s);
+        pm::launch_sort(w, P->n, s);
+        pm::launch_p2g(*prm, parts, w, s);
+        pm::launch_grid(*prm, w, s);
+        pm::launch_g2p(*prm, parts, w, s);
+    }
+    return cuda_check("pm_substep");
+}
+
+int pm_substep(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, const pm_clock *clk,
+               void *stream) {
+    if (!clk) return fail(PM_ERR_ARG, "clock is NULL");
+    return substep_common(prm, P, ws, ws_bytes, clk, nullptr, 0, stream);
+}
+
+int pm_substep_dev_clock(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes,
+                         const pm_clock *dev_clocks, int32_t row, void *stream) {
+    if (!dev_clocks || row < 0) return fail(PM_ERR_ARG, "bad device clock table");
+    return substep_common(prm, P, ws, ws_bytes, nullptr, dev_clocks, row, stream);
+}
+
+int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, pm_status_info *out, void *stream) {
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (!out) return fail(PM_ERR_ARG, "out is NULL");
+    pm::WS w;
+    if ((rc = get_ws(const_cast<void *>(ws), ws_bytes, n, n_grid, &w))) return rc;
+    pm::Ctrl c;
+    if (cudaMemcpyAsync(&c, w.ctrl, sizeof c, cudaMemcpyDeviceToHost, (cudaStream_t)stream) != cudaSuccess ||
+        cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+        return cuda_check("pm_read_status");
+    out->nonfinite = c.nonfinite;
+    out->tile_fallbacks = c.tile_fallbacks;
+    out->n_active_blocks = c.n_active;
+    out->any_allow = c.any_allow;
+    return PM_OK;
+}
+
+int pm_sym_eig(const float *A, int64_t n, int32_t sweeps, float *evals, float *evecs, void *stream) {
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (n < 0) return fail(PM_ERR_ARG, "n < 0");
+    if (n > 0 && (!A || !evals || !evecs)) return fail(PM_ERR_ARG, "NULL array");
+    if (sweeps < 1) return fail(PM_ERR_ARG, "sweeps must be >= 1");
+    pm::launch_sym_eig(A, n, sweeps, evals, evecs, (cudaStream_t)stream);
+    return cuda_check("pm_sym_eig");
+}
+
+int pm_bin_sort(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid, double inv_dx, uint32_t *keys_out,
+                int32_t *perm_out, void *ws, size_t ws_bytes, void *stream) {
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (n < 0 || plane_stride < n || n_grid < 4 || n_grid > 1024 || !(inv_dx > 0.0))
+        return fail(PM_ERR_ARG, "bad size argument");
+    if (n > 0 && (!x || !keys_out || !perm_out)) return fail(PM_ERR_ARG, "NULL array");
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, n, n_grid, &w))) return rc;
+    if (n == 0) return PM_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    pm::launch_keys_only(x, n, plane_stride, n_grid, (float)inv_dx, false, w, s);
+    pm::launch_sort(w, n, s);
+    if (cudaMemcpyAsync(keys_out, w.sorted_keys, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(perm_out, w.perm, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return cuda_check("pm_bin_sort");
+    return cuda_check("pm_bin_sort");
+}
+
+}  // extern "C"

@@ -1,0 +1,330 @@
+// Shared device code of the AnisoMPM substep: control block, workspace
+// layout, 3x3 algebra, the cyclic Jacobi eigensolver and the B-spline
+// weights.  Reference: anisompm_py/src/anisompm.py.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "peelmpm.h"
+
+namespace pm {
+
+constexpr int kBlockEdge = 4;          // grid block = 4^3 nodes (active-block granularity)
+constexpr int kSortBlock = 8;          // sort block = 8^3 cells (P2G work unit)
+constexpr int kSortBlockBits = 9;      // log2(8^3)
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;   // keys per radix tile
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+
+// Device control block: per-substep inputs and status counters.
+struct Ctrl {
+    double time;
+    long long step;
+    int any_allow;
+    unsigned n_active;
+    unsigned nonfinite;
+    unsigned tile_fallbacks;
+    float col_origin[PM_MAX_COLLIDERS][3];
+    float col_vel[PM_MAX_COLLIDERS][3];
+};
+
+__host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+__host__ __device__ inline int sort_bits(int n_grid) {
+    unsigned long long cells = (unsigned long long)n_grid * n_grid * n_grid;
+    int b = 1;
+    while ((1ull << b) < cells) ++b;
+    return b;
+}
+
+__host__ __device__ inline int sort_blocks_per_axis(int ng) { return (ng + kSortBlock - 1) / kSortBlock; }
+__host__ __device__ inline int blocked_key_bits(int ng) {
+    const unsigned long long nb = (unsigned long long)sort_blocks_per_axis(ng);
+    const unsigned long long blocks = nb * nb * nb;
+    int b = 0;
+    while ((1ull << b) < blocks) ++b;
+    return b + kSortBlockBits;
+}
+
+struct Layout {
+    size_t ctrl, keys_a, keys_b, vals_a, vals_b, hist, block_mask, block_list;
+    size_t g_mom, g_dmg, g_vel, g_gd, total;
+    int passes, n_tiles, nbs;
+    long long n_blocks, n_nodes;
+};
+
+__host__ __device__ inline Layout make_layout(long long n, int ng) {
+    Layout L;
+    const size_t A = 256;
+    L.n_tiles = (int)((n + kSortTile - 1) / kSortTile);
+    if (L.n_tiles < 1) L.n_tiles = 1;
+    {
+        const int kb = sort_bits(ng) > blocked_key_bits(ng) ? sort_bits(ng) : blocked_key_bits(ng);
+        L.passes = (kb + kRadixBits - 1) / kRadixBits;
+    }
+    L.nbs = (ng + kBlockEdge - 1) / kBlockEdge;
+    L.n_blocks = (long long)L.nbs * L.nbs * L.nbs;
+    L.n_nodes = (long long)ng * ng * ng;
+    size_t nn = (size_t)(n > 0 ? n : 1);
+    size_t o = 0;
+    L.ctrl = o;       o = align_up(o + sizeof(Ctrl), A);
+    L.keys_a = o;     o = align_up(o + 4 * nn, A);
+    L.keys_b = o;     o = align_up(o + 4 * nn, A);
+    L.vals_a = o;     o = align_up(o + 4 * nn, A);
+    L.vals_b = o;     o = align_up(o + 4 * nn, A);
+    L.hist = o;       o = align_up(o + 4 * ((size_t)kRadix * L.n_tiles + kRadix), A);
+    L.block_mask = o; o = align_up(o + (size_t)L.n_blocks, A);
+    L.block_list = o; o = align_up(o + 4 * (size_t)L.n_blocks, A);
+    L.g_mom = o;      o = align_up(o + 16 * (size_t)L.n_nodes, A);
+    L.g_dmg = o;      o = align_up(o + 8 * (size_t)L.n_nodes, A);
+    L.g_vel = o;      o = align_up(o + 16 * (size_t)L.n_nodes, A);
+    L.g_gd = o;       o = align_up(o + 4 * (size_t)L.n_nodes, A);
+    L.total = o;
+    return L;
+}
+
+// Raw views of the workspace for kernels.
+struct WS {
+    Ctrl *ctrl;
+    unsigned *keys_a, *keys_b;
+    int *vals_a, *vals_b;
+    unsigned *hist;          // [kRadix][n_tiles] tile counts
+    unsigned *dtot;          // [kRadix] digit totals of the current pass
+    unsigned char *block_mask;
+    int *block_list;
+    float4 *g_mom;      // {mv.x, mv.y, mv.z, m}, zero between substeps
+    float2 *g_dmg;      // {sum w d, sum w}, zero between substeps
+    float4 *g_vel;      // {v.x, v.y, v.z, unused}
+    float *g_gd;        // normalised damage field
+    const unsigned *sorted_keys;
+    const int *perm;
+    int passes, n_tiles, nbs;
+    long long n_blocks;
+};
+
+inline WS make_ws(void *base, const Layout &L) {
+    char *b = (char *)base;
+    WS w;
+    w.ctrl = (Ctrl *)(b + L.ctrl);
+    w.keys_a = (unsigned *)(b + L.keys_a);
+    w.keys_b = (unsigned *)(b + L.keys_b);
+    w.vals_a = (int *)(b + L.vals_a);
+    w.vals_b = (int *)(b + L.vals_b);
+    w.hist = (unsigned *)(b + L.hist);
+    w.dtot = w.hist + (size_t)kRadix * L.n_tiles;
+    w.block_mask = (unsigned char *)(b + L.block_mask);
+    w.block_list = (int *)(b + L.block_list);
+    w.g_mom = (float4 *)(b + L.g_mom);
+    w.g_dmg = (float2 *)(b + L.g_dmg);
+    w.g_vel = (float4 *)(b + L.g_vel);
+    w.g_gd = (float *)(b + L.g_gd);
+    w.passes = L.passes;
+    w.n_tiles = L.n_tiles;
+    w.nbs = L.nbs;
+    w.n_blocks = L.n_blocks;
+    // pass 0 reads keys_a and writes keys_b; the result of an odd pass count is in *_b
+    w.sorted_keys = (L.passes & 1) ? w.keys_b : w.keys_a;
+    w.perm = (L.passes & 1) ? w.vals_b : w.vals_a;
+    return w;
+}
+
+// Particle pointers as kernels see them (plane stride folded in).
+struct Parts {
+    long long n, ps;
+    float *x, *v, *F, *C, *d, *lap, *D_hist;
+    const float *vol0, *mass, *mu, *lam, *sigma_c, *eta, *zeta, *l0, *residual, *A0;
+    const unsigned char *allow;
+    const float *n_interface;
+    const unsigned char *interface_mask;
+    const signed char *grip_tag;
+    float *phi, *phi_shear, *tau_last, *J_last;
+};
+
+inline Parts make_parts(const pm_particles *P) {
+    Parts q;
+    q.n = P->n; q.ps = P->plane_stride;
+    q.x = P->x; q.v = P->v; q.F = P->F; q.C = P->C; q.d = P->d; q.lap = P->lap; q.D_hist = P->D_hist;
+    q.vol0 = P->vol0; q.mass = P->mass; q.mu = P->mu; q.lam = P->lam; q.sigma_c = P->sigma_c;
+    q.eta = P->eta; q.zeta = P->zeta; q.l0 = P->l0; q.residual = P->residual; q.A0 = P->A0;
+    q.allow = P->allow; q.n_interface = P->n_interface; q.interface_mask = P->interface_mask;
+    q.grip_tag = (const signed char *)P->grip_tag; q.phi = P->phi; q.phi_shear = P->phi_shear;
+    q.tau_last = P->tau_last; q.J_last = P->J_last;
+    return q;
+}
+
+// ------------------------------------------------------------------ cells
+// floor(v).to(long) then clamp, as the reference forms base cells: NaN or a
+// value outside int64 becomes INT64_MIN in torch and clamps to node 0; values
+// far outside the grid clamp to the edge, so the base is saturated to
+// [-8, ng+8] (every stencil node then clamps identically).
+__device__ __forceinline__ int sat_base(float f, int ng) {
+    if (!(f >= -9.2233720368547758e18f && f < 9.2233720368547758e18f)) return -8;
+    return (int)fminf(fmaxf(f, -8.0f), (float)(ng + 8));
+}
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Quadratic B-spline (anisompm.py:544-557): base = floor(X - 0.5), fx = X - base,
+// w0 = 0.5(1.5-fx)^2, w1 = 0.75-(fx-1)^2, w2 = 0.5(fx-0.5)^2.  X = x * fp32(inv_dx)
+// and X - 0.5 are rounded exactly as the reference's two tensor ops.
+struct Quad {
+    int b[3];
+    float fx[3];
+    float w[3][3];   // [node][axis]
+};
+__device__ __forceinline__ void quad_weights(const float x[3], float inv_dx, int ng, Quad &q) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float X = __fmul_rn(x[a], inv_dx);
+        const float fb = floorf(__fsub_rn(X, 0.5f));
+        q.b[a] = sat_base(fb, ng);
+        const float f = __fsub_rn(X, fb);
+        q.fx[a] = f;
+        const float t0 = 1.5f - f, t1 = f - 1.0f, t2 = f - 0.5f;
+        q.w[0][a] = 0.5f * (t0 * t0);
+        q.w[1][a] = 0.75f - t1 * t1;
+        q.w[2][a] = 0.5f * (t2 * t2);
+    }
+}
+
+// Cubic B-spline with second derivatives (anisompm.py:559-584): base =
+// floor(X) - 1, f = X - floor(X).
+struct Cubic {
+    int b[3];
+    float w[4][3];
+    float w2[4][3];
+};
+__device__ __forceinline__ void cubic_weights(const float x[3], float inv_dx, int ng, Cubic &c) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float X = __fmul_rn(x[a], inv_dx);
+        const float fb = floorf(X);
+        const int bb = sat_base(fb, ng);
+        c.b[a] = bb - 1;
+        const float f = __fsub_rn(X, fb);
+        const float one = 1.0f - f;
+        c.w[0][a] = (1.0f / 6.0f) * (one * one * one);
+        c.w[1][a] = (2.0f / 3.0f - f * f) + 0.5f * (f * f * f);
+        c.w[2][a] = (2.0f / 3.0f - one * one) + 0.5f * (one * one * one);
+        c.w[3][a] = (1.0f / 6.0f) * (f * f * f);
+        c.w2[0][a] = one;
+        c.w2[1][a] = 3.0f * f - 2.0f;
+        c.w2[2][a] = 1.0f - 3.0f * f;
+        c.w2[3][a] = f;
+    }
+}
+
+// _node_index of the base cell (anisompm.py:586-590): x-major, z fastest.
+__device__ __forceinline__ unsigned cell_key(const int b[3], int ng) {
+    const int x = clampi(b[0], 0, ng - 1), y = clampi(b[1], 0, ng - 1), z = clampi(b[2], 0, ng - 1);
+    return ((unsigned)x * (unsigned)ng + (unsigned)y) * (unsigned)ng + (unsigned)z;
+}
+
+// Sort key of the substep: the same base cell, numbered block-major (8^3-cell
+// blocks in x-major order, cells x-major inside a block) so that a run of the
+// sorted order is a compact brick.  A bijection of cell_key.
+__device__ __forceinline__ unsigned blocked_key(const int b[3], int ng) {
+    const int x = clampi(b[0], 0, ng - 1), y = clampi(b[1], 0, ng - 1), z = clampi(b[2], 0, ng - 1);
+    const unsigned nb = (unsigned)sort_blocks_per_axis(ng);
+    const unsigned blk = ((unsigned)(x >> 3) * nb + (unsigned)(y >> 3)) * nb + (unsigned)(z >> 3);
+    return (blk << kSortBlockBits) | ((unsigned)(x & 7) << 6) | ((unsigned)(y & 7) << 3) | (unsigned)(z & 7);
+}
+
+// ------------------------------------------------------------ 3x3 algebra
+// Row-major 3x3; products accumulate k = 0, 1, 2.
+__device__ __forceinline__ void mm3(const float *A, const float *B, float *Cm) {
+    float T[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            T[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Cm[k] = T[k];
+}
+__device__ __forceinline__ void mmt3(const float *A, const float *B, float *Cm) {   // A B^T
+    float T[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            T[3 * i + j] = A[3 * i] * B[3 * j] + A[3 * i + 1] * B[3 * j + 1] + A[3 * i + 2] * B[3 * j + 2];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Cm[k] = T[k];
+}
+
+__device__ __forceinline__ float nan_to_num(float a) {
+    if (a != a) return 0.0f;
+    if (a > 3.402823466e38f) return 3.402823466e38f;
+    if (a < -3.402823466e38f) return -3.402823466e38f;
+    return a;
+}
+
+// One Jacobi rotation on pair (p,q) with the third index r, for a symmetric
+// matrix stored as app/aqq/apq/apr/aqr (anisompm.py:72-91).
+#define PM_JACOBI_ROT(APP, AQQ, APQ, APR, AQR, P, Q)                                  \
+    {                                                                                 \
+        const float app = APP, aqq = AQQ, apq = APQ, apr = APR, aqr = AQR;            \
+        float t = 0.0f;                                                               \
+        if (fabsf(apq) > 1e-30f) {                                                    \
+            const float z = (aqq - app) / (2.0f * apq);                               \
+            const float sgn = (z >= 0.0f) ? 1.0f : -1.0f;                             \
+            t = sgn / (fabsf(z) + sqrtf(1.0f + z * z));                               \
+        }                                                                             \
+        const float c = 1.0f / sqrtf(1.0f + t * t);                                   \
+        const float s = c * t;                                                        \
+        APP = c * c * app - 2.0f * s * c * apq + s * s * aqq;                         \
+        AQQ = s * s * app + 2.0f * s * c * apq + c * c * aqq;                         \
+        APQ = 0.0f;                                                                   \
+        APR = c * apr - s * aqr;                                                      \
+        AQR = s * apr + c * aqr;                                                      \
+        _Pragma("unroll") for (int i_ = 0; i_ < 3; ++i_) {                            \
+            const float vp = V[3 * i_ + P], vq = V[3 * i_ + Q];                       \
+            V[3 * i_ + P] = c * vp - s * vq;                                          \
+            V[3 * i_ + Q] = s * vp + c * vq;                                          \
+        }                                                                             \
+    }
+
+// sym_eig (anisompm.py:48-95): symmetrise + nan_to_num, 5 (or `sweeps`) cyclic
+// sweeps over pairs (0,1),(0,2),(1,2), eigenvalues ascending (stable order),
+// eigenvector columns in V (row-major).
+template <int SWEEPS>
+__device__ __forceinline__ void sym_eig3(const float *Ain, float ev[3], float V[9]) {
+    float a00 = nan_to_num(0.5f * (Ain[0] + Ain[0]));
+    float a11 = nan_to_num(0.5f * (Ain[4] + Ain[4]));
+    float a22 = nan_to_num(0.5f * (Ain[8] + Ain[8]));
+    float a01 = nan_to_num(0.5f * (Ain[1] + Ain[3]));
+    float a02 = nan_to_num(0.5f * (Ain[2] + Ain[6]));
+    float a12 = nan_to_num(0.5f * (Ain[5] + Ain[7]));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) V[k] = (k % 4 == 0) ? 1.0f : 0.0f;
+#pragma unroll
+    for (int sw = 0; sw < SWEEPS; ++sw) {
+        PM_JACOBI_ROT(a00, a11, a01, a02, a12, 0, 1)
+        PM_JACOBI_ROT(a00, a22, a02, a01, a12, 0, 2)
+        PM_JACOBI_ROT(a11, a22, a12, a01, a02, 1, 2)
+    }
+    ev[0] = a00; ev[1] = a11; ev[2] = a22;
+    // stable ascending sort of three, eigenvector columns follow
+#define PM_SWAPCOL(I, J)                                                               \
+    {                                                                                  \
+        float te = ev[I]; ev[I] = ev[J]; ev[J] = te;                                   \
+        _Pragma("unroll") for (int r_ = 0; r_ < 3; ++r_) {                             \
+            float tv = V[3 * r_ + I]; V[3 * r_ + I] = V[3 * r_ + J]; V[3 * r_ + J] = tv; \
+        }                                                                              \
+    }
+    if (ev[1] < ev[0]) PM_SWAPCOL(0, 1)
+    if (ev[2] < ev[1]) PM_SWAPCOL(1, 2)
+    if (ev[1] < ev[0]) PM_SWAPCOL(0, 1)
+#undef PM_SWAPCOL
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+}  // namespace pm

@@ -1,0 +1,288 @@
+// Grid update (active 4^3 blocks only), G2P with the damage Laplacian and
+// advection, the per-substep clock, and the standalone batched eigensolver.
+#include "pm_kernels.cuh"
+
+namespace pm {
+
+// ------------------------------------------------------------------ clock
+__global__ void k_set_clock(Ctrl *c, const pm_clock clk, int ncol) {
+    const int t = threadIdx.x;
+    if (t == 0) {
+        c->time = clk.time;
+        c->step = clk.step;
+        c->any_allow = 0;
+        c->n_active = 0;
+    }
+    if (t < ncol) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float o = (float)clk.col_origin[t][a], o2 = (float)clk.col_origin_next[t][a];
+            c->col_origin[t][a] = o;
+            c->col_vel[t][a] = __fdiv_rn(__fsub_rn(o2, o), 1e-4f);   // (o2 - o) / dt_fd (anisompm.py:838, 862)
+        }
+    }
+}
+
+__global__ void k_set_clock_dev(Ctrl *c, const pm_clock *dev, int row, int ncol) {
+    const pm_clock *clk = dev + row;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        c->time = clk->time;
+        c->step = clk->step;
+        c->any_allow = 0;
+        c->n_active = 0;
+    }
+    if (t < ncol) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float o = (float)clk->col_origin[t][a], o2 = (float)clk->col_origin_next[t][a];
+            c->col_origin[t][a] = o;
+            c->col_vel[t][a] = __fdiv_rn(__fsub_rn(o2, o), 1e-4f);
+        }
+    }
+}
+
+void launch_set_clock(const pm_params &prm, const WS &w, const pm_clock &clk, cudaStream_t s) {
+    k_set_clock<<<1, 32, 0, s>>>(w.ctrl, clk, prm.n_colliders);
+}
+void launch_set_clock_dev(const pm_params &prm, const WS &w, const pm_clock *dev, int row, cudaStream_t s) {
+    k_set_clock_dev<<<1, 32, 0, s>>>(w.ctrl, dev, row, prm.n_colliders);
+}
+
+// ------------------------------------------------------------ grid update
+// _resolve (anisompm.py:811-825) for one node
+__device__ __forceinline__ void resolve(float v[3], const float vc[3], const float nn[3], bool sticky, float fr) {
+    if (sticky) {
+        v[0] = vc[0]; v[1] = vc[1]; v[2] = vc[2];
+        return;
+    }
+    const float r0 = v[0] - vc[0], r1 = v[1] - vc[1], r2 = v[2] - vc[2];
+    const float vn = r0 * nn[0] + r1 * nn[1] + r2 * nn[2];
+    const float inward = vn < 0.0f ? vn : 0.0f;
+    float t0 = r0 - vn * nn[0], t1 = r1 - vn * nn[1], t2 = r2 - vn * nn[2];
+    if (fr > 0.0f) {
+        const float vtm = sqrtf(t0 * t0 + t1 * t1 + t2 * t2);
+        float sc = 1.0f + fr * inward / (vtm + 1e-9f);
+        sc = sc < 0.0f ? 0.0f : sc;
+        t0 *= sc; t1 *= sc; t2 *= sc;
+    }
+    const float keep = vn - inward;
+    v[0] = vc[0] + t0 + keep * nn[0];
+    v[1] = vc[1] + t1 + keep * nn[1];
+    v[2] = vc[2] + t2 + keep * nn[2];
+}
+
+// One thread per node of the active blocks.  Reads and clears the P2G
+// accumulators, writes grid velocity and the normalised damage field
+// (anisompm.py:727-746, 777-779).
+__global__ void __launch_bounds__(256) k_grid(const pm_params prm, const WS w) {
+    const Ctrl *ctrl = w.ctrl;
+    const long long nact = min((long long)ctrl->n_active, w.n_blocks);
+    const long long items = nact * 64;
+    const int ng = prm.n_grid, nbs = w.nbs;
+    const float dt = (float)prm.dt;
+    const float gdt[3] = {dt * (float)prm.gravity[0], dt * (float)prm.gravity[1], dt * (float)prm.gravity[2]};
+    const float damp = (float)prm.grid_damp;
+    const bool do_damp = prm.grid_damp != 1.0;
+    const float dx = (float)prm.dx;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int b = w.block_list[it >> 6];
+        const int l = (int)(it & 63);
+        const int bx = b / (nbs * nbs), by = (b / nbs) % nbs, bz = b % nbs;
+        const int ix = bx * kBlockEdge + (l >> 4), iy = by * kBlockEdge + ((l >> 2) & 3), iz = bz * kBlockEdge + (l & 3);
+        if (ix >= ng || iy >= ng || iz >= ng) continue;
+        const long long node = ((long long)ix * ng + iy) * ng + iz;
+        const float4 mom = w.g_mom[node];
+        const float2 dmg = w.g_dmg[node];
+        w.g_mom[node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w.g_dmg[node] = make_float2(0.0f, 0.0f);
+        const bool active = mom.w > 1e-12f;
+        const float inv_m = active ? 1.0f / mom.w : 0.0f;
+        float v[3] = {mom.x * inv_m + gdt[0], mom.y * inv_m + gdt[1], mom.z * inv_m + gdt[2]};
+        if (do_damp) {
+            v[0] *= damp; v[1] *= damp; v[2] *= damp;
+        }
+        if (!active) v[0] = v[1] = v[2] = 0.0f;
+        if (active && prm.n_colliders > 0) {
+            const float pos[3] = {(float)ix * dx, (float)iy * dx, (float)iz * dx};
+            for (int c = 0; c < prm.n_colliders; ++c) {
+                const pm_collider col = prm.colliders[c];
+                const float *o = ctrl->col_origin[c];
+                const float *vc = ctrl->col_vel[c];
+                if (col.kind == 0) {   // halfspace_collider (847-867)
+                    const float nn[3] = {(float)col.normal[0], (float)col.normal[1], (float)col.normal[2]};
+                    const float sd = (pos[0] - o[0]) * nn[0] + (pos[1] - o[1]) * nn[1] + (pos[2] - o[2]) * nn[2];
+                    if (sd < 0.0f) resolve(v, vc, nn, col.mode == 1, (float)col.friction);
+                } else {               // sphere_collider (828-844)
+                    const float r0 = pos[0] - o[0], r1 = pos[1] - o[1], r2 = pos[2] - o[2];
+                    const float dist = sqrtf(r0 * r0 + r1 * r1 + r2 * r2);
+                    if (dist < (float)col.radius) {
+                        const float den = dist + 1e-9f;
+                        const float nn[3] = {r0 / den, r1 / den, r2 / den};
+                        resolve(v, vc, nn, col.mode == 1, (float)col.friction);
+                    }
+                }
+            }
+        }
+        w.g_vel[node] = make_float4(v[0], v[1], v[2], 0.0f);
+        w.g_gd[node] = dmg.y > 1e-12f ? dmg.x / dmg.y : 0.0f;
+    }
+}
+
+void launch_grid(const pm_params &prm, const WS &w, cudaStream_t s) {
+    const long long max_items = w.n_blocks * 64;
+    const int blocks = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, 148LL * 8));
+    k_grid<<<blocks, 256, 0, s>>>(prm, w);
+}
+
+// --------------------------------------------------------------------- G2P
+// One thread per particle in sorted order: quadratic gather of grid velocity
+// (APIC v and C), cubic gather of the damage Laplacian at the start-of-step
+// position, then x += dt v, F <- (I + dt C) F, x clamped to [2dx, lim-2dx]
+// (anisompm.py:749-760, 781-803).
+__global__ void __launch_bounds__(256) k_g2p(const pm_params prm, const Parts P, const WS w) {
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n) return;
+    const long long p = w.perm[s];
+    const long long ps = P.ps;
+    const int ng = prm.n_grid;
+    const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx, dt = (float)prm.dt;
+    const float xp[3] = {P.x[p], P.x[ps + p], P.x[2 * ps + p]};
+
+    float nv[3] = {0.0f, 0.0f, 0.0f}, nC[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) nC[k] = 0.0f;
+    {
+        Quad q;
+        quad_weights(xp, inv_dx, ng, q);
+        int NX[3], NY[3], NZ[3];
+        float DX[3], DY[3], DZ[3];
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            NX[o] = clampi(q.b[0] + o, 0, ng - 1) * ng * ng;
+            NY[o] = clampi(q.b[1] + o, 0, ng - 1) * ng;
+            NZ[o] = clampi(q.b[2] + o, 0, ng - 1);
+            DX[o] = ((float)o - q.fx[0]) * dx;
+            DY[o] = ((float)o - q.fx[1]) * dx;
+            DZ[o] = ((float)o - q.fx[2]) * dx;
+        }
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy) {
+                const float wxy = q.w[ox][0] * q.w[oy][1];
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) {
+                    const float wk = wxy * q.w[oz][2];
+                    const float4 g = __ldg(&w.g_vel[NX[ox] + NY[oy] + NZ[oz]]);
+                    nv[0] += wk * g.x; nv[1] += wk * g.y; nv[2] += wk * g.z;
+                    const float dp[3] = {DX[ox], DY[oy], DZ[oz]};
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        nC[j] += wk * (g.x * dp[j]);
+                        nC[3 + j] += wk * (g.y * dp[j]);
+                        nC[6 + j] += wk * (g.z * dp[j]);
+                    }
+                }
+            }
+        const float cfac = (float)(4.0 * prm.inv_dx * prm.inv_dx);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) nC[k] *= cfac;
+    }
+    float lap = 0.0f;
+    {
+        Cubic c;
+        cubic_weights(xp, inv_dx, ng, c);
+        int NX[4], NY[4], NZ[4];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            NX[o] = clampi(c.b[0] + o, 0, ng - 1) * ng * ng;
+            NY[o] = clampi(c.b[1] + o, 0, ng - 1) * ng;
+            NZ[o] = clampi(c.b[2] + o, 0, ng - 1);
+        }
+        const float lfac = (float)(prm.inv_dx * prm.inv_dx);
+#pragma unroll
+        for (int ox = 0; ox < 4; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 4; ++oy) {
+                const float a = c.w2[ox][0] * c.w[oy][1], b = c.w[ox][0] * c.w2[oy][1], e = c.w[ox][0] * c.w[oy][1];
+#pragma unroll
+                for (int oz = 0; oz < 4; ++oz) {
+                    const float lw = lfac * (a * c.w[oz][2] + b * c.w[oz][2] + e * c.w2[oz][2]);
+                    lap += lw * __ldg(&w.g_gd[NX[ox] + NY[oy] + NZ[oz]]);
+                }
+            }
+    }
+    // advection, F update, domain clamp (793-802)
+    const float pad = (float)(2.0 * prm.dx), hi = (float)(prm.grid_lim - 2.0 * prm.dx);
+    float xn[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float t = xp[a] + dt * nv[a];
+        t = t < pad ? pad : t;
+        xn[a] = t > hi ? hi : t;
+    }
+    float F[9], Fn[9], A[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        F[k] = P.F[k * ps + p];
+        A[k] = ((k % 4 == 0) ? 1.0f : 0.0f) + dt * nC[k];
+    }
+    mm3(A, F, Fn);
+    bool finite = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) finite = finite && isfinite(xn[a]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) finite = finite && isfinite(Fn[k]);
+    const unsigned bad = __ballot_sync(__activemask(), !finite);
+    if (bad && (threadIdx.x & 31) == __ffs(bad) - 1) atomicAdd(&w.ctrl->nonfinite, (unsigned)__popc(bad));
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        P.x[a * ps + p] = xn[a];
+        P.v[a * ps + p] = nv[a];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        P.F[k * ps + p] = Fn[k];
+        P.C[k * ps + p] = nC[k];
+    }
+    P.lap[p] = lap;
+}
+
+void launch_g2p(const pm_params &prm, const Parts &P, const WS &w, cudaStream_t s) {
+    const long long blocks = (P.n + 255) / 256;
+    if (blocks <= 0) return;
+    k_g2p<<<(unsigned)blocks, 256, 0, s>>>(prm, P, w);
+}
+
+// ---------------------------------------------------------------- sym_eig
+__global__ void __launch_bounds__(256) k_sym_eig(const float *__restrict__ A, long long n, int sweeps,
+                                                 float *__restrict__ ev, float *__restrict__ V) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float a[9], e[3], vv[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = A[9 * p + k];
+    switch (sweeps) {
+        case 1: sym_eig3<1>(a, e, vv); break;
+        case 2: sym_eig3<2>(a, e, vv); break;
+        case 3: sym_eig3<3>(a, e, vv); break;
+        case 4: sym_eig3<4>(a, e, vv); break;
+        default: sym_eig3<5>(a, e, vv); break;
+        case 6: sym_eig3<6>(a, e, vv); break;
+        case 8: sym_eig3<8>(a, e, vv); break;
+        case 12: sym_eig3<12>(a, e, vv); break;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ev[3 * p + k] = e[k];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) V[9 * p + k] = vv[k];
+}
+
+void launch_sym_eig(const float *A, long long n, int sweeps, float *ev, float *V, cudaStream_t s) {
+    if (n <= 0) return;
+    k_sym_eig<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, n, sweeps, ev, V);
+}
+
+}  // namespace pm

@@ -1,0 +1,347 @@
+"""Parity of the sm_100a path with the oracle and the reference goldens.
+
+Every call goes through the C ABI (libpeelmpm.so).  Metric: relative L2 over
+all particles, per field.  Bounds:
+  * binning: bit-exact (integer keys and permutation);
+  * one substep or a pre-fracture window: 1e-5 (float32 rounding: FMA
+    contraction and atomic summation order differ from the reference);
+  * x, v, F, C after the full step counts: 1e-4 (the parity target);
+  * d and lap after fracture: 10x the reference's own scatter-order noise
+    (tests/golden/reference_goldens.json), because the damage update's
+    threshold branches flip under any rounding change, float64 included.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import FIELDS, golden_state, goldens, gpu_state, make_gpu_sim, rel_l2
+import oracle as orc
+from peel_mpm_b200 import _lib, scenes
+import peel_mpm_b200 as pm
+
+pytestmark = pytest.mark.gpu
+
+KIN = ("x", "v", "F", "C")
+
+
+def ws_views(sim):
+    L = _lib.workspace_layout(sim.n, sim.n_grid)
+    G = sim.n_grid ** 3
+    ws = sim._ws
+
+    def view(off, nbytes, dtype):
+        return ws[off:off + nbytes].view(dtype)
+
+    par = L.sort_passes & 1
+    return {
+        "g_mom": view(L.g_mom, 16 * G, torch.float32).view(G, 4),
+        "g_dmg": view(L.g_dmg, 8 * G, torch.float32).view(G, 2),
+        "g_vel": view(L.g_vel, 16 * G, torch.float32).view(G, 4),
+        "g_gd": view(L.g_gd, 4 * G, torch.float32),
+        "keys": view(L.keys_b if par else L.keys_a, 4 * sim.n, torch.int32),
+        "perm": view(L.vals_b if par else L.vals_a, 4 * sim.n, torch.int32),
+    }
+
+
+def run_pieces(sim, time, stages):
+    """Enqueue some of the substep's pieces through the C ABI, in order:
+    'bin' (clock + binning), 'p2g', 'grid', 'g2p'."""
+    grips, calls = sim._descriptors()
+    assert not calls
+    sim._grip_tags(grips)
+    prm = sim._build_params(grips)
+    sim._ensure_ws()
+    P = sim._particles()
+    lib = sim._lib
+    s = torch.cuda.current_stream().cuda_stream
+    ws, nb = sim._ws.data_ptr(), sim._ws_bytes
+    if "bin" in stages:
+        clk = sim._clock(time, sim._step)
+        _lib.check(lib.pm_set_clock(C.byref(prm), ws, nb, sim.n, C.byref(clk), s))
+        _lib.check(lib.pm_bin(C.byref(prm), C.byref(P), ws, nb, s))
+    if "p2g" in stages:
+        _lib.check(lib.pm_p2g(C.byref(prm), C.byref(P), ws, nb, s))
+    if "grid" in stages:
+        _lib.check(lib.pm_grid_update(C.byref(prm), ws, nb, sim.n, s))
+    if "g2p" in stages:
+        _lib.check(lib.pm_g2p(C.byref(prm), C.byref(P), ws, nb, s))
+        sim._step += 1
+
+
+def blocked_keys_np(x, ng, inv_dx):
+    """Block-major sort key from the oracle's (reference) base cells."""
+    k = orc.bin_keys(x, ng, inv_dx)
+    cx, cy, cz = k // (ng * ng), (k // ng) % ng, k % ng
+    nb = (ng + 7) // 8
+    blk = ((cx >> 3) * nb + (cy >> 3)) * nb + (cz >> 3)
+    return (blk << 9) | ((cx & 7) << 6) | ((cy & 7) << 3) | (cz & 7)
+
+
+# ------------------------------------------------------------------ eigensolver
+def test_sym_eig_matches_reference_goldens():
+    arr, _ = goldens()
+    A = torch.tensor(arr["sym_eig/A"], device="cuda")
+    ev, V = pm.sym_eig(A)
+    ev, V = ev.cpu().numpy(), V.cpu().numpy()
+    ref_ev = arr["sym_eig/evals"]
+    assert np.max(np.abs(ev - ref_ev)) <= 2e-5 * max(1.0, np.abs(ref_ev).max())
+    An = arr["sym_eig/A"].astype(np.float64)
+    recon = V @ (ev[:, :, None] * np.swapaxes(V, 1, 2))
+    assert np.max(np.abs(recon - An)) < 1e-4 * max(1.0, np.abs(An).max())
+    ortho = np.swapaxes(V, 1, 2) @ V - np.eye(3)
+    assert np.max(np.abs(ortho)) < 1e-5
+    assert np.all(np.diff(ev, axis=1) >= 0)
+
+
+def test_sym_eig_degenerate_and_empty():
+    A = torch.eye(3, device="cuda").expand(5, 3, 3).contiguous() * 2.0
+    ev, V = pm.sym_eig(A)
+    assert torch.equal(ev, torch.full((5, 3), 2.0, device="cuda"))
+    assert torch.equal(V, torch.eye(3, device="cuda").expand(5, 3, 3))
+    ev, V = pm.sym_eig(torch.zeros(0, 3, 3, device="cuda"))
+    assert ev.shape == (0, 3) and V.shape == (0, 3, 3)
+
+
+# ------------------------------------------------------------------ binning
+@pytest.mark.parametrize("name", ["plain_small", "tiny_bar"])
+@pytest.mark.parametrize("s", [0, 1])
+def test_bin_sort_bit_exact_vs_reference(name, s):
+    arr, _ = goldens()
+    x = torch.tensor(arr[f"bin/{name}/{s}/x"], device="cuda")
+    sc = scenes.SCENES[name]()
+    keys, perm = pm.bin_particles(x, sc.n_grid, 1.0 / sc.dx)
+    assert np.array_equal(keys.cpu().numpy(), arr[f"bin/{name}/{s}/keys"][arr[f"bin/{name}/{s}/perm"]])
+    assert np.array_equal(perm.cpu().numpy(), arr[f"bin/{name}/{s}/perm"])
+
+
+@pytest.mark.parametrize("n,ng,seed", [(1 << 20, 128, 0), (100_003, 64, 1), (4097, 36, 2), (1, 8, 3), (0, 16, 4)])
+def test_bin_sort_bit_exact_random(n, ng, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-0.05, 1.05, size=(n, 3)).astype(np.float32)
+    if n > 10:
+        x[:5] = [[np.nan, 0.5, 0.5], [1e30, 0.2, 0.3], [-1e30, 0.1, 0.9], [0.5, 0.5, 0.5], [0, 0, 0]]
+    keys_ref, perm_ref = orc.bin_particles(x, ng, float(ng))
+    keys, perm = pm.bin_particles(torch.tensor(x, device="cuda"), ng, float(ng))
+    assert np.array_equal(perm.cpu().numpy(), perm_ref)
+    assert np.array_equal(keys.cpu().numpy(), keys_ref[perm_ref])
+
+
+def test_substep_sort_is_stable_argsort_of_blocked_keys():
+    sc = scenes.plain_1m(cells=(24, 16, 40), lo=(40, 50, 30))
+    sim = make_gpu_sim(sc)
+    run_pieces(sim, 0.0, ("bin",))
+    w = ws_views(sim)
+    x = sim.x.cpu().numpy()
+    kb = blocked_keys_np(x, sc.n_grid, 1.0 / sc.dx)
+    perm_ref = np.argsort(kb, kind="stable")
+    assert np.array_equal(w["perm"].cpu().numpy(), perm_ref)
+    assert np.array_equal(w["keys"].cpu().numpy().astype(np.int64), kb[perm_ref])
+
+
+# ------------------------------------------------------------------ per kernel
+@pytest.mark.parametrize("name", ["tiny_bar", "knobs_drop", "interface_peel"])
+def test_kernels_match_oracle_grids(name):
+    sc = scenes.SCENES[name]()
+    sim = make_gpu_sim(sc)
+    ora = orc.OracleSim(sc, np.float32)
+    # advance both a few steps so C, F, d are non-trivial
+    for s in range(3):
+        sim.substep(s * sc.dt)
+        ora.substep(s * sc.dt)
+    t = 3 * sc.dt
+    grids = ora.alloc_grids()
+    ora.substep(t, grids=grids)
+    G = sc.n_grid ** 3
+
+    run_pieces(sim, t, ("bin", "p2g"))
+    w = ws_views(sim)
+    mom = w["g_mom"].cpu().numpy().astype(np.float64)
+    dmg = w["g_dmg"].cpu().numpy().astype(np.float64)
+    assert rel_l2(grids["grid_mv"], mom[:, :3]) < 1e-5
+    assert rel_l2(grids["grid_m"], mom[:, 3]) < 1e-6
+    assert rel_l2(grids["grid_dc"], dmg[:, 0]) < 1e-5
+    assert rel_l2(grids["grid_dwc"], dmg[:, 1]) < 1e-6
+    for f in ("d", "D_hist"):
+        assert rel_l2(getattr(ora, f), getattr(sim, f).cpu().numpy()) < 1e-6, f
+
+    run_pieces(sim, t, ("grid",))
+    w = ws_views(sim)
+    active = grids["grid_m"] > 1e-12
+    vel = w["g_vel"].cpu().numpy()[:, :3]
+    assert rel_l2(grids["grid_v"][active], vel[active]) < 1e-5
+    assert rel_l2(grids["gd"], np.where(grids["grid_dwc"] > 1e-12, w["g_gd"].cpu().numpy(), 0.0)) < 1e-5
+    # the grid update leaves the accumulators zeroed for the next substep
+    assert float(w["g_mom"].abs().max()) == 0.0 and float(w["g_dmg"].abs().max()) == 0.0
+
+    run_pieces(sim, t, ("g2p",))
+    st = gpu_state(sim)
+    for f in FIELDS:
+        assert rel_l2(getattr(ora, f), st[f]) < 1e-5, f
+
+
+# ------------------------------------------------------------------ whole substeps vs goldens
+def _compare_to_goldens(name, steps, stride):
+    _, meta = goldens()
+    sc = scenes.SCENES[name]()
+    sim = make_gpu_sim(sc)
+    out = {}
+    for s in range(max(steps)):
+        sim.substep(s * sc.dt)
+        if s + 1 in steps:
+            g = golden_state(name, "f32", s + 1)
+            st = gpu_state(sim, stride)
+            out[s + 1] = {f: rel_l2(g[f], st[f]) for f in FIELDS}
+    assert sim.status()["nonfinite"] == 0
+    return out, meta
+
+
+def test_tiny_bar_vs_reference():
+    errs, meta = _compare_to_goldens("tiny_bar", [1, 10, 50, 200], 1)
+    env = meta["noise_envelope"]["tiny_bar_200"]
+    for f in FIELDS:
+        assert errs[1][f] < 1e-5, (f, errs[1])
+        assert errs[10][f] < 1e-4, (f, errs[10])
+    for s in (50, 200):
+        for f in KIN:
+            assert errs[s][f] < 1e-4, (s, f, errs[s])
+    for f in ("d", "lap"):
+        assert errs[200][f] < 10 * max(env[f], 1e-4), (f, errs[200])
+
+
+def test_plain_small_vs_reference():
+    errs, meta = _compare_to_goldens("plain_small", [1, 50, 200], 8)
+    env = meta["noise_envelope"]["plain_small_200"]
+    for f in FIELDS:
+        assert errs[1][f] < 1e-5, (f, errs[1])
+    for s in (50, 200):
+        for f in KIN:
+            assert errs[s][f] < 1e-4, (s, f, errs[s])
+    for f in ("d", "lap"):
+        assert errs[200][f] < 10 * max(env[f], 1e-4), (f, errs[200])
+
+
+@pytest.mark.parametrize("name", ["knobs_drop", "interface_peel"])
+def test_knob_scenes_vs_reference(name):
+    errs, _ = _compare_to_goldens(name, [10, 60], 1)
+    for f in FIELDS:
+        assert errs[10][f] < 1e-4, (f, errs[10])
+    for f in KIN:
+        assert errs[60][f] < 1e-4, (f, errs[60])
+
+
+def test_plain_slab_vs_oracle_long_run():
+    """A 32k-particle slab with the 1M scene's statistics, 100 substeps."""
+    sc = scenes.plain_1m(cells=(16, 16, 16), lo=(56, 56, 56))
+    sim = make_gpu_sim(sc)
+    ora = orc.OracleSim(sc, np.float32, nthreads=8, scatter_mode=1)
+    for s in range(100):
+        sim.substep(s * sc.dt)
+        ora.substep(s * sc.dt)
+    st = gpu_state(sim)
+    for f in KIN:
+        assert rel_l2(getattr(ora, f), st[f]) < 1e-4, f
+    for f in ("d", "D_hist", "lap"):
+        assert rel_l2(getattr(ora, f), st[f]) < 1e-3, f
+
+
+# ------------------------------------------------------------------ full size, size-independent properties
+def test_plain_1m_properties_and_first_step():
+    sc = scenes.plain_1m()
+    sim = make_gpu_sim(sc)
+    ora = orc.OracleSim(sc, np.float32, nthreads=8, scatter_mode=1)
+    sim.substep(0.0)
+    ora.substep(0.0)
+    st = gpu_state(sim)
+    for f in FIELDS:
+        assert rel_l2(getattr(ora, f), st[f]) < 1e-5, f
+    d_prev = sim.d.clone()
+    dh_prev = sim.D_hist.clone()
+    frozen = ~sim.allow
+    d_frozen = sim.d[frozen].clone()
+    for s in range(1, 30):
+        sim.substep(s * sc.dt)
+        assert bool((sim.d >= d_prev).all())          # monotone damage (685)
+        assert bool((sim.D_hist >= dh_prev).all())    # history max (679)
+        d_prev.copy_(sim.d)
+        dh_prev.copy_(sim.D_hist)
+    assert float(sim.d.min()) >= 0.0 and float(sim.d.max()) <= 1.0
+    assert torch.equal(sim.d[frozen], d_frozen)
+    lo, hi = 2 * sim.dx, sim.grid_lim - 2 * sim.dx
+    assert float(sim.x.min()) >= np.float32(lo) and float(sim.x.max()) <= np.float32(hi)
+    st = sim.status()
+    assert st["nonfinite"] == 0 and st["any_allow"] == 1 and st["n_active_blocks"] > 0
+
+
+# ------------------------------------------------------------------ edge cases
+def test_particles_outside_grid_and_odd_grid_size():
+    """Positions beyond the domain clamp onto edge nodes exactly as the
+    reference's _node_index does; n_grid not a multiple of the block size."""
+    rng = np.random.default_rng(5)
+    ng = 36
+    x = rng.uniform(0.3, 0.7, size=(3000, 3))
+    x[:10] = [[-0.2, 0.5, 0.5], [1.3, 0.5, 0.5], [0.5, -1.0, 2.0], [0.01, 0.01, 0.01], [0.99, 0.99, 0.99],
+              [0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [0.5, 0.5, 1.2], [-0.01, 0.5, 0.5], [0.5, 1.01, 0.5]]
+    sc = scenes.Scene(name="edge", n_grid=ng, grid_lim=1.0, dt=1e-4, n_steps=5, x=x, vol=np.full(3000, 1e-6),
+                      rho=800.0, E=np.full(3000, 5e3), nu=0.3, fibers=None, alpha=0.0,
+                      sigma_c=np.full(3000, 50.0), d0=rng.uniform(0, 0.2, 3000), allow=np.ones(3000, bool),
+                      gravity=(0.0, -9.8, 0.0))
+    sim = make_gpu_sim(sc)
+    ora = orc.OracleSim(sc, np.float32)
+    for s in range(5):
+        sim.substep(s * sc.dt)
+        ora.substep(s * sc.dt)
+    st = gpu_state(sim)
+    for f in FIELDS:
+        assert rel_l2(getattr(ora, f), st[f]) < 1e-5, f
+
+
+def test_single_particle_and_empty_solver():
+    sim = pm.AnisoMPM(n_grid=16, dt=1e-4, device="cuda:0")
+    sim.substep(0.0)                      # no particles: a no-op
+    assert sim._step == 1
+    sim.add_object(torch.tensor([[0.5, 0.5, 0.5]]), torch.tensor([1e-6]), E=1e3)
+    for s in range(3):
+        sim.substep(s * 1e-4)
+    v = sim.v.cpu().numpy()
+    np.testing.assert_allclose(v[0], [0.0, -9.8 * 3e-4, 0.0], rtol=1e-5, atol=1e-9)
+
+
+def test_nonfinite_position_is_contained_and_reported():
+    """A NaN position maps to node 0 (as torch's floor().long() does) and is
+    counted by the device status; other particles far away are unaffected."""
+    sc = scenes.tiny_bar()
+    sim = make_gpu_sim(sc)
+    ref = make_gpu_sim(sc)
+    with torch.no_grad():
+        sim.x[0] = float("nan")
+    sim.substep(0.0)
+    ref.substep(0.0)
+    assert sim.status()["nonfinite"] >= 1
+    far = torch.arange(1, sc.n, device="cuda")
+    assert rel_l2(ref.x[far].cpu().numpy(), sim.x[far].cpu().numpy()) < 1e-6
+    assert rel_l2(ref.v[far].cpu().numpy(), sim.v[far].cpu().numpy()) < 1e-5
+
+
+def test_c_abi_rejects_bad_arguments():
+    sim = make_gpu_sim(scenes.tiny_bar())
+    sim.substep(0.0)
+    grips, _ = sim._descriptors()
+    prm = sim._build_params(grips)
+    P = sim._particles()
+    clk = sim._clock(0.0, 0)
+    lib = sim._lib
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib.pm_substep(C.byref(prm), C.byref(P), sim._ws.data_ptr(), 1024, C.byref(clk), s) == \
+        _lib.PM_ERR_WORKSPACE
+    bad = _lib.pm_params.from_buffer_copy(prm)
+    bad.n_grid = 2
+    assert lib.pm_substep(C.byref(bad), C.byref(P), sim._ws.data_ptr(), sim._ws_bytes, C.byref(clk), s) == \
+        _lib.PM_ERR_ARG
+    assert lib.pm_substep(C.byref(prm), C.byref(P), sim._ws.data_ptr() + 8, sim._ws_bytes, C.byref(clk), s) == \
+        _lib.PM_ERR_WORKSPACE
+    with pytest.raises(NotImplementedError):
+        pm.AnisoMPM(n_grid=16, dtype=torch.float64)
+    with pytest.raises(ValueError):
+        pm.AnisoMPM(n_grid=16, device="cpu")
