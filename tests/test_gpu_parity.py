@@ -293,8 +293,13 @@ def test_particles_outside_grid_and_odd_grid_size():
         sim.substep(s * sc.dt)
         ora.substep(s * sc.dt)
     st = gpu_state(sim)
-    for f in FIELDS:
+    for f in ("x", "v", "F", "d", "lap", "D_hist"):
         assert rel_l2(getattr(ora, f), st[f]) < 1e-5, f
+    # C is ~0 here (near-uniform motion of sparse particles): its float32 value
+    # is rounding noise (the oracle's own two scatter orders differ by ~20%),
+    # so bound the difference by the scale of a velocity gradient, |v| 4/dx.
+    scale = np.linalg.norm(ora.v) * 4.0 * sim.inv_dx
+    assert np.linalg.norm(ora.C - st["C"]) / scale < 1e-6
 
 
 def test_single_particle_and_empty_solver():
