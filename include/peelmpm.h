@@ -194,6 +194,24 @@ int pm_sym_eig(const float *A, int64_t n, int32_t sweeps, float *evals, float *e
 int pm_bin_sort(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid, double inv_dx,
                 uint32_t *keys_out, int32_t *perm_out, void *ws, size_t ws_bytes, void *stream);
 
+/* Binning exactly as pm_bin_sort, for callers that cannot allocate device
+ * memory: a host application that owns every device allocation and hands a
+ * plugin only its input and output buffers, or code that must not call
+ * cudaMalloc/cudaFree (which can synchronise the whole device) in a
+ * latency-bound loop.  The sort's scratch is a static array inside this
+ * library (PM_BIN_STATIC_SCRATCH_BYTES on every GPU that loads it, held until
+ * the process exits), so the caller passes only x, keys_out and perm_out.
+ * n above PM_BIN_STATIC_MAX_N returns PM_ERR_ARG.  The first call on a device
+ * looks up the array's device address; make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller.
+ * No counterpart in the reference, which has no binning and never allocates
+ * outside PyTorch. */
+#define PM_BIN_STATIC_MAX_N 262144
+#define PM_BIN_STATIC_SCRATCH_BYTES (16u * PM_BIN_STATIC_MAX_N + 4u * (256u * (PM_BIN_STATIC_MAX_N / 4096u) + 256u))
+int pm_bin_sort_static(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid, double inv_dx,
+                       uint32_t *keys_out, int32_t *perm_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

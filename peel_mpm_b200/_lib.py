@@ -19,8 +19,9 @@ PM_OK, PM_ERR_ARG, PM_ERR_CUDA, PM_ERR_WORKSPACE, PM_ERR_UNSUPPORTED = 0, 1, 2, 
 EXPORTS = (
     "pm_abi_version", "pm_last_error", "pm_struct_size", "pm_workspace_size", "pm_workspace_init",
     "pm_workspace_layout", "pm_substep", "pm_substep_dev_clock", "pm_set_clock", "pm_bin", "pm_p2g",
-    "pm_grid_update", "pm_g2p", "pm_read_status", "pm_sym_eig", "pm_bin_sort",
+    "pm_grid_update", "pm_g2p", "pm_read_status", "pm_sym_eig", "pm_bin_sort", "pm_bin_sort_static",
 )
+PM_BIN_STATIC_MAX_N = 262144
 
 
 class pm_grip(C.Structure):
@@ -106,6 +107,7 @@ def load():
         "pm_read_status": (C.c_int, [vp, sz, i64, i32, C.POINTER(pm_status_info), vp]),
         "pm_sym_eig": (C.c_int, [vp, i64, i32, vp, vp, vp]),
         "pm_bin_sort": (C.c_int, [vp, i64, i64, i32, C.c_double, vp, vp, vp, sz, vp]),
+        "pm_bin_sort_static": (C.c_int, [vp, i64, i64, i32, C.c_double, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

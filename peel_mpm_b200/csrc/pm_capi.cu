@@ -73,6 +73,11 @@ int get_ws(void *ws, size_t bytes, long long n, int ng, pm::WS *out) {
 
 }  // namespace
 
+namespace pm {
+// Lets other translation units of the library report through pm_last_error().
+int report_error(int code, const char *msg) { return fail(code, msg); }
+}  // namespace pm
+
 extern "C" {
 
 int pm_abi_version(void) { return PM_ABI_VERSION; }
