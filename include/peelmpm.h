@@ -128,6 +128,11 @@ const char *pm_last_error(void);
  * 2 pm_clock, 3 pm_status_info, 4 pm_ws_layout, 5 pm_grip, 6 pm_collider. */
 size_t pm_struct_size(int32_t which);
 
+/* One-time set-up of the current device (kernel attributes).  Every entry
+ * point does it on first use; call it before capturing pm_* calls into a CUDA
+ * graph, since attribute changes are not stream operations. */
+int pm_prepare(void);
+
 /* Workspace for n particles on an n_grid^3 grid: grids, sort buffers, block
  * lists and the control block.  Must be zeroed once by pm_workspace_init. */
 int pm_workspace_size(int64_t n, int32_t n_grid, size_t *bytes);
@@ -136,7 +141,7 @@ int pm_workspace_init(void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, void
 /* Byte offsets of the workspace's views (for inspection and tests). */
 typedef struct pm_ws_layout {
     size_t ctrl, keys_a, keys_b, vals_a, vals_b, hist, block_mask, block_list;
-    size_t g_mom, g_dmg, g_vel, g_gd, total;
+    size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, total;
     int32_t sort_passes;             /* sorted keys/perm end in *_a if even, *_b if odd */
     int32_t n_tiles;
 } pm_ws_layout;

@@ -17,7 +17,7 @@ PM_MAX_COLLIDERS = 8
 PM_OK, PM_ERR_ARG, PM_ERR_CUDA, PM_ERR_WORKSPACE, PM_ERR_UNSUPPORTED = 0, 1, 2, 3, 4
 
 EXPORTS = (
-    "pm_abi_version", "pm_last_error", "pm_struct_size", "pm_workspace_size", "pm_workspace_init",
+    "pm_abi_version", "pm_last_error", "pm_struct_size", "pm_prepare", "pm_workspace_size", "pm_workspace_init",
     "pm_workspace_layout", "pm_substep", "pm_substep_dev_clock", "pm_set_clock", "pm_bin", "pm_p2g",
     "pm_grid_update", "pm_g2p", "pm_read_status", "pm_sym_eig", "pm_bin_sort", "pm_bin_sort_static",
 )
@@ -67,7 +67,7 @@ class pm_status_info(C.Structure):
 
 class pm_ws_layout(C.Structure):
     _fields_ = [(f, C.c_size_t) for f in ("ctrl", "keys_a", "keys_b", "vals_a", "vals_b", "hist", "block_mask",
-                                          "block_list", "g_mom", "g_dmg", "g_vel", "g_gd", "total")] + \
+                                          "block_list", "g_mom", "g_dmg", "g_vel", "g_gd", "payload", "inv_perm", "total")] + \
                [("sort_passes", C.c_int32), ("n_tiles", C.c_int32)]
 
 
@@ -94,6 +94,7 @@ def load():
         "pm_abi_version": (C.c_int, []),
         "pm_last_error": (C.c_char_p, []),
         "pm_struct_size": (sz, [i32]),
+        "pm_prepare": (C.c_int, []),
         "pm_workspace_size": (C.c_int, [i64, i32, C.POINTER(sz)]),
         "pm_workspace_init": (C.c_int, [vp, sz, i64, i32, vp]),
         "pm_workspace_layout": (C.c_int, [i64, i32, C.POINTER(pm_ws_layout)]),

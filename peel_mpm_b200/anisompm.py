@@ -59,7 +59,9 @@ class ParticleGrip:
     """Prescribed-velocity particles: ``v = velocity * min(t / ramp, 1)``
     (ramp <= 0: no ramp) overwrites v before P2G, inside the P2G kernel.
     Device form of a particle_bc closure that pins ``s.v[mask]``
-    (test_block.py:109-113, peel_test.py:233-236)."""
+    (test_block.py:109-113, peel_test.py:233-236).  The solver turns the mask
+    into a per-particle tag once per descriptor: make a new descriptor rather
+    than editing the mask of one already in ``particle_bc``."""
 
     def __init__(self, mask, velocity: Sequence[float], ramp: float = 0.0):
         self.mask = mask
@@ -197,6 +199,7 @@ class AnisoMPM:
         self.particle_bc = []
         self.n = 0
         self.record_stress = False
+        self.use_graphs = True
         self._S = None            # float32 planes (N_PLANES, stride)
         self._allow = None        # bool (N)
         self._imask = None        # bool (N)
@@ -420,7 +423,7 @@ class AnisoMPM:
 
     def _grip_tags(self, grips):
         key = tuple(id(g) for g in grips)
-        if self._tag is not None and key == self._tag_key:
+        if self._tag_key is not None and key == self._tag_key:
             return
         if not grips:
             self._tag = None
@@ -527,9 +530,48 @@ class AnisoMPM:
         self._step += 1
 
     def run_frame(self, n_sub: int, time0: float = 0.0):
-        """anisompm.py:805-807"""
+        """n_sub substeps at time0 + s*dt (anisompm.py:805-807).
+
+        With ``use_graphs`` (default) and only device descriptors in
+        ``particle_bc``, the frame's substeps are captured once into a CUDA
+        graph per (n_sub, parameters, storage) and replayed; each frame's
+        times, step numbers and collider origins go to the device in one copy
+        from pinned memory, so a frame costs one graph launch on the host."""
+        n_sub = int(n_sub)
+        if n_sub <= 0:
+            return
+        grips, calls = self._descriptors()
+        if calls or not self.use_graphs or self.n == 0:
+            for s in range(n_sub):
+                self.substep(time0 + s * self.dt)
+            return
+        self._grip_tags(grips)
+        prm = self._build_params(grips)
+        self._ensure_ws()
+        P = self._particles()
+        host = torch.empty(n_sub * C.sizeof(_lib.pm_clock), dtype=torch.uint8, pin_memory=True)
+        clocks = (_lib.pm_clock * n_sub).from_address(host.data_ptr())
         for s in range(n_sub):
-            self.substep(time0 + s * self.dt)
+            clocks[s] = self._clock(time0 + s * self.dt, self._step + s)
+        key = (n_sub, self._params_key, id(P), self._ws.data_ptr(), self._S.data_ptr())
+        entry = self._graphs.get(key)
+        if entry is None:
+            table = torch.empty(host.numel(), dtype=torch.uint8, device=self.device)
+            _lib.check(self._lib.pm_prepare(), "pm_prepare")
+            torch.cuda.synchronize(self.device)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                st = torch.cuda.current_stream().cuda_stream
+                for s in range(n_sub):   # row s of the device clock table drives substep s
+                    _lib.check(self._lib.pm_substep_dev_clock(C.byref(prm), C.byref(P), self._ws.data_ptr(),
+                                                              self._ws_bytes, table.data_ptr(), s, st),
+                               "pm_substep_dev_clock")
+            entry = (g, table, prm, P)
+            self._graphs[key] = entry
+        g, table = entry[0], entry[1]
+        table.copy_(host, non_blocking=True)
+        g.replay()
+        self._step += n_sub
 
     # ------------------------------------------------------------------ status
     def status(self) -> dict:

@@ -1,5 +1,6 @@
 // Particle binning: per-substep cell keys and a stable LSD radix sort of
-// (key, particle id), plus the list of active 4^3 grid blocks.
+// (key, particle id), and the compaction of the active 4^3 grid blocks that
+// P2G marks.
 //
 // Key = _node_index(base) of the quadratic base cell (anisompm.py:544-548,
 // 586-590), x-major with z fastest.  The permutation equals the stable
@@ -8,34 +9,21 @@
 
 namespace pm {
 
-// Keys, identity ids, active-block marks and allow.any().  blocked = false
-// gives the reference's x-major cell index, true the block-major sort key.
+// Keys, identity ids and allow.any().  blocked = false gives the reference's
+// x-major cell index, true the block-major sort key.
 __global__ void __launch_bounds__(256) k_keys(const float *__restrict__ x, long long n, long long ps, int ng,
                                               float inv_dx, bool blocked, unsigned *__restrict__ keys,
-                                              int *__restrict__ vals, unsigned char *__restrict__ block_mask,
-                                              int nbs, const unsigned char *__restrict__ allow, Ctrl *ctrl) {
+                                              int *__restrict__ vals, const unsigned char *__restrict__ allow,
+                                              Ctrl *ctrl) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     bool any = false;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         const float xp[3] = {x[p], x[ps + p], x[2 * ps + p]};
-        int qb[3], lo[3], hi[3];
+        int qb[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float X = __fmul_rn(xp[a], inv_dx);
-            qb[a] = sat_base(floorf(__fsub_rn(X, 0.5f)), ng);
-            const int cb = sat_base(floorf(X), ng) - 1;
-            // nodes touched by the quadratic [qb, qb+2] and cubic [cb, cb+3] stencils
-            const int l = min(qb[a], cb), h = max(qb[a] + 2, cb + 3);
-            lo[a] = clampi(l, 0, ng - 1) / kBlockEdge;
-            hi[a] = clampi(h, 0, ng - 1) / kBlockEdge;
-        }
+        for (int a = 0; a < 3; ++a) qb[a] = sat_base(floorf(__fsub_rn(__fmul_rn(xp[a], inv_dx), 0.5f)), ng);
         keys[p] = blocked ? blocked_key(qb, ng) : cell_key(qb, ng);
         vals[p] = (int)p;
-        if (block_mask == nullptr) continue;
-        for (int bx = lo[0]; bx <= hi[0]; ++bx)
-            for (int by = lo[1]; by <= hi[1]; ++by)
-                for (int bz = lo[2]; bz <= hi[2]; ++bz)
-                    block_mask[((long long)bx * nbs + by) * nbs + bz] = 1;
         if (allow != nullptr && allow[p]) any = true;
     }
     if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0 && ctrl != nullptr) ctrl->any_allow = 1;
@@ -63,21 +51,31 @@ __global__ void __launch_bounds__(256) k_compact_blocks(unsigned char *__restric
 
 // ------------------------------------------------------------ radix sort
 // Per tile (kSortTile keys) digit histogram -> hist[digit * n_tiles + tile].
+// Full tiles load keys as uint4 (order does not matter for a histogram); int32
+// shared atomics aggregate equal addresses in hardware.
 __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const unsigned *__restrict__ keys, long long n,
                                                              int shift, unsigned *__restrict__ hist, int n_tiles) {
     __shared__ unsigned cnt[kRadix];
     for (int i = threadIdx.x; i < kRadix; i += blockDim.x) cnt[i] = 0;
     __syncthreads();
     const long long t0 = (long long)blockIdx.x * kSortTile;
-    const int lane = threadIdx.x & 31;
-#pragma unroll 4
-    for (int it = 0; it < kSortItems; ++it) {
-        const long long i = t0 + (long long)it * kSortThreads + threadIdx.x;
-        const bool ok = i < n;
-        const unsigned dg = ok ? (keys[i] >> shift) & (kRadix - 1) : 0xffffffffu;
-        // warp-aggregate equal digits (sorted-ish input repeats digits a lot)
-        const unsigned peers = __match_any_sync(0xffffffffu, dg);
-        if (ok && lane == __ffs(peers) - 1) atomicAdd(&cnt[dg], (unsigned)__popc(peers));
+    if (t0 + kSortTile <= n) {
+        const uint4 *k4 = reinterpret_cast<const uint4 *>(keys + t0);
+        uint4 v[kSortItems / 4];
+#pragma unroll
+        for (int it = 0; it < kSortItems / 4; ++it) v[it] = k4[it * kSortThreads + threadIdx.x];
+#pragma unroll
+        for (int it = 0; it < kSortItems / 4; ++it) {
+            atomicAdd(&cnt[(v[it].x >> shift) & (kRadix - 1)], 1u);
+            atomicAdd(&cnt[(v[it].y >> shift) & (kRadix - 1)], 1u);
+            atomicAdd(&cnt[(v[it].z >> shift) & (kRadix - 1)], 1u);
+            atomicAdd(&cnt[(v[it].w >> shift) & (kRadix - 1)], 1u);
+        }
+    } else {
+        for (int it = 0; it < kSortItems; ++it) {
+            const long long i = t0 + (long long)it * kSortThreads + threadIdx.x;
+            if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & (kRadix - 1)], 1u);
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kRadix; i += blockDim.x) hist[(long long)i * n_tiles + blockIdx.x] = cnt[i];
@@ -118,36 +116,30 @@ __global__ void __launch_bounds__(256) k_radix_rowscan(unsigned *__restrict__ hi
 
 // Stable scatter of one digit pass.  Warp w of a tile owns keys
 // [w*512, w*512+512) of the tile and ranks them in 16 rounds of 32 in index
-// order; per-warp digit counters are then offset by the earlier warps.
+// order; per-warp digit counters are then offset by the earlier warps.  The
+// tile is first written to shared memory in (digit, rank) order, then copied
+// out so that consecutive threads write consecutive addresses of one digit's
+// run.
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *__restrict__ kin,
                                                                 const int *__restrict__ vin,
                                                                 unsigned *__restrict__ kout, int *__restrict__ vout,
                                                                 long long n, int shift,
                                                                 const unsigned *__restrict__ offs, int n_tiles,
-                                                                const unsigned *__restrict__ dtot) {
+                                                                const unsigned *__restrict__ dtot,
+                                                                int *__restrict__ inv) {
     constexpr int W = kSortThreads / 32;
     __shared__ unsigned wcnt[W][kRadix];
-    __shared__ unsigned dbase[kRadix];
+    __shared__ unsigned gbase[kRadix];     // global start of the tile's run of each digit
+    __shared__ unsigned lbase[kRadix];     // tile-local start of each digit
     __shared__ unsigned wtot[W];
+    __shared__ unsigned skey[kSortTile];
+    __shared__ int sval[kSortTile];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < W * kRadix; i += blockDim.x) (&wcnt[0][0])[i] = 0;
-    {   // exclusive scan of the digit totals (kRadix == kSortThreads)
-        const unsigned v = dtot[threadIdx.x];
-        unsigned incl = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) wtot[wid] = incl;
-        __syncthreads();
-        unsigned wpre = 0;
-#pragma unroll
-        for (int w = 0; w < W; ++w) wpre += (w < wid) ? wtot[w] : 0u;
-        dbase[threadIdx.x] = wpre + incl - v;
-    }
     __syncthreads();
-    const long long t0 = (long long)blockIdx.x * kSortTile + (long long)wid * (32 * kSortItems);
+    const long long tile0 = (long long)blockIdx.x * kSortTile;
+    const int tile_len = (int)min((long long)kSortTile, n - tile0);
+    const long long t0 = tile0 + (long long)wid * (32 * kSortItems);
     unsigned key[kSortItems];
     int val[kSortItems];
     unsigned rank[kSortItems];
@@ -171,30 +163,59 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *
         __syncwarp();
     }
     __syncthreads();
-    // exclusive prefix over warps per digit, then add the global tile offset
-    for (int dg = threadIdx.x; dg < kRadix; dg += blockDim.x) {
-        unsigned run = dbase[dg] + offs[(long long)dg * n_tiles + blockIdx.x];
+    {   // per digit (one per thread): exclusive prefix over warps, tile count
+        const int dg = threadIdx.x;   // kRadix == kSortThreads
+        unsigned run = 0;
 #pragma unroll
         for (int w = 0; w < W; ++w) {
             const unsigned c = wcnt[w][dg];
             wcnt[w][dg] = run;
             run += c;
         }
+        // exclusive scans over digits: global digit bases (dtot) and the tile's own counts
+        unsigned v = dtot[dg], vi = v, c = run, ci = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, vi, o);
+            const unsigned z = __shfl_up_sync(0xffffffffu, ci, o);
+            if (lane >= o) { vi += y; ci += z; }
+        }
+        __shared__ unsigned wv[W], wc[W];
+        if (lane == 31) { wv[wid] = vi; wc[wid] = ci; }
+        __syncthreads();
+        unsigned pv = 0, pc = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            pv += (w < wid) ? wv[w] : 0u;
+            pc += (w < wid) ? wc[w] : 0u;
+        }
+        gbase[dg] = pv + vi - v + offs[(long long)dg * n_tiles + blockIdx.x];
+        lbase[dg] = pc + ci - c;
     }
+    (void)wtot;
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const long long i = t0 + r * 32 + lane;
         if (i < n) {
             const unsigned dg = (key[r] >> shift) & (kRadix - 1);
-            const unsigned pos = wcnt[wid][dg] + rank[r];
-            kout[pos] = key[r];
-            vout[pos] = val[r];
+            const unsigned lp = lbase[dg] + wcnt[wid][dg] + rank[r];
+            skey[lp] = key[r];
+            sval[lp] = val[r];
         }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < tile_len; i += kSortThreads) {
+        const unsigned k = skey[i];
+        const unsigned dg = (k >> shift) & (kRadix - 1);
+        const unsigned gp = gbase[dg] + (unsigned)i - lbase[dg];
+        kout[gp] = k;
+        vout[gp] = sval[i];
+        if (inv != nullptr) inv[sval[i]] = (int)gp;   // last pass: position of each particle in the order
     }
 }
 
-void launch_sort(const WS &w, long long n, cudaStream_t s) {
+void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv) {
     const int tiles = w.n_tiles;
     unsigned *kin = w.keys_a, *kout = w.keys_b;
     int *vin = w.vals_a, *vout = w.vals_b;
@@ -202,7 +223,8 @@ void launch_sort(const WS &w, long long n, cudaStream_t s) {
         const int shift = pass * kRadixBits;
         k_radix_hist<<<tiles, kSortThreads, 0, s>>>(kin, n, shift, w.hist, tiles);
         k_radix_rowscan<<<kRadix, 256, 0, s>>>(w.hist, tiles, w.dtot);
-        k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, w.hist, tiles, w.dtot);
+        k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, w.hist, tiles, w.dtot,
+                                                       pass == w.passes - 1 ? inv : nullptr);
         unsigned *tk = kin; kin = kout; kout = tk;
         int *tv = vin; vin = vout; vout = tv;
     }
@@ -210,8 +232,11 @@ void launch_sort(const WS &w, long long n, cudaStream_t s) {
 
 void launch_keys(const WS &w, const Parts &P, int ng, float inv_dx, cudaStream_t s) {
     const int blocks = (int)std::min<long long>((P.n + 255) / 256, 148LL * 16);
-    k_keys<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(P.x, P.n, P.ps, ng, inv_dx, true, w.keys_a, w.vals_a,
-                                                  w.block_mask, w.nbs, P.allow, w.ctrl);
+    k_keys<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(P.x, P.n, P.ps, ng, inv_dx, true, w.keys_a, w.vals_a, P.allow,
+                                                  w.ctrl);
+}
+
+void launch_compact(const WS &w, cudaStream_t s) {
     const int cb = (int)std::min<long long>((w.n_blocks + 255) / 256, 148LL * 8);
     k_compact_blocks<<<cb > 0 ? cb : 1, 256, 0, s>>>(w.block_mask, w.n_blocks, w.block_list, w.ctrl);
 }
@@ -219,8 +244,8 @@ void launch_keys(const WS &w, const Parts &P, int ng, float inv_dx, cudaStream_t
 void launch_keys_only(const float *x, long long n, long long ps, int ng, float inv_dx, bool blocked, const WS &w,
                       cudaStream_t s) {
     const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-    k_keys<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(x, n, ps, ng, inv_dx, blocked, w.keys_a, w.vals_a, nullptr, 0,
-                                                  nullptr, nullptr);
+    k_keys<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(x, n, ps, ng, inv_dx, blocked, w.keys_a, w.vals_a, nullptr,
+                                                  nullptr);
 }
 
 }  // namespace pm

@@ -97,6 +97,13 @@ size_t pm_struct_size(int32_t which) {
     }
 }
 
+int pm_prepare(void) {
+    int rc = check_device();
+    if (rc) return rc;
+    pm::prepare_p2g();
+    return cuda_check("pm_prepare");
+}
+
 int pm_workspace_size(int64_t n, int32_t n_grid, size_t *bytes) {
     if (!bytes) return fail(PM_ERR_ARG, "bytes is NULL");
     if (n < 0 || n_grid < 4 || n_grid > 1024) return fail(PM_ERR_ARG, "bad n or n_grid");
@@ -110,7 +117,8 @@ int pm_workspace_layout(int64_t n, int32_t n_grid, pm_ws_layout *out) {
     const pm::Layout L = pm::make_layout(n, n_grid);
     out->ctrl = L.ctrl; out->keys_a = L.keys_a; out->keys_b = L.keys_b; out->vals_a = L.vals_a;
     out->vals_b = L.vals_b; out->hist = L.hist; out->block_mask = L.block_mask; out->block_list = L.block_list;
-    out->g_mom = L.g_mom; out->g_dmg = L.g_dmg; out->g_vel = L.g_vel; out->g_gd = L.g_gd; out->total = L.total;
+    out->g_mom = L.g_mom; out->g_dmg = L.g_dmg; out->g_vel = L.g_vel; out->g_gd = L.g_gd;
+    out->payload = L.payload; out->inv_perm = L.inv_perm; out->total = L.total;
     out->sort_passes = L.passes;
     out->n_tiles = L.n_tiles;
     return PM_OK;
@@ -144,7 +152,7 @@ int pm_bin(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     const pm::Parts parts = pm::make_parts(P);
     cudaStream_t s = (cudaStream_t)stream;
     pm::launch_keys(w, parts, prm->n_grid, (float)prm->inv_dx, s);
-    pm::launch_sort(w, P->n, s);
+    pm::launch_sort(w, P->n, s, w.inv_perm);
     return cuda_check("pm_bin");
 }
 
@@ -154,6 +162,7 @@ int pm_p2g(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
     pm::launch_p2g(*prm, pm::make_parts(P), w, (cudaStream_t)stream);
+    pm::launch_compact(w, (cudaStream_t)stream);
     return cuda_check("pm_p2g");
 }
 
@@ -189,8 +198,9 @@ static int substep_common(const pm_params *prm, const pm_particles *P, void *ws,
         pm::launch_set_clock_dev(*prm, w, dev_clocks, row, s);
     if (P->n > 0) {
         pm::launch_keys(w, parts, prm->n_grid, (float)prm->inv_dx, s);
-        pm::launch_sort(w, P->n, s);
+        pm::launch_sort(w, P->n, s, w.inv_perm);
         pm::launch_p2g(*prm, parts, w, s);
+        pm::launch_compact(w, s);
         pm::launch_grid(*prm, w, s);
         pm::launch_g2p(*prm, parts, w, s);
     }

@@ -51,7 +51,7 @@ __host__ __device__ inline int blocked_key_bits(int ng) {
 
 struct Layout {
     size_t ctrl, keys_a, keys_b, vals_a, vals_b, hist, block_mask, block_list;
-    size_t g_mom, g_dmg, g_vel, g_gd, total;
+    size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, total;
     int passes, n_tiles, nbs;
     long long n_blocks, n_nodes;
 };
@@ -82,6 +82,8 @@ __host__ __device__ inline Layout make_layout(long long n, int ng) {
     L.g_dmg = o;      o = align_up(o + 8 * (size_t)L.n_nodes, A);
     L.g_vel = o;      o = align_up(o + 16 * (size_t)L.n_nodes, A);
     L.g_gd = o;       o = align_up(o + 4 * (size_t)L.n_nodes, A);
+    L.payload = o;    o = align_up(o + 80 * nn, A);
+    L.inv_perm = o;   o = align_up(o + 4 * nn, A);
     L.total = o;
     return L;
 }
@@ -99,8 +101,10 @@ struct WS {
     float2 *g_dmg;      // {sum w d, sum w}, zero between substeps
     float4 *g_vel;      // {v.x, v.y, v.z, unused}
     float *g_gd;        // normalised damage field
+    float4 *payload;    // P2G payload, 5 float4 per particle in sorted order
     const unsigned *sorted_keys;
     const int *perm;
+    int *inv_perm;      // particle -> sorted position, written by the last radix pass
     int passes, n_tiles, nbs;
     long long n_blocks;
 };
@@ -121,6 +125,7 @@ inline WS make_ws(void *base, const Layout &L) {
     w.g_dmg = (float2 *)(b + L.g_dmg);
     w.g_vel = (float4 *)(b + L.g_vel);
     w.g_gd = (float *)(b + L.g_gd);
+    w.payload = (float4 *)(b + L.payload);
     w.passes = L.passes;
     w.n_tiles = L.n_tiles;
     w.nbs = L.nbs;
@@ -128,6 +133,7 @@ inline WS make_ws(void *base, const Layout &L) {
     // pass 0 reads keys_a and writes keys_b; the result of an odd pass count is in *_b
     w.sorted_keys = (L.passes & 1) ? w.keys_b : w.keys_a;
     w.perm = (L.passes & 1) ? w.vals_b : w.vals_a;
+    w.inv_perm = (int *)(b + L.inv_perm);
     return w;
 }
 
@@ -263,18 +269,32 @@ __device__ __forceinline__ float nan_to_num(float a) {
 }
 
 // One Jacobi rotation on pair (p,q) with the third index r, for a symmetric
-// matrix stored as app/aqq/apq/apr/aqr (anisompm.py:72-91).
+// matrix stored as app/aqq/apq/apr/aqr (anisompm.py:72-91).  The reference's
+// tangent t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = (aqq-app)/(2apq),
+// is evaluated as t = sign(zeta) |b| / (|a| + sqrt(a^2 + b^2)) with
+// (a, b) = (aqq - app, 2 apq) / max(|aqq - app|, |2 apq|): the same value
+// without its two divisions and square root, and without overflow for any
+// finite input (the reference's zeta^2 overflows to t = 0 only where t is
+// below 3e-20 anyway); the normalisation is an exact power of two taken from
+// the exponent bits.  The skip rule |apq| <= 1e-30 and sign(0) = +1 are the
+// reference's.  Three MUFU operations (rsqrt, rcp, rsqrt) per rotation.
 #define PM_JACOBI_ROT(APP, AQQ, APQ, APR, AQR, P, Q)                                  \
     {                                                                                 \
         const float app = APP, aqq = AQQ, apq = APQ, apr = APR, aqr = AQR;            \
-        float t = 0.0f;                                                               \
+        float c = 1.0f, s = 0.0f;                                                     \
         if (fabsf(apq) > 1e-30f) {                                                    \
-            const float z = (aqq - app) / (2.0f * apq);                               \
-            const float sgn = (z >= 0.0f) ? 1.0f : -1.0f;                             \
-            t = sgn / (fabsf(z) + sqrtf(1.0f + z * z));                               \
+            const float dd = aqq - app, bb = 2.0f * apq;                              \
+            const float mx = fmaxf(fabsf(dd), fabsf(bb));                             \
+            const unsigned ex_ = min((__float_as_uint(mx) >> 23) & 0xffu, 253u);      \
+            const float im = __uint_as_float((254u - ex_) << 23); /* 2^(127-ex_) */ \
+            const float a_ = dd * im, b_ = bb * im;                                   \
+            const float h2 = fmaf(a_, a_, b_ * b_);                                   \
+            const float hh = h2 * rsqrtf(h2);                                         \
+            const float sg = (dd == 0.0f || ((dd > 0.0f) == (apq > 0.0f))) ? 1.0f : -1.0f; \
+            const float t = sg * __fdividef(fabsf(b_), fabsf(a_) + hh);               \
+            c = rsqrtf(fmaf(t, t, 1.0f));                                             \
+            s = c * t;                                                                \
         }                                                                             \
-        const float c = 1.0f / sqrtf(1.0f + t * t);                                   \
-        const float s = c * t;                                                        \
         APP = c * c * app - 2.0f * s * c * apq + s * s * aqq;                         \
         AQQ = s * s * app + 2.0f * s * c * apq + c * c * aqq;                         \
         APQ = 0.0f;                                                                   \
@@ -302,6 +322,18 @@ __device__ __forceinline__ void sym_eig3(const float *Ain, float ev[3], float V[
     for (int k = 0; k < 9; ++k) V[k] = (k % 4 == 0) ? 1.0f : 0.0f;
 #pragma unroll
     for (int sw = 0; sw < SWEEPS; ++sw) {
+        // Once every lane's off-diagonal is below 1e-10 of its diagonal, the
+        // remaining sweeps of the reference change nothing at float32
+        // precision: a rotation with |t| ~ |apq|/gap <= 1e-10 leaves c = 1 and
+        // moves entries by less than half an ulp, and where eigenvalues lie
+        // closer than the off-diagonals it only turns the eigenvector pair
+        // inside their (numerically) degenerate plane, which leaves R, S and
+        // sigma+ unchanged.  The warp then stops early.
+        if (sw >= 1) {
+            const float off = fabsf(a01) + fabsf(a02) + fabsf(a12);
+            const float dia = fabsf(a00) + fabsf(a11) + fabsf(a22);
+            if (__all_sync(__activemask(), off <= 1e-10f * dia)) break;
+        }
         PM_JACOBI_ROT(a00, a11, a01, a02, a12, 0, 1)
         PM_JACOBI_ROT(a00, a22, a02, a01, a12, 0, 2)
         PM_JACOBI_ROT(a11, a22, a12, a01, a02, 1, 2)

@@ -137,19 +137,29 @@ void launch_grid(const pm_params &prm, const WS &w, cudaStream_t s) {
 }
 
 // --------------------------------------------------------------------- G2P
-// One thread per particle in sorted order: quadratic gather of grid velocity
-// (APIC v and C), cubic gather of the damage Laplacian at the start-of-step
+// One CTA per 256 particles in particle order (coalesced state reads and
+// writes; inputs built from lattices or meshes are spatially coherent in that
+// order).  The CTA first stages its grid footprint in shared memory:
+// velocities of the quadratic nodes [lo, hi+2] and the damage field of the
+// cubic nodes [lo-1, hi+3] of its base cells' bounding box [lo, hi]
+// (coalesced along z).  Then one thread per
+// particle gathers from shared memory: quadratic gather of grid velocity (APIC
+// v and C), cubic gather of the damage Laplacian at the start-of-step
 // position, then x += dt v, F <- (I + dt C) F, x clamped to [2dx, lim-2dx]
-// (anisompm.py:749-760, 781-803).
-__global__ void __launch_bounds__(256) k_g2p(const pm_params prm, const Parts P, const WS w) {
-    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n) return;
-    const long long p = w.perm[s];
+// (anisompm.py:749-760, 781-803).  A footprint larger than the staging
+// buffers (incoherent particle order), or a particle whose stencil needs the
+// reference's edge clamping, gathers from global memory instead.
+constexpr int kG2PThreads = 256;
+constexpr int kGTQ = 1200;   // staged quadratic nodes (float4)
+constexpr int kGTC = 2400;   // staged cubic nodes (float)
+
+template <bool TILE>
+__device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &P, const WS &w, long long p,
+                                             const float xp[3], const float F[9], const int lo[3], const int qd[3],
+                                             const int cd[3], const float4 *sq, const float *sc) {
     const long long ps = P.ps;
     const int ng = prm.n_grid;
     const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx, dt = (float)prm.dt;
-    const float xp[3] = {P.x[p], P.x[ps + p], P.x[2 * ps + p]};
-
     float nv[3] = {0.0f, 0.0f, 0.0f}, nC[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) nC[k] = 0.0f;
@@ -160,9 +170,15 @@ __global__ void __launch_bounds__(256) k_g2p(const pm_params prm, const Parts P,
         float DX[3], DY[3], DZ[3];
 #pragma unroll
         for (int o = 0; o < 3; ++o) {
-            NX[o] = clampi(q.b[0] + o, 0, ng - 1) * ng * ng;
-            NY[o] = clampi(q.b[1] + o, 0, ng - 1) * ng;
-            NZ[o] = clampi(q.b[2] + o, 0, ng - 1);
+            if (TILE) {
+                NX[o] = (q.b[0] + o - lo[0]) * qd[1] * qd[2];
+                NY[o] = (q.b[1] + o - lo[1]) * qd[2];
+                NZ[o] = q.b[2] + o - lo[2];
+            } else {
+                NX[o] = clampi(q.b[0] + o, 0, ng - 1) * ng * ng;
+                NY[o] = clampi(q.b[1] + o, 0, ng - 1) * ng;
+                NZ[o] = clampi(q.b[2] + o, 0, ng - 1);
+            }
             DX[o] = ((float)o - q.fx[0]) * dx;
             DY[o] = ((float)o - q.fx[1]) * dx;
             DZ[o] = ((float)o - q.fx[2]) * dx;
@@ -175,14 +191,16 @@ __global__ void __launch_bounds__(256) k_g2p(const pm_params prm, const Parts P,
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
                     const float wk = wxy * q.w[oz][2];
-                    const float4 g = __ldg(&w.g_vel[NX[ox] + NY[oy] + NZ[oz]]);
-                    nv[0] += wk * g.x; nv[1] += wk * g.y; nv[2] += wk * g.z;
+                    const int node = NX[ox] + NY[oy] + NZ[oz];
+                    const float4 g = TILE ? sq[node] : __ldg(&w.g_vel[node]);
+                    const float u0 = wk * g.x, u1 = wk * g.y, u2 = wk * g.z;
+                    nv[0] += u0; nv[1] += u1; nv[2] += u2;
                     const float dp[3] = {DX[ox], DY[oy], DZ[oz]};
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
-                        nC[j] += wk * (g.x * dp[j]);
-                        nC[3 + j] += wk * (g.y * dp[j]);
-                        nC[6 + j] += wk * (g.z * dp[j]);
+                        nC[j] += u0 * dp[j];
+                        nC[3 + j] += u1 * dp[j];
+                        nC[6 + j] += u2 * dp[j];
                     }
                 }
             }
@@ -197,22 +215,30 @@ __global__ void __launch_bounds__(256) k_g2p(const pm_params prm, const Parts P,
         int NX[4], NY[4], NZ[4];
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
-            NX[o] = clampi(c.b[0] + o, 0, ng - 1) * ng * ng;
-            NY[o] = clampi(c.b[1] + o, 0, ng - 1) * ng;
-            NZ[o] = clampi(c.b[2] + o, 0, ng - 1);
+            if (TILE) {
+                NX[o] = (c.b[0] + o - lo[0] + 1) * cd[1] * cd[2];
+                NY[o] = (c.b[1] + o - lo[1] + 1) * cd[2];
+                NZ[o] = c.b[2] + o - lo[2] + 1;
+            } else {
+                NX[o] = clampi(c.b[0] + o, 0, ng - 1) * ng * ng;
+                NY[o] = clampi(c.b[1] + o, 0, ng - 1) * ng;
+                NZ[o] = clampi(c.b[2] + o, 0, ng - 1);
+            }
         }
-        const float lfac = (float)(prm.inv_dx * prm.inv_dx);
+        // (w''x wy wz + wx w''y wz + wx wy w''z) = (w''x wy + wx w''y) wz + (wx wy) w''z
 #pragma unroll
         for (int ox = 0; ox < 4; ++ox)
 #pragma unroll
             for (int oy = 0; oy < 4; ++oy) {
-                const float a = c.w2[ox][0] * c.w[oy][1], b = c.w[ox][0] * c.w2[oy][1], e = c.w[ox][0] * c.w[oy][1];
+                const float ab = c.w2[ox][0] * c.w[oy][1] + c.w[ox][0] * c.w2[oy][1];
+                const float e = c.w[ox][0] * c.w[oy][1];
 #pragma unroll
                 for (int oz = 0; oz < 4; ++oz) {
-                    const float lw = lfac * (a * c.w[oz][2] + b * c.w[oz][2] + e * c.w2[oz][2]);
-                    lap += lw * __ldg(&w.g_gd[NX[ox] + NY[oy] + NZ[oz]]);
+                    const int node = NX[ox] + NY[oy] + NZ[oz];
+                    lap += (ab * c.w[oz][2] + e * c.w2[oz][2]) * (TILE ? sc[node] : __ldg(&w.g_gd[node]));
                 }
             }
+        lap *= (float)(prm.inv_dx * prm.inv_dx);
     }
     // advection, F update, domain clamp (793-802)
     const float pad = (float)(2.0 * prm.dx), hi = (float)(prm.grid_lim - 2.0 * prm.dx);
@@ -223,20 +249,16 @@ __global__ void __launch_bounds__(256) k_g2p(const pm_params prm, const Parts P,
         t = t < pad ? pad : t;
         xn[a] = t > hi ? hi : t;
     }
-    float F[9], Fn[9], A[9];
+    float Fn[9], A[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        F[k] = P.F[k * ps + p];
-        A[k] = ((k % 4 == 0) ? 1.0f : 0.0f) + dt * nC[k];
-    }
+    for (int k = 0; k < 9; ++k) A[k] = ((k % 4 == 0) ? 1.0f : 0.0f) + dt * nC[k];
     mm3(A, F, Fn);
     bool finite = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a) finite = finite && isfinite(xn[a]);
 #pragma unroll
     for (int k = 0; k < 9; ++k) finite = finite && isfinite(Fn[k]);
-    const unsigned bad = __ballot_sync(__activemask(), !finite);
-    if (bad && (threadIdx.x & 31) == __ffs(bad) - 1) atomicAdd(&w.ctrl->nonfinite, (unsigned)__popc(bad));
+    if (!finite) atomicAdd(&w.ctrl->nonfinite, 1u);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         P.x[a * ps + p] = xn[a];
@@ -250,10 +272,79 @@ __global__ void __launch_bounds__(256) k_g2p(const pm_params prm, const Parts P,
     P.lap[p] = lap;
 }
 
+__global__ void __launch_bounds__(kG2PThreads, 3) k_g2p(const pm_params prm, const Parts P, const WS w) {
+    __shared__ float4 sq[kGTQ];
+    __shared__ float sc[kGTC];
+    __shared__ int s_box[6];
+    const int tid = threadIdx.x;
+    // particle order: state reads and writes are coalesced
+    const long long p = (long long)blockIdx.x * kG2PThreads + tid;
+    const bool valid = p < P.n;
+    const int ng = prm.n_grid;
+    const long long ps = P.ps;
+    const float inv_dx = (float)prm.inv_dx;
+    float xp[3] = {0.0f, 0.0f, 0.0f}, F[9];
+    int qb[3] = {0, 0, 0};
+    bool reg = valid;
+    if (valid) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) xp[a] = P.x[a * ps + p];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) F[k] = P.F[k * ps + p];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float fb = floorf(__fsub_rn(__fmul_rn(xp[a], inv_dx), 0.5f));
+            reg = reg && (fb >= 1.0f) && (fb <= (float)(ng - 4));
+            qb[a] = reg ? (int)fb : 0;
+        }
+    }
+    // bounding box of the regular particles' base cells
+    int cl[3], ch[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        cl[a] = reg ? qb[a] : 0x7fffffff;
+        ch[a] = reg ? qb[a] : -0x7fffffff;
+    }
+    if (tid < 6) s_box[tid] = tid < 3 ? 0x7fffffff : -0x7fffffff;
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int mn = __reduce_min_sync(0xffffffffu, cl[a]), mx = __reduce_max_sync(0xffffffffu, ch[a]);
+        if ((tid & 31) == 0) {
+            atomicMin(&s_box[a], mn);
+            atomicMax(&s_box[3 + a], mx);
+        }
+    }
+    __syncthreads();
+    const int lo[3] = {s_box[0], s_box[1], s_box[2]};
+    const bool any = s_box[3] >= lo[0];
+    const int qd[3] = {s_box[3] - lo[0] + 3, s_box[4] - lo[1] + 3, s_box[5] - lo[2] + 3};
+    const int cd[3] = {qd[0] + 2, qd[1] + 2, qd[2] + 2};
+    const long long qn = any ? (long long)qd[0] * qd[1] * qd[2] : 0, cn = any ? (long long)cd[0] * cd[1] * cd[2] : 0;
+    const bool tile = any && qn <= kGTQ && cn <= kGTC;
+    if (tile) {   // regular nodes lie inside the grid, so no bounds test is needed
+        for (int i = tid; i < qn; i += kG2PThreads) {
+            const int gx = lo[0] + i / (qd[1] * qd[2]), gy = lo[1] + (i / qd[2]) % qd[1], gz = lo[2] + i % qd[2];
+            sq[i] = w.g_vel[((long long)gx * ng + gy) * ng + gz];
+        }
+        for (int i = tid; i < cn; i += kG2PThreads) {
+            const int gx = lo[0] - 1 + i / (cd[1] * cd[2]), gy = lo[1] - 1 + (i / cd[2]) % cd[1],
+                      gz = lo[2] - 1 + i % cd[2];
+            sc[i] = w.g_gd[((long long)gx * ng + gy) * ng + gz];
+        }
+    }
+    __syncthreads();
+    if (!valid) return;
+    if (reg && tile)
+        g2p_particle<true>(prm, P, w, p, xp, F, lo, qd, cd, sq, sc);
+    else
+        g2p_particle<false>(prm, P, w, p, xp, F, lo, qd, cd, sq, sc);
+}
+
 void launch_g2p(const pm_params &prm, const Parts &P, const WS &w, cudaStream_t s) {
-    const long long blocks = (P.n + 255) / 256;
+    const long long blocks = (P.n + kG2PThreads - 1) / kG2PThreads;
     if (blocks <= 0) return;
-    k_g2p<<<(unsigned)blocks, 256, 0, s>>>(prm, P, w);
+    k_g2p<<<(unsigned)blocks, kG2PThreads, 0, s>>>(prm, P, w);
 }
 
 // ---------------------------------------------------------------- sym_eig

@@ -1,18 +1,22 @@
-// Fused constitutive update + P2G.
+// Fused constitutive update + P2G, cell-aggregated.
 //
 // One CTA takes 2048 consecutive particles of the block-sorted order and splits
-// them into segments that share one 8^3-cell sort block.  For each segment a
-// 12^3-node shared-memory tile (the block's stencil footprint) is zeroed, then
-// in sub-chunks of 256:
-//   phase 1 (one particle per thread): particle BC, polar decomposition by a
-//   Jacobi eigensolve of F^T F, fixed-corotated Kirchhoff stress, anisotropic
-//   phase-field damage (second Jacobi eigensolve, of the Cauchy stress),
-//   degradation and the APIC affine term; the P2G payload goes to shared
-//   memory;
-//   phase 2: lane l of warp w scatters element 8*l + w of the sub-chunk, so
-//   the lanes of a warp hold particles ~8 apart in cell order (mostly in
-//   different cells) and their shared-memory atomics rarely hit one address.
-// The tile is then flushed with one vector atomic per touched node.
+// them into segments that share one 8^3-cell sort block.  Each segment owns two
+// shared-memory tiles: the quadratic momentum tile (nodes [8b, 8b+10)^3,
+// {mv, m}) and the cubic damage tile (nodes [8b-1, 8b+11)^3, {sum w d, sum w}).
+// Sub-chunks of 256 particles then go through
+//   phase 1, one particle per thread: particle BC, polar decomposition (Jacobi
+//     eigensolve of F^T F), fixed-corotated Kirchhoff stress, anisotropic
+//     phase-field damage (Jacobi eigensolve of the Cauchy stress), degradation
+//     and the APIC affine term; the P2G payload goes to shared memory;
+//   phase 2, one work item per (cell, x-slab): all particles of a cell share
+//     their quadratic base, so an item sums the cell's contributions to 9
+//     quadratic nodes (3 slabs) or 25 cubic nodes (5 slabs; a cell's cubic
+//     stencils span 5^3 nodes) in registers and adds each node once.  Lanes hold
+//     distinct cells, so the float shared atomics rarely meet on one address.
+// The tiles are flushed with one vector atomic per touched node.  Particles
+// whose stencil needs the reference's edge clamping (base cell outside
+// [1, n_grid-4]) scatter directly to global memory instead.
 //
 // Reference: anisompm.py:601-724 (constitutive, damage, P2G) and 768-776
 // (cubic damage scatter).
@@ -201,17 +205,70 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
     }
 }
 
-// Static shared tile of one sort block: nodes [8*blk - 1, 8*blk + 11) per axis
-// hold every quadratic [qb, qb+2] and cubic [qb-1, qb+3] stencil node of the
-// block's particles (clamped coordinates included).
-constexpr int kTE = kSortBlock + 4;            // 12
-constexpr int kTileNodes = kTE * kTE * kTE;    // 1728
+// One thread per particle in particle order: particle BC, constitutive update,
+// damage update, degradation and the APIC affine term (anisompm.py:601-713);
+// the P2G payload goes to w.payload[s] (5 float4, coalesced):
+//   {fx | x, m} {m v, d} {affine 0..3} {affine 4..7} {affine 8, regular, 0, 0}
+// with fx = X - floor(X - 0.5) per axis for particles whose stencil needs no
+// clamping (regular, base cell in [1, n_grid-4]) and the position x otherwise.
+__global__ void __launch_bounds__(256, 3) k_stress(const pm_params prm, const Parts P, const WS w) {
+    // particle order: the state reads and writes are coalesced; the payload
+    // goes to the particle's sorted position
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.n) return;
+    const long long s = w.inv_perm[p];
+    const long long ps = P.ps;
+    const int ng = prm.n_grid;
+    const float inv_dx = (float)prm.inv_dx;
+    const Ctrl *ctrl = w.ctrl;
+    const bool do_damage = ctrl->any_allow != 0 && (ctrl->step % (long long)prm.damage_every) == 0;
+    float tau[9];
+    constitutive(prm, P, p, do_damage, tau);
+    float v[3] = {P.v[p], P.v[ps + p], P.v[2 * ps + p]};
+    if (P.grip_tag) {                                                // particle BCs (601-602)
+        const int g = P.grip_tag[p];
+        if (g >= 0 && g < prm.n_grips) {
+            const double f = prm.grips[g].ramp > 0.0 ? fmin(ctrl->time / prm.grips[g].ramp, 1.0) : 1.0;
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) v[ax] = (float)(prm.grips[g].vel[ax] * f);
+        }
+    }
+    const float m = P.mass[p];
+    // stress_coeff = -dt*vol0*4*inv_dx*inv_dx; affine = coeff*tau + m*C (711-713)
+    const float coeff =
+        __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), P.vol0[p]), 4.0f), inv_dx), inv_dx);
+    float aff[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) aff[k] = coeff * tau[k] + m * P.C[k * ps + p];
+    float xp[3], fx[3];
+    bool reg = true;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        xp[ax] = P.x[ax * ps + p];
+        const float X = __fmul_rn(xp[ax], inv_dx);
+        const float fb = floorf(__fsub_rn(X, 0.5f));
+        reg = reg && (fb >= 1.0f) && (fb <= (float)(ng - 4));
+        fx[ax] = __fsub_rn(X, fb);                                   // in [0.5, 1.5)
+    }
+    float4 *dst = w.payload + 5 * s;
+    dst[0] = reg ? make_float4(fx[0], fx[1], fx[2], m) : make_float4(xp[0], xp[1], xp[2], m);
+    dst[1] = make_float4(m * v[0], m * v[1], m * v[2], P.d[p]);
+    dst[2] = make_float4(aff[0], aff[1], aff[2], aff[3]);
+    dst[3] = make_float4(aff[4], aff[5], aff[6], aff[7]);
+    dst[4] = make_float4(aff[8], reg ? 1.0f : 0.0f, 0.0f, 0.0f);
+}
 
-// Scatter one particle's quadratic momentum (27 nodes) and cubic damage (64
-// nodes) into the shared tile whose node origin is org.
-__device__ __forceinline__ void scatter_particle(const float xp[3], const float mv[3], const float aff[9], float m,
-                                                 float d, float inv_dx, float dx, int ng, const int org[3],
-                                                 float *__restrict__ tile) {
+// Scatter one particle straight into the global grid with the reference's
+// clamped node indices (anisompm.py:716-724, 771-776): the path for particles
+// whose stencil leaves the grid.
+__device__ __forceinline__ void mark_node_block(unsigned char *mask, int nbs, int x, int y, int z) {
+    unsigned char *m = &mask[((long long)(x >> 2) * nbs + (y >> 2)) * nbs + (z >> 2)];
+    if (*m == 0) *m = 1;
+}
+
+__device__ __noinline__ void scatter_particle_global(const float xp[3], const float mv[3], const float aff[9],
+                                                     float m, float d, float inv_dx, float dx, int ng, float4 *g_mom,
+                                                     float2 *g_dmg, unsigned char *mask, int nbs) {
     {
         Quad q;
         quad_weights(xp, inv_dx, ng, q);
@@ -219,10 +276,10 @@ __device__ __forceinline__ void scatter_particle(const float xp[3], const float 
         float DX[3], DY[3], DZ[3];
 #pragma unroll
         for (int o = 0; o < 3; ++o) {
-            NX[o] = (clampi(q.b[0] + o, 0, ng - 1) - org[0]) * (kTE * kTE);
-            NY[o] = (clampi(q.b[1] + o, 0, ng - 1) - org[1]) * kTE;
-            NZ[o] = clampi(q.b[2] + o, 0, ng - 1) - org[2];
-            DX[o] = ((float)o - q.fx[0]) * dx;                       // dpos (718)
+            NX[o] = clampi(q.b[0] + o, 0, ng - 1) * ng * ng;
+            NY[o] = clampi(q.b[1] + o, 0, ng - 1) * ng;
+            NZ[o] = clampi(q.b[2] + o, 0, ng - 1);
+            DX[o] = ((float)o - q.fx[0]) * dx;
             DY[o] = ((float)o - q.fx[1]) * dx;
             DZ[o] = ((float)o - q.fx[2]) * dx;
         }
@@ -234,14 +291,12 @@ __device__ __forceinline__ void scatter_particle(const float xp[3], const float 
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
                     const float wk = wxy * q.w[oz][2];
-                    const int node = NX[ox] + NY[oy] + NZ[oz];
                     const float a0 = aff[0] * DX[ox] + aff[1] * DY[oy] + aff[2] * DZ[oz];
                     const float a1 = aff[3] * DX[ox] + aff[4] * DY[oy] + aff[5] * DZ[oz];
                     const float a2 = aff[6] * DX[ox] + aff[7] * DY[oy] + aff[8] * DZ[oz];
-                    atomicAdd(&tile[0 * kTileNodes + node], wk * (mv[0] + a0));
-                    atomicAdd(&tile[1 * kTileNodes + node], wk * (mv[1] + a1));
-                    atomicAdd(&tile[2 * kTileNodes + node], wk * (mv[2] + a2));
-                    atomicAdd(&tile[3 * kTileNodes + node], wk * m);
+                    atomicAdd(&g_mom[NX[ox] + NY[oy] + NZ[oz]],
+                              make_float4(wk * (mv[0] + a0), wk * (mv[1] + a1), wk * (mv[2] + a2), wk * m));
+                    mark_node_block(mask, nbs, NX[ox] / (ng * ng), NY[oy] / ng, NZ[oz]);
                 }
             }
     }
@@ -251,9 +306,9 @@ __device__ __forceinline__ void scatter_particle(const float xp[3], const float 
         int NX[4], NY[4], NZ[4];
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
-            NX[o] = (clampi(c.b[0] + o, 0, ng - 1) - org[0]) * (kTE * kTE);
-            NY[o] = (clampi(c.b[1] + o, 0, ng - 1) - org[1]) * kTE;
-            NZ[o] = clampi(c.b[2] + o, 0, ng - 1) - org[2];
+            NX[o] = clampi(c.b[0] + o, 0, ng - 1) * ng * ng;
+            NY[o] = clampi(c.b[1] + o, 0, ng - 1) * ng;
+            NZ[o] = clampi(c.b[2] + o, 0, ng - 1);
         }
 #pragma unroll
         for (int ox = 0; ox < 4; ++ox)
@@ -263,49 +318,53 @@ __device__ __forceinline__ void scatter_particle(const float xp[3], const float 
 #pragma unroll
                 for (int oz = 0; oz < 4; ++oz) {
                     const float wk = wxy * c.w[oz][2];
-                    const int node = NX[ox] + NY[oy] + NZ[oz];
-                    atomicAdd(&tile[4 * kTileNodes + node], wk * d);
-                    atomicAdd(&tile[5 * kTileNodes + node], wk);
+                    atomicAdd(&g_dmg[NX[ox] + NY[oy] + NZ[oz]], make_float2(wk * d, wk));
+                    mark_node_block(mask, nbs, NX[ox] / (ng * ng), NY[oy] / ng, NZ[oz]);
                 }
             }
     }
 }
 
-constexpr int kP2GRange = 2048;   // sorted particles per CTA
-constexpr size_t kP2GSmem = sizeof(float) * (6 * kTileNodes + kPay * kPayStride) +
-                            sizeof(unsigned) * kP2GRange + sizeof(int) * (kP2GRange + 2);
+constexpr int kQE = kSortBlock + 2;            // 10: quadratic tile edge, nodes [8b, 8b+10)
+constexpr int kCE = kSortBlock + 4;            // 12: cubic tile edge, nodes [8b-1, 8b+11)
+constexpr int kQN = kQE * kQE * kQE;           // 1000
+constexpr int kCN = kCE * kCE * kCE;           // 1728
+constexpr int kP2GMaxRange = 4096;             // sorted particles per CTA at most
+constexpr int kP2GDefaultRange = 512;
+constexpr int kSub = kP2GThreads;              // particles per sub-chunk
+constexpr int kCW = 15;                        // expanded cubic weights per particle (5 per axis)
+constexpr size_t kP2GSmem = sizeof(float) * (4 * kQN + 2 * kCN + (kPay + kCW) * kPayStride) + sizeof(int) * (kSub + 2) +
+                            kSub + sizeof(short) * (kP2GMaxRange + 2);
 
-// One CTA per kP2GRange sorted particles, split into segments of one sort
-// block each; a segment is accumulated in the block's tile and flushed.
-template <int STRIDE>
-__global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(const pm_params prm, const Parts P, const WS w) {
-    extern __shared__ float4 s_raw[];
-    float *s_tile = (float *)s_raw;                                   // [6][kTileNodes]
-    float (*s_pay)[kPayStride] = (float (*)[kPayStride])(s_tile + 6 * kTileNodes);
-    unsigned *s_blk = (unsigned *)(s_tile + 6 * kTileNodes + kPay * kPayStride);
-    int *s_seg = (int *)(s_blk + kP2GRange);                          // segment starts, then count
-    __shared__ int s_wcnt[kP2GThreads / 32];
+// Quadratic weights of one axis from fx (anisompm.py:549-556).
+__device__ __forceinline__ void qw(float f, float w[3]) {
+    const float t0 = 1.5f - f, t1 = f - 1.0f, t2 = f - 0.5f;
+    w[0] = 0.5f * (t0 * t0);
+    w[1] = 0.75f - t1 * t1;
+    w[2] = 0.5f * (t2 * t2);
+}
+// Cubic weights of one axis expanded onto the 5 nodes [qb-1, qb+3] of a cell:
+// with s = (fx >= 1) the particle's cubic base is qb - 1 + s and its fraction
+// f = fx - s (both exact), so node n takes weight w[n - s] (anisompm.py:575-583).
+__device__ __forceinline__ void cw5(float fx, float e[5]) {
+    const bool s1 = fx >= 1.0f;
+    const float f = s1 ? fx - 1.0f : fx;
+    const float one = 1.0f - f;
+    const float w0 = (1.0f / 6.0f) * (one * one * one);
+    const float w1 = (2.0f / 3.0f - f * f) + 0.5f * (f * f * f);
+    const float w2 = (2.0f / 3.0f - one * one) + 0.5f * (one * one * one);
+    const float w3 = (1.0f / 6.0f) * (f * f * f);
+    e[0] = s1 ? 0.0f : w0;
+    e[1] = s1 ? w0 : w1;
+    e[2] = s1 ? w1 : w2;
+    e[3] = s1 ? w2 : w3;
+    e[4] = s1 ? w3 : 0.0f;
+}
 
+// Ordered compaction of flagged positions [0, n) held PER per thread.
+template <int PER>
+__device__ __forceinline__ int compact_flags(int flags, int *out_short_or_int, bool as_short, int *s_wcnt) {
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const long long n = P.n;
-    const long long r0 = (long long)blockIdx.x * kP2GRange;
-    const int len = (int)min((long long)kP2GRange, n - r0);
-    const int ng = prm.n_grid;
-    const int nb = sort_blocks_per_axis(ng);
-    const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
-    const Ctrl *ctrl = w.ctrl;
-    const bool do_damage = ctrl->any_allow != 0 && (ctrl->step % (long long)prm.damage_every) == 0;
-
-    // ---- segment the range at sort-block boundaries (ordered compaction)
-    for (int i = tid; i < len; i += kP2GThreads) s_blk[i] = w.sorted_keys[r0 + i] >> kSortBlockBits;
-    __syncthreads();
-    constexpr int PER = kP2GRange / kP2GThreads;
-    int flags = 0;
-#pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const int i = tid * PER + k;
-        if (i < len && (i == 0 || s_blk[i] != s_blk[i - 1])) flags |= 1 << k;
-    }
     const int cnt = __popc(flags);
     int incl = cnt;
 #pragma unroll
@@ -315,99 +374,334 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(const pm_params prm, con
     }
     if (lane == 31) s_wcnt[wid] = incl;
     __syncthreads();
-    int pos = incl - cnt;
-    for (int w2 = 0; w2 < wid; ++w2) pos += s_wcnt[w2];
+    int pos = incl - cnt, total = 0;
+#pragma unroll
+    for (int w2 = 0; w2 < kP2GThreads / 32; ++w2) {
+        pos += (w2 < wid) ? s_wcnt[w2] : 0;
+        total += s_wcnt[w2];
+    }
 #pragma unroll
     for (int k = 0; k < PER; ++k)
-        if (flags & (1 << k)) s_seg[pos++] = tid * PER + k;
-    if (tid == kP2GThreads - 1) {
-        int total = 0;
-        for (int w2 = 0; w2 < kP2GThreads / 32; ++w2) total += s_wcnt[w2];
-        s_seg[kP2GRange + 1] = total;
-    }
+        if (flags & (1 << k)) {
+            if (as_short)
+                ((short *)out_short_or_int)[pos++] = (short)(tid * PER + k);
+            else
+                out_short_or_int[pos++] = tid * PER + k;
+        }
     __syncthreads();
-    const int nseg = s_seg[kP2GRange + 1];
+    return total;
+}
 
+__global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const pm_params prm, const WS w, long long n,
+                                                             int range) {
+    extern __shared__ float4 s_raw[];
+    float *qt = (float *)s_raw;                                        // [4][kQN]
+    float *ct = qt + 4 * kQN;                                          // [2][kCN]
+    float (*pay)[kPayStride] = (float (*)[kPayStride])(ct + 2 * kCN);  // [kPay][kPayStride]
+    float (*cwt)[kPayStride] = (float (*)[kPayStride])(pay[kPay]);    // [kCW][kPayStride]
+    int *runs = (int *)(cwt[kCW]);                                     // [kSub + 2]
+    unsigned char *regular = (unsigned char *)(runs + kSub + 2);       // [kSub]
+    short *seg = (short *)(regular + kSub);                            // [kP2GRange + 2]
+    __shared__ int s_wcnt[kP2GThreads / 32];
+    __shared__ unsigned char s_bmark[64];
+    __shared__ int s_cb[6];   // cell bounding box of the segment inside its block
+
+    const int tid = threadIdx.x;
+    const long long r0 = (long long)blockIdx.x * range;
+    const int len = (int)min((long long)range, n - r0);
+    const int ng = prm.n_grid;
+    const int nb = sort_blocks_per_axis(ng);
+    const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
+    const unsigned *keys = w.sorted_keys + r0;
+
+    // ---- segments: runs of one sort block in [0, len)
+    int nseg;
+    {
+        constexpr int PER = kP2GMaxRange / kP2GThreads;
+        int flags = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int i = tid * PER + k;
+            if (i < len && (i == 0 || (keys[i] >> kSortBlockBits) != (keys[i - 1] >> kSortBlockBits)))
+                flags |= 1 << k;
+        }
+        nseg = compact_flags<PER>(flags, (int *)seg, true, s_wcnt);
+    }
+
+    // tiles start zero; every flush clears what it visits, so they stay zero
+    for (int i = tid; i < 4 * kQN + 2 * kCN; i += kP2GThreads) qt[i] = 0.0f;   // qt and ct are contiguous
+    __syncthreads();
     for (int sg = 0; sg < nseg; ++sg) {
-        const int a = s_seg[sg];
-        const int b = (sg + 1 < nseg) ? s_seg[sg + 1] : len;
-        const unsigned blk = s_blk[a];
+        const int a = seg[sg];
+        const int b = (sg + 1 < nseg) ? seg[sg + 1] : len;
+        const unsigned blk = keys[a] >> kSortBlockBits;
         const int bz = (int)(blk % nb), by = (int)((blk / nb) % nb), bx = (int)(blk / ((unsigned)nb * nb));
-        const int org[3] = {bx * kSortBlock - 1, by * kSortBlock - 1, bz * kSortBlock - 1};
-        for (int i = tid; i < 6 * kTileNodes; i += kP2GThreads) s_tile[i] = 0.0f;
-
-        for (int sub = a; sub < b; sub += kP2GThreads) {
-            // phase 1: constitutive update of one particle per thread
-            const int cnt_sub = min(kP2GThreads, b - sub);
-            if (tid < cnt_sub) {
-                const long long p = w.perm[r0 + sub + tid];
-                const long long ps = P.ps;
-                float tau[9];
-                constitutive(prm, P, p, do_damage, tau);
-                float v[3] = {P.v[p], P.v[ps + p], P.v[2 * ps + p]};
-                if (P.grip_tag) {                                    // particle BCs (601-602)
-                    const int g = P.grip_tag[p];
-                    if (g >= 0 && g < prm.n_grips) {
-                        const double f = prm.grips[g].ramp > 0.0 ? fmin(ctrl->time / prm.grips[g].ramp, 1.0) : 1.0;
-#pragma unroll
-                        for (int ax = 0; ax < 3; ++ax) v[ax] = (float)(prm.grips[g].vel[ax] * f);
-                    }
-                }
-                const float m = P.mass[p];
-                // stress_coeff = -dt*vol0*4*inv_dx*inv_dx; affine = coeff*tau + m*C (711-713)
-                const float coeff = __fmul_rn(
-                    __fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), P.vol0[p]), 4.0f), inv_dx), inv_dx);
-                const int t = tid + (tid >> 5);
-#pragma unroll
-                for (int k = 0; k < 9; ++k) s_pay[6 + k][t] = coeff * tau[k] + m * P.C[k * ps + p];
+        const int org[3] = {bx * kSortBlock, by * kSortBlock, bz * kSortBlock};   // quadratic tile origin
+        {   // the segment's cell bounding box (inside the block): the flush visits only its footprint
+            int lo[3] = {7, 7, 7}, hi[3] = {0, 0, 0};
+            for (int i = a + tid; i < b; i += kP2GThreads) {
+                const unsigned k = keys[i];
+                const int c[3] = {(int)((k >> 6) & 7), (int)((k >> 3) & 7), (int)(k & 7)};
 #pragma unroll
                 for (int ax = 0; ax < 3; ++ax) {
-                    s_pay[ax][t] = P.x[ax * ps + p];
-                    s_pay[3 + ax][t] = m * v[ax];
+                    lo[ax] = min(lo[ax], c[ax]);
+                    hi[ax] = max(hi[ax], c[ax]);
                 }
-                s_pay[15][t] = m;
-                s_pay[16][t] = P.d[p];
             }
+            if (tid < 6) s_cb[tid] = tid < 3 ? 7 : 0;
             __syncthreads();
-            // phase 2: scatter; lane l of warp w takes element STRIDE*l + w
-            const int j = (STRIDE == 1) ? tid : (lane * STRIDE + wid);
-            if (j < cnt_sub) {
-                const int t = j + (j >> 5);
-                const float xp[3] = {s_pay[0][t], s_pay[1][t], s_pay[2][t]};
-                const float mv[3] = {s_pay[3][t], s_pay[4][t], s_pay[5][t]};
-                float aff[9];
 #pragma unroll
-                for (int k = 0; k < 9; ++k) aff[k] = s_pay[6 + k][t];
-                scatter_particle(xp, mv, aff, s_pay[15][t], s_pay[16][t], inv_dx, dx, ng, org, s_tile);
+            for (int ax = 0; ax < 3; ++ax) {
+                const int mn = __reduce_min_sync(0xffffffffu, lo[ax]), mx = __reduce_max_sync(0xffffffffu, hi[ax]);
+                if ((tid & 31) == 0) {
+                    atomicMin(&s_cb[ax], mn);
+                    atomicMax(&s_cb[3 + ax], mx);
+                }
             }
             __syncthreads();
         }
-        // flush the tile: one vector atomic per touched node
-        for (int i = tid; i < kTileNodes; i += kP2GThreads) {
-            const int tx = i / (kTE * kTE), ty = (i / kTE) % kTE, tz = i % kTE;
-            const int gx = org[0] + tx, gy = org[1] + ty, gz = org[2] + tz;
-            if (gx < 0 || gy < 0 || gz < 0 || gx >= ng || gy >= ng || gz >= ng) continue;
-            const float a0 = s_tile[i], a1 = s_tile[kTileNodes + i], a2 = s_tile[2 * kTileNodes + i],
-                        a3 = s_tile[3 * kTileNodes + i], a4 = s_tile[4 * kTileNodes + i],
-                        a5 = s_tile[5 * kTileNodes + i];
-            const long long node = ((long long)gx * ng + gy) * ng + gz;
-            if (a0 != 0.0f || a1 != 0.0f || a2 != 0.0f || a3 != 0.0f)
-                atomicAdd(&w.g_mom[node], make_float4(a0, a1, a2, a3));
-            if (a4 != 0.0f || a5 != 0.0f) atomicAdd(&w.g_dmg[node], make_float2(a4, a5));
+        const int cmin[3] = {s_cb[0], s_cb[1], s_cb[2]};
+        const int cext[3] = {s_cb[3] - s_cb[0] + 1, s_cb[4] - s_cb[1] + 1, s_cb[5] - s_cb[2] + 1};
+
+        for (int sub = a; sub < b; sub += kSub) {
+            const int cnt = min(kSub, b - sub);
+            // ---------------- phase 1: the sub-chunk's payload (written by k_stress in
+            // sorted order) into shared memory: coalesced float4 loads
+            if (tid < cnt) {
+                const float4 *src = w.payload + 5 * (r0 + sub + tid);
+                const float4 q0 = src[0], q1 = src[1], q2 = src[2], q3 = src[3], q4 = src[4];
+                const int t = tid + (tid >> 5);
+                pay[0][t] = q0.x; pay[1][t] = q0.y; pay[2][t] = q0.z; pay[15][t] = q0.w;
+                pay[3][t] = q1.x; pay[4][t] = q1.y; pay[5][t] = q1.z; pay[16][t] = q1.w;
+                pay[6][t] = q2.x; pay[7][t] = q2.y; pay[8][t] = q2.z; pay[9][t] = q2.w;
+                pay[10][t] = q3.x; pay[11][t] = q3.y; pay[12][t] = q3.z; pay[13][t] = q3.w;
+                pay[14][t] = q4.x;
+                regular[tid] = q4.y != 0.0f ? 1 : 0;
+                if (q4.y != 0.0f) {   // the cubic weights of the cell's 5 node layers, once per particle
+                    float e[5];
+                    cw5(q0.x, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cwt[k][t] = e[k];
+                    cw5(q0.y, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cwt[5 + k][t] = e[k];
+                    cw5(q0.z, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cwt[10 + k][t] = e[k];
+                }
+            }
+            // runs of equal cell key inside the sub-chunk
+            int nruns;
+            {
+                const int i = sub + tid;
+                const int flag = (tid < cnt && (tid == 0 || keys[i] != keys[i - 1])) ? 1 : 0;
+                nruns = compact_flags<1>(flag, runs, false, s_wcnt);   // also orders the payload writes
+                if (tid == 0) runs[nruns] = cnt;
+                __syncthreads();
+            }
+            // ---------------- phase 2a: particles that need clamped nodes
+            if (tid < cnt && !regular[tid]) {
+                const int t = tid + (tid >> 5);
+                const float xp[3] = {pay[0][t], pay[1][t], pay[2][t]};   // positions for these particles
+                const float mv[3] = {pay[3][t], pay[4][t], pay[5][t]};
+                float aff[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) aff[k] = pay[6 + k][t];
+                scatter_particle_global(xp, mv, aff, pay[15][t], pay[16][t], inv_dx, dx, ng, w.g_mom, w.g_dmg,
+                                        w.block_mask, w.nbs);
+            }
+            // ---------------- phase 2b: (cell, slab) items into the tiles
+            // items 0 .. 3*nruns-1 are quadratic x-slabs, then 5*nruns cubic x-slabs,
+            // so a warp mostly runs one kind
+            for (int it = tid; it < nruns * 8; it += kP2GThreads) {
+                const bool quad = it < 3 * nruns;
+                const int r = quad ? it / 3 : (it - 3 * nruns) / 5;
+                const int sl = quad ? it - 3 * r : 3 + (it - 3 * nruns - 5 * r);
+                const int ja = runs[r], jb = runs[r + 1];
+                const unsigned key = keys[sub + ja];
+                const int cq[3] = {(int)((key >> 6) & 7), (int)((key >> 3) & 7), (int)(key & 7)};  // cell in block
+                if (sl < 3) {
+                    const int ox = sl;
+                    float acc[3][3][4];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) acc[i][j][c] = 0.0f;
+                    for (int j = ja; j < jb; ++j) {
+                        if (!regular[j]) continue;
+                        const int t = j + (j >> 5);
+                        const float fx0 = pay[0][t], fx1 = pay[1][t], fx2 = pay[2][t];
+                        float wx[3], wy[3], wz[3];
+                        qw(fx0, wx); qw(fx1, wy); qw(fx2, wz);
+                        const float dxo = ((float)ox - fx0) * dx;
+                        const float m = pay[15][t];
+                        float base[3], ay[3], az[3];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            base[c] = pay[3 + c][t] + pay[6 + 3 * c][t] * dxo;
+                            ay[c] = pay[7 + 3 * c][t];
+                            az[c] = pay[8 + 3 * c][t];
+                        }
+                        const float wxs = ox == 0 ? wx[0] : (ox == 1 ? wx[1] : wx[2]);
+                        float bz[3][3];   // mv + aff (dpos_x, ., dpos_z) for each oz
+#pragma unroll
+                        for (int oz = 0; oz < 3; ++oz) {
+                            const float dz = ((float)oz - fx2) * dx;
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) bz[oz][c] = base[c] + az[c] * dz;
+                        }
+#pragma unroll
+                        for (int oy = 0; oy < 3; ++oy) {
+                            const float dy = ((float)oy - fx1) * dx;
+                            const float wxy = wxs * wy[oy];
+                            const float ady[3] = {ay[0] * dy, ay[1] * dy, ay[2] * dy};
+#pragma unroll
+                            for (int oz = 0; oz < 3; ++oz) {
+                                const float wk = wxy * wz[oz];
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) acc[oy][oz][c] += wk * (bz[oz][c] + ady[c]);
+                                acc[oy][oz][3] += wk * m;
+                            }
+                        }
+                    }
+                    const int nx = cq[0] + ox;
+#pragma unroll
+                    for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                        for (int oz = 0; oz < 3; ++oz) {
+                            const int idx = (nx * kQE + cq[1] + oy) * kQE + cq[2] + oz;
+#pragma unroll
+                            for (int c = 0; c < 4; ++c)
+                                if (acc[oy][oz][c] != 0.0f) atomicAdd(&qt[c * kQN + idx], acc[oy][oz][c]);
+                        }
+                } else {
+                    const int nxs = sl - 3;
+                    float adc[5][5], adw[5][5];
+#pragma unroll
+                    for (int i = 0; i < 5; ++i)
+#pragma unroll
+                        for (int j = 0; j < 5; ++j) adc[i][j] = adw[i][j] = 0.0f;
+                    for (int j = ja; j < jb; ++j) {
+                        if (!regular[j]) continue;
+                        const int t = j + (j >> 5);
+                        const float wxs = cwt[nxs][t];
+                        float ey[5], ez[5];
+#pragma unroll
+                        for (int k = 0; k < 5; ++k) {
+                            ey[k] = cwt[5 + k][t];
+                            ez[k] = cwt[10 + k][t];
+                        }
+                        const float d = pay[16][t];
+#pragma unroll
+                        for (int ny = 0; ny < 5; ++ny) {
+                            const float wxy = wxs * ey[ny];
+#pragma unroll
+                            for (int nz = 0; nz < 5; ++nz) {
+                                const float wk = wxy * ez[nz];
+                                adc[ny][nz] += wk * d;
+                                adw[ny][nz] += wk;
+                            }
+                        }
+                    }
+                    // cubic tile origin is 8b - 1, the cell's 5 nodes start at qb - 1
+                    const int nx = cq[0] + nxs;
+#pragma unroll
+                    for (int ny = 0; ny < 5; ++ny)
+#pragma unroll
+                        for (int nz = 0; nz < 5; ++nz) {
+                            const int idx = (nx * kCE + cq[1] + ny) * kCE + cq[2] + nz;
+                            if (adc[ny][nz] != 0.0f) atomicAdd(&ct[idx], adc[ny][nz]);
+                            if (adw[ny][nz] != 0.0f) atomicAdd(&ct[kCN + idx], adw[ny][nz]);
+                        }
+                }
+            }
+            __syncthreads();
+        }
+        // ---------------- flush: one vector atomic per touched node, and mark
+        // the touched 4^3 node blocks (tile nodes span blocks [2b-1, 2b+2] per
+        // axis; s_bmark is indexed from 2b-1)
+        if (tid < 64) s_bmark[tid] = 0;
+        __syncthreads();
+        {   // quadratic footprint: local nodes [cmin, cmin + cext + 2) per axis
+            const int ex = cext[0] + 2, ey = cext[1] + 2, ez = cext[2] + 2;
+            for (int i = tid; i < ex * ey * ez; i += kP2GThreads) {
+                const int tx = cmin[0] + i / (ey * ez), ty = cmin[1] + (i / ez) % ey, tz = cmin[2] + i % ez;
+                const int li = (tx * kQE + ty) * kQE + tz;
+                const float a0 = qt[li], a1 = qt[kQN + li], a2 = qt[2 * kQN + li], a3 = qt[3 * kQN + li];
+                if (a0 != 0.0f || a1 != 0.0f || a2 != 0.0f || a3 != 0.0f) {
+                    qt[li] = 0.0f; qt[kQN + li] = 0.0f; qt[2 * kQN + li] = 0.0f; qt[3 * kQN + li] = 0.0f;
+                    const int gx = org[0] + tx, gy = org[1] + ty, gz = org[2] + tz;   // in the grid: regular nodes only
+                    atomicAdd(&w.g_mom[((long long)gx * ng + gy) * ng + gz], make_float4(a0, a1, a2, a3));
+                    s_bmark[(((tx >> 2) + 1) * 4 + ((ty >> 2) + 1)) * 4 + ((tz >> 2) + 1)] = 1;   // node 8b+t: block 2b+(t>>2)
+                }
+            }
+        }
+        {   // cubic footprint: local nodes [cmin, cmin + cext + 4) per axis (tile origin 8b-1)
+            const int ex = cext[0] + 4, ey = cext[1] + 4, ez = cext[2] + 4;
+            for (int i = tid; i < ex * ey * ez; i += kP2GThreads) {
+                const int tx = cmin[0] + i / (ey * ez), ty = cmin[1] + (i / ez) % ey, tz = cmin[2] + i % ez;
+                const int li = (tx * kCE + ty) * kCE + tz;
+                const float a4 = ct[li], a5 = ct[kCN + li];
+                if (a4 != 0.0f || a5 != 0.0f) {
+                    ct[li] = 0.0f; ct[kCN + li] = 0.0f;
+                    const int gx = org[0] - 1 + tx, gy = org[1] - 1 + ty, gz = org[2] - 1 + tz;
+                    atomicAdd(&w.g_dmg[((long long)gx * ng + gy) * ng + gz], make_float2(a4, a5));
+                    s_bmark[(((tx + 3) >> 2) * 4 + ((ty + 3) >> 2)) * 4 + ((tz + 3) >> 2)] = 1;   // node 8b-1+t: block 2b-1+((t+3)>>2)
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < 64 && s_bmark[tid]) {
+            const int bxx = 2 * bx - 1 + (tid >> 4), byy = 2 * by - 1 + ((tid >> 2) & 3), bzz = 2 * bz - 1 + (tid & 3);
+            if (bxx >= 0 && byy >= 0 && bzz >= 0 && bxx < w.nbs && byy < w.nbs && bzz < w.nbs)
+                w.block_mask[((long long)bxx * w.nbs + byy) * w.nbs + bzz] = 1;
         }
         __syncthreads();
     }
 }
 
-void launch_p2g(const pm_params &prm, const Parts &P, const WS &w, cudaStream_t s) {
-    const long long blocks = (P.n + kP2GRange - 1) / kP2GRange;
-    if (blocks <= 0) return;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_p2g<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
-        configured = true;
+// Particles per CTA: equal ranges that fill whole waves of the resident CTA
+// slots, so no SM idles behind a partial last wave.
+int balanced_range(long long n, int slots, int max_range) {
+    if (slots < 1) slots = 1;
+    const long long waves = (n + (long long)slots * max_range - 1) / ((long long)slots * max_range);
+    long long r = (n + slots * waves - 1) / (slots * waves);
+    r = (r + 31) / 32 * 32;
+    return (int)std::max<long long>(32, std::min<long long>(r, max_range));
+}
+
+int resident_slots(const void *kernel, int threads, size_t smem) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
+    return std::max(1, sms * std::max(per, 1));
+}
+
+// One-time kernel attribute set-up for the current device (not a stream
+// operation, so it must not first happen inside a stream capture).
+void prepare_p2g() {
+    static int done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        done[dev] = 1;
     }
-    k_p2g<8><<<(unsigned)blocks, kP2GThreads, kP2GSmem, s>>>(prm, P, w);
+}
+
+void launch_p2g(const pm_params &prm, const Parts &P, const WS &w, cudaStream_t s, int range) {
+    if (P.n <= 0) return;
+    k_stress<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(prm, P, w);
+    prepare_p2g();
+    // small fixed ranges let the hardware scheduler balance CTAs whose segment
+    // structure differs (measured: 512 beats one balanced wave by 18% at 1M)
+    if (range <= 0) range = kP2GDefaultRange;
+    range = std::max(64, std::min(range, kP2GMaxRange)) / 32 * 32;
+    const long long blocks = (P.n + range - 1) / range;
+    k_scatter<<<(unsigned)blocks, kP2GThreads, kP2GSmem, s>>>(prm, w, P.n, range);
 }
 
 }  // namespace pm

@@ -39,12 +39,12 @@ def test_abi_version():
 def test_workspace_layout_is_aligned_and_disjoint(n, ng):
     L = _lib.workspace_layout(n, ng)
     offs = [L.ctrl, L.keys_a, L.keys_b, L.vals_a, L.vals_b, L.hist, L.block_mask, L.block_list, L.g_mom, L.g_dmg,
-            L.g_vel, L.g_gd, L.total]
+            L.g_vel, L.g_gd, L.payload, L.inv_perm, L.total]
     assert all(o % 256 == 0 for o in offs)
     assert offs == sorted(offs) and len(set(offs)) == len(offs)
     nn = max(n, 1)
     G = ng ** 3
-    assert L.keys_b - L.keys_a >= 4 * nn and L.g_dmg - L.g_mom >= 16 * G and L.total - L.g_gd >= 4 * G
+    assert L.keys_b - L.keys_a >= 4 * nn and L.g_dmg - L.g_mom >= 16 * G and L.payload - L.g_gd >= 4 * G and L.inv_perm - L.payload >= 80 * nn and L.total - L.inv_perm >= 4 * nn
     assert L.sort_passes == 3 if ng >= 64 else L.sort_passes >= 1
     assert _lib.workspace_size(n, ng) == L.total
 
