@@ -5,9 +5,9 @@
  *   - returns PM_OK (0) or a pm_status code; pm_last_error() describes the
  *     last failure on the calling thread;
  *   - enqueues work on the given CUDA stream (a cudaStream_t passed as
- *     void*), never synchronises and never allocates device memory: the
- *     caller provides every buffer, including the workspace, so every call
- *     can be captured in a CUDA graph;
+ *     void*) and never allocates device memory: the caller provides every
+ *     buffer, including the workspace; entry points not marked
+ *     "synchronises" never synchronise and can be captured in a CUDA graph;
  *   - reads and writes particle state in place.
  *
  * Particle state is structure-of-arrays: a field with c components is c
@@ -125,7 +125,8 @@ int pm_abi_version(void);
 const char *pm_last_error(void);
 
 /* sizeof the ABI structs, for binding checks: 0 pm_params, 1 pm_particles,
- * 2 pm_clock, 3 pm_status_info, 4 pm_ws_layout, 5 pm_grip, 6 pm_collider. */
+ * 2 pm_clock, 3 pm_status_info, 4 pm_ws_layout, 5 pm_grip, 6 pm_collider,
+ * 7 pm_batch_layout. */
 size_t pm_struct_size(int32_t which);
 
 /* One-time set-up of the current device (kernel attributes).  Every entry
@@ -183,6 +184,53 @@ int pm_g2p(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
 /* Copies the status counters to host memory (synchronises `stream`). */
 int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, pm_status_info *out,
                    void *stream);
+
+/* ---------------------------------------------------------------- batches */
+
+/* Many independent scenes advanced by one set of launches per substep.  The
+ * scenes' particles are concatenated (scene s owns particles
+ * [sum n[<s], sum n[<=s]) of one pm_particles whose n is the total); each
+ * scene keeps its own grid (n_grid from its pm_params), parameters, grips,
+ * colliders, clock and damage cadence.  The scene parameters and the packing
+ * tables are stored in the workspace by pm_batch_workspace_init (and
+ * pm_batch_set_params), so pm_batch_substep reads no host data besides the
+ * (n, n_grid) arrays that size its launches, which must equal those the
+ * workspace was initialised for (the library keeps a host record per
+ * workspace and returns PM_ERR_WORKSPACE otherwise).
+ * Replaces a Python loop over many AnisoMPM objects calling run_frame
+ * (anisompm.py:805-807) one scene at a time; the reference has no batch API. */
+#define PM_MAX_BATCH_SCENES 4096
+
+typedef struct pm_batch_layout {
+    pm_ws_layout ws;                 /* ctrl holds one control block per scene */
+    size_t params;                   /* pm_params[n_scenes] */
+    size_t tables;                   /* int64 particle / node / sort-block / grid-block / CTA prefix tables */
+    int64_t n_total, n_nodes, n_grid_blocks, n_sort_blocks, n_g2p_ctas;
+} pm_batch_layout;
+
+int pm_batch_workspace_size(int32_t n_scenes, const int64_t *n, const int32_t *n_grid, size_t *bytes);
+int pm_batch_workspace_layout(int32_t n_scenes, const int64_t *n, const int32_t *n_grid, pm_batch_layout *out);
+
+/* Zeroes the workspace and stores the scene tables and prms[n_scenes] (host
+ * array).  Synchronises `stream`; not capturable. */
+int pm_batch_workspace_init(void *ws, size_t ws_bytes, int32_t n_scenes, const int64_t *n, const pm_params *prms,
+                            void *stream);
+/* Replaces the stored parameters (same n and n_grid).  Synchronises `stream`. */
+int pm_batch_set_params(void *ws, size_t ws_bytes, int32_t n_scenes, const int64_t *n, const pm_params *prms,
+                        void *stream);
+/* Forgets the host record of a workspace that is about to be freed. */
+int pm_batch_workspace_release(const void *ws);
+
+/* One substep of every scene: scene s reads its clock from dev_clocks[s]
+ * (device memory, n_scenes consecutive pm_clock), so a graph captured over
+ * rows of a device clock table replays with new times. */
+int pm_batch_substep(int32_t n_scenes, const int64_t *n, const int32_t *n_grid, const pm_particles *P, void *ws,
+                     size_t ws_bytes, const pm_clock *dev_clocks, void *stream);
+
+/* Status counters of every scene into out[n_scenes] (n_active_blocks is the
+ * batch total).  Synchronises `stream`. */
+int pm_batch_read_status(const void *ws, size_t ws_bytes, int32_t n_scenes, const int64_t *n, const int32_t *n_grid,
+                         pm_status_info *out, void *stream);
 
 /* ---------------------------------------------------------------- helpers */
 

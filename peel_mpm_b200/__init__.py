@@ -9,6 +9,7 @@ device and the built library, and fails otherwise.
 """
 from .anisompm import (AnisoMPM, Collider, ParticleGrip, bin_particles, grip_bc, halfspace_collider,
                        sphere_collider, sym_eig)
+from .batched import BatchedAnisoMPM
 
-__all__ = ["AnisoMPM", "Collider", "ParticleGrip", "bin_particles", "grip_bc", "halfspace_collider",
-           "sphere_collider", "sym_eig"]
+__all__ = ["AnisoMPM", "BatchedAnisoMPM", "Collider", "ParticleGrip", "bin_particles", "grip_bc",
+           "halfspace_collider", "sphere_collider", "sym_eig"]

@@ -20,7 +20,10 @@ EXPORTS = (
     "pm_abi_version", "pm_last_error", "pm_struct_size", "pm_prepare", "pm_workspace_size", "pm_workspace_init",
     "pm_workspace_layout", "pm_substep", "pm_substep_dev_clock", "pm_set_clock", "pm_bin", "pm_p2g",
     "pm_grid_update", "pm_g2p", "pm_read_status", "pm_sym_eig", "pm_bin_sort", "pm_bin_sort_static",
+    "pm_batch_workspace_size", "pm_batch_workspace_layout", "pm_batch_workspace_init", "pm_batch_set_params",
+    "pm_batch_workspace_release", "pm_batch_substep", "pm_batch_read_status",
 )
+PM_MAX_BATCH_SCENES = 4096
 PM_BIN_STATIC_MAX_N = 262144
 
 
@@ -71,7 +74,12 @@ class pm_ws_layout(C.Structure):
                [("sort_passes", C.c_int32), ("n_tiles", C.c_int32)]
 
 
-STRUCTS = (pm_params, pm_particles, pm_clock, pm_status_info, pm_ws_layout, pm_grip, pm_collider)
+class pm_batch_layout(C.Structure):
+    _fields_ = [("ws", pm_ws_layout), ("params", C.c_size_t), ("tables", C.c_size_t)] + \
+               [(f, C.c_int64) for f in ("n_total", "n_nodes", "n_grid_blocks", "n_sort_blocks", "n_g2p_ctas")]
+
+
+STRUCTS = (pm_params, pm_particles, pm_clock, pm_status_info, pm_ws_layout, pm_grip, pm_collider, pm_batch_layout)
 
 _lib = None
 
@@ -109,6 +117,13 @@ def load():
         "pm_sym_eig": (C.c_int, [vp, i64, i32, vp, vp, vp]),
         "pm_bin_sort": (C.c_int, [vp, i64, i64, i32, C.c_double, vp, vp, vp, sz, vp]),
         "pm_bin_sort_static": (C.c_int, [vp, i64, i64, i32, C.c_double, vp, vp, vp]),
+        "pm_batch_workspace_size": (C.c_int, [i32, vp, vp, C.POINTER(sz)]),
+        "pm_batch_workspace_layout": (C.c_int, [i32, vp, vp, C.POINTER(pm_batch_layout)]),
+        "pm_batch_workspace_init": (C.c_int, [vp, sz, i32, vp, C.POINTER(pm_params), vp]),
+        "pm_batch_set_params": (C.c_int, [vp, sz, i32, vp, C.POINTER(pm_params), vp]),
+        "pm_batch_workspace_release": (C.c_int, [vp]),
+        "pm_batch_substep": (C.c_int, [i32, vp, vp, C.POINTER(pm_particles), vp, sz, vp, vp]),
+        "pm_batch_read_status": (C.c_int, [vp, sz, i32, vp, vp, C.POINTER(pm_status_info), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -144,4 +159,29 @@ def workspace_layout(n: int, n_grid: int) -> pm_ws_layout:
     lib = load()
     lay = pm_ws_layout()
     check(lib.pm_workspace_layout(int(n), int(n_grid), C.byref(lay)), "pm_workspace_layout")
+    return lay
+
+
+def _scene_arrays(ns, grids):
+    S = len(ns)
+    if S != len(grids):
+        raise ValueError("one n_grid per scene")
+    n_arr = (C.c_int64 * S)(*[int(v) for v in ns])
+    g_arr = (C.c_int32 * S)(*[int(v) for v in grids])
+    return S, n_arr, g_arr
+
+
+def batch_workspace_size(ns, grids) -> int:
+    lib = load()
+    S, n_arr, g_arr = _scene_arrays(ns, grids)
+    out = C.c_size_t(0)
+    check(lib.pm_batch_workspace_size(S, n_arr, g_arr, C.byref(out)), "pm_batch_workspace_size")
+    return int(out.value)
+
+
+def batch_workspace_layout(ns, grids) -> pm_batch_layout:
+    lib = load()
+    S, n_arr, g_arr = _scene_arrays(ns, grids)
+    lay = pm_batch_layout()
+    check(lib.pm_batch_workspace_layout(S, n_arr, g_arr, C.byref(lay)), "pm_batch_workspace_layout")
     return lay

@@ -212,6 +212,7 @@ class AnisoMPM:
         self._params_key = None
         self._tag_key = None
         self._graphs = {}
+        self._batch = None
 
     # ------------------------------------------------------------------ views
     def _view(self, name):
@@ -285,6 +286,8 @@ class AnisoMPM:
                    alpha: float = -1.0, percentage: float = 0.15, l0_scale: float = 0.5, eta: float = 0.01,
                    zeta: float = 1.0, residual: float = 0.001, allow_damage: bool = True):
         """Append particles (anisompm.py:350-427, _append 429-463)."""
+        if getattr(self, "_batch", None) is not None:
+            raise RuntimeError("this scene is packed into a BatchedAnisoMPM; call its unpack() before add_object")
         dev, dt = self.device, self.dtype
         x = torch.as_tensor(x).to(dev, dt)
         vol = torch.as_tensor(vol).to(dev, dt)
@@ -479,9 +482,9 @@ class AnisoMPM:
             return self._P
         P = _lib.pm_particles()
         P.n = self.n
-        P.plane_stride = self._S.shape[1]
+        P.plane_stride = self._S.stride(0)
         base = self._S.data_ptr()
-        st = self._S.shape[1] * 4
+        st = self._S.stride(0) * 4
         for name in ("x", "v", "F", "C", "d", "lap", "D_hist", "vol0", "mass", "mu", "lam", "sigma_c", "eta",
                      "zeta", "l0", "residual", "A0", "phi"):
             setattr(P, name, base + _PLANES[name][0] * st)

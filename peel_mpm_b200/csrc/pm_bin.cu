@@ -29,6 +29,36 @@ __global__ void __launch_bounds__(256) k_keys(const float *__restrict__ x, long 
     if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0 && ctrl != nullptr) ctrl->any_allow = 1;
 }
 
+// Substep keys: block-major sort key of the base cell, offset by the scene's
+// first sort block; identity ids; allow.any() per scene (a warp whose lanes
+// share a scene votes once).
+template <class SC>
+__global__ void __launch_bounds__(256) k_keys_t(const SC sc, const float *__restrict__ x, long long n, long long ps,
+                                                unsigned *__restrict__ keys, int *__restrict__ vals,
+                                                const unsigned char *__restrict__ allow, Ctrl *ctrl) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const int sid = sc.of_particle(p);
+        const pm_params &prm = sc.params(sid);
+        const int ng = prm.n_grid;
+        const float inv_dx = (float)prm.inv_dx;
+        int qb[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) qb[a] = sat_base(floorf(__fsub_rn(__fmul_rn(x[a * ps + p], inv_dx), 0.5f)), ng);
+        keys[p] = (sc.sblock_base(sid) << kSortBlockBits) + blocked_key(qb, ng);
+        vals[p] = (int)p;
+        const bool a = allow[p] != 0;
+        const unsigned act = __activemask();
+        const int lane = threadIdx.x & 31, first = __ffs(act) - 1;
+        const int s0 = __shfl_sync(act, sid, first);
+        if (__all_sync(act, sid == s0)) {
+            if (__any_sync(act, a) && lane == first) ctrl[s0].any_allow = 1;
+        } else if (a) {
+            ctrl[sid].any_allow = 1;
+        }
+    }
+}
+
 // Compacts the marked blocks into block_list and clears the marks.
 __global__ void __launch_bounds__(256) k_compact_blocks(unsigned char *__restrict__ block_mask, long long nb,
                                                         int *__restrict__ block_list, Ctrl *ctrl) {
@@ -230,11 +260,13 @@ void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv) {
     }
 }
 
-void launch_keys(const WS &w, const Parts &P, int ng, float inv_dx, cudaStream_t s) {
+template <class SC>
+void launch_keys(const SC &sc, const WS &w, const Parts &P, cudaStream_t s) {
     const int blocks = (int)std::min<long long>((P.n + 255) / 256, 148LL * 16);
-    k_keys<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(P.x, P.n, P.ps, ng, inv_dx, true, w.keys_a, w.vals_a, P.allow,
-                                                  w.ctrl);
+    k_keys_t<SC><<<blocks > 0 ? blocks : 1, 256, 0, s>>>(sc, P.x, P.n, P.ps, w.keys_a, w.vals_a, P.allow, w.ctrl);
 }
+template void launch_keys<PlainScenes>(const PlainScenes &, const WS &, const Parts &, cudaStream_t);
+template void launch_keys<BatchScenes>(const BatchScenes &, const WS &, const Parts &, cudaStream_t);
 
 void launch_compact(const WS &w, cudaStream_t s) {
     const int cb = (int)std::min<long long>((w.n_blocks + 255) / 256, 148LL * 8);

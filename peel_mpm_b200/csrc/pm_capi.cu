@@ -76,6 +76,10 @@ int get_ws(void *ws, size_t bytes, long long n, int ng, pm::WS *out) {
 namespace pm {
 // Lets other translation units of the library report through pm_last_error().
 int report_error(int code, const char *msg) { return fail(code, msg); }
+int api_check_device() { return check_device(); }
+int api_check_params(const pm_params *prm) { return check_params(prm); }
+int api_check_particles(const pm_particles *P, bool need_all) { return check_particles(P, need_all); }
+int api_cuda_check(const char *where) { return cuda_check(where); }
 }  // namespace pm
 
 extern "C" {
@@ -93,6 +97,7 @@ size_t pm_struct_size(int32_t which) {
         case 4: return sizeof(pm_ws_layout);
         case 5: return sizeof(pm_grip);
         case 6: return sizeof(pm_collider);
+        case 7: return sizeof(pm_batch_layout);
         default: return 0;
     }
 }
@@ -151,7 +156,7 @@ int pm_bin(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
     const pm::Parts parts = pm::make_parts(P);
     cudaStream_t s = (cudaStream_t)stream;
-    pm::launch_keys(w, parts, prm->n_grid, (float)prm->inv_dx, s);
+    pm::launch_keys(pm::PlainScenes{*prm}, w, parts, s);
     pm::launch_sort(w, P->n, s, w.inv_perm);
     return cuda_check("pm_bin");
 }
@@ -161,7 +166,7 @@ int pm_p2g(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
-    pm::launch_p2g(*prm, pm::make_parts(P), w, (cudaStream_t)stream);
+    pm::launch_p2g(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream);
     pm::launch_compact(w, (cudaStream_t)stream);
     return cuda_check("pm_p2g");
 }
@@ -171,7 +176,7 @@ int pm_grid_update(const pm_params *prm, void *ws, size_t ws_bytes, int64_t n, v
     if ((rc = check_device()) || (rc = check_params(prm))) return rc;
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, n, prm->n_grid, &w))) return rc;
-    pm::launch_grid(*prm, w, (cudaStream_t)stream);
+    pm::launch_grid(pm::PlainScenes{*prm}, w, (cudaStream_t)stream);
     return cuda_check("pm_grid_update");
 }
 
@@ -180,7 +185,7 @@ int pm_g2p(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
-    pm::launch_g2p(*prm, pm::make_parts(P), w, (cudaStream_t)stream);
+    pm::launch_g2p(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream);
     return cuda_check("pm_g2p");
 }
 
@@ -197,12 +202,13 @@ static int substep_common(const pm_params *prm, const pm_particles *P, void *ws,
     else
         pm::launch_set_clock_dev(*prm, w, dev_clocks, row, s);
     if (P->n > 0) {
-        pm::launch_keys(w, parts, prm->n_grid, (float)prm->inv_dx, s);
+        const pm::PlainScenes sc{*prm};
+        pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, P->n, s, w.inv_perm);
-        pm::launch_p2g(*prm, parts, w, s);
+        pm::launch_p2g(sc, parts, w, s);
         pm::launch_compact(w, s);
-        pm::launch_grid(*prm, w, s);
-        pm::launch_g2p(*prm, parts, w, s);
+        pm::launch_grid(sc, w, s);
+        pm::launch_g2p(sc, parts, w, s);
     }
     return cuda_check("pm_substep");
 }

@@ -18,6 +18,7 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;   // keys per radix tile
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
+constexpr int kG2PThreads = 256;     // G2P particles per CTA
 
 // Device control block: per-substep inputs and status counters.
 struct Ctrl {
@@ -51,26 +52,27 @@ __host__ __device__ inline int blocked_key_bits(int ng) {
 
 struct Layout {
     size_t ctrl, keys_a, keys_b, vals_a, vals_b, hist, block_mask, block_list;
-    size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, total;
+    size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, tables, total;
     int passes, n_tiles, nbs;
     long long n_blocks, n_nodes;
 };
 
-__host__ __device__ inline Layout make_layout(long long n, int ng) {
+// n particles, n_nodes grid nodes, n_blocks 4^3 grid blocks, sort keys of
+// key_bits bits, n_ctrl control blocks and table_bytes of scene tables.
+__host__ __device__ inline Layout make_layout_sized(long long n, long long n_nodes, long long n_blocks, int key_bits,
+                                                    int n_ctrl, size_t table_bytes) {
     Layout L;
     const size_t A = 256;
     L.n_tiles = (int)((n + kSortTile - 1) / kSortTile);
     if (L.n_tiles < 1) L.n_tiles = 1;
-    {
-        const int kb = sort_bits(ng) > blocked_key_bits(ng) ? sort_bits(ng) : blocked_key_bits(ng);
-        L.passes = (kb + kRadixBits - 1) / kRadixBits;
-    }
-    L.nbs = (ng + kBlockEdge - 1) / kBlockEdge;
-    L.n_blocks = (long long)L.nbs * L.nbs * L.nbs;
-    L.n_nodes = (long long)ng * ng * ng;
+    L.passes = (key_bits + kRadixBits - 1) / kRadixBits;
+    if (L.passes < 1) L.passes = 1;
+    L.nbs = 0;
+    L.n_blocks = n_blocks;
+    L.n_nodes = n_nodes;
     size_t nn = (size_t)(n > 0 ? n : 1);
     size_t o = 0;
-    L.ctrl = o;       o = align_up(o + sizeof(Ctrl), A);
+    L.ctrl = o;       o = align_up(o + sizeof(Ctrl) * (size_t)(n_ctrl > 0 ? n_ctrl : 1), A);
     L.keys_a = o;     o = align_up(o + 4 * nn, A);
     L.keys_b = o;     o = align_up(o + 4 * nn, A);
     L.vals_a = o;     o = align_up(o + 4 * nn, A);
@@ -84,7 +86,18 @@ __host__ __device__ inline Layout make_layout(long long n, int ng) {
     L.g_gd = o;       o = align_up(o + 4 * (size_t)L.n_nodes, A);
     L.payload = o;    o = align_up(o + 80 * nn, A);
     L.inv_perm = o;   o = align_up(o + 4 * nn, A);
+    L.tables = o;     o = align_up(o + table_bytes, A);
     L.total = o;
+    return L;
+}
+
+// Single scene: the sort must also hold the reference (x-major) numbering of
+// pm_bin_sort.
+__host__ __device__ inline Layout make_layout(long long n, int ng) {
+    const int nbs = (ng + kBlockEdge - 1) / kBlockEdge;
+    const int kb = sort_bits(ng) > blocked_key_bits(ng) ? sort_bits(ng) : blocked_key_bits(ng);
+    Layout L = make_layout_sized(n, (long long)ng * ng * ng, (long long)nbs * nbs * nbs, kb, 1, 0);
+    L.nbs = nbs;
     return L;
 }
 
@@ -160,6 +173,61 @@ inline Parts make_parts(const pm_particles *P) {
     q.tau_last = P->tau_last; q.J_last = P->J_last;
     return q;
 }
+
+// ------------------------------------------------------------------ scenes
+// Kernels are written once against a scene policy.  PlainScenes is the single
+// scene of AnisoMPM.substep, its parameters passed by value; every lookup is a
+// constant.  BatchScenes describes many independent scenes packed into one
+// particle array, one grid buffer and one sort: scene s owns particles
+// [p_begin[s], p_begin[s+1]), grid nodes from node_base[s], sort blocks from
+// sblock_base[s], 4^3 grid blocks from gblock_base[s] and G2P CTAs from
+// cta_base[s]; lookups are binary searches over these prefix tables.
+__device__ __forceinline__ int upper_index(const long long *a, int n, long long v) {
+    int lo = 0, hi = n - 1;   // largest i in [0, n) with a[i] <= v
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct PlainScenes {
+    pm_params prm;
+    static constexpr bool batched = false;
+    __device__ __forceinline__ int of_particle(long long) const { return 0; }
+    __device__ __forceinline__ int of_sblock(unsigned) const { return 0; }
+    __device__ __forceinline__ int of_gblock(long long) const { return 0; }
+    __device__ __forceinline__ int of_cta(long long) const { return 0; }
+    __device__ __forceinline__ const pm_params &params(int) const { return prm; }
+    __device__ __forceinline__ long long p_begin(int) const { return 0; }
+    __device__ __forceinline__ long long p_end(int, long long n) const { return n; }
+    __device__ __forceinline__ long long node_base(int) const { return 0; }
+    __device__ __forceinline__ unsigned sblock_base(int) const { return 0; }
+    __device__ __forceinline__ long long gblock_base(int) const { return 0; }
+    __device__ __forceinline__ long long cta_base(int) const { return 0; }
+};
+
+struct BatchScenes {
+    const pm_params *prms;        // [n]
+    const long long *pb;          // particle begin, [n + 1]
+    const long long *nodeb;       // grid node base, [n]
+    const long long *sblk;        // first sort block, [n + 1]
+    const long long *gblk;        // first 4^3 grid block, [n + 1]
+    const long long *ctab;        // first G2P CTA, [n + 1]
+    int n;
+    static constexpr bool batched = true;
+    __device__ __forceinline__ int of_particle(long long p) const { return upper_index(pb, n, p); }
+    __device__ __forceinline__ int of_sblock(unsigned b) const { return upper_index(sblk, n, (long long)b); }
+    __device__ __forceinline__ int of_gblock(long long b) const { return upper_index(gblk, n, b); }
+    __device__ __forceinline__ int of_cta(long long c) const { return upper_index(ctab, n, c); }
+    __device__ __forceinline__ const pm_params &params(int s) const { return prms[s]; }
+    __device__ __forceinline__ long long p_begin(int s) const { return pb[s]; }
+    __device__ __forceinline__ long long p_end(int s, long long) const { return pb[s + 1]; }
+    __device__ __forceinline__ long long node_base(int s) const { return nodeb[s]; }
+    __device__ __forceinline__ unsigned sblock_base(int s) const { return (unsigned)sblk[s]; }
+    __device__ __forceinline__ long long gblock_base(int s) const { return gblk[s]; }
+    __device__ __forceinline__ long long cta_base(int s) const { return ctab[s]; }
+};
 
 // ------------------------------------------------------------------ cells
 // floor(v).to(long) then clamp, as the reference forms base cells: NaN or a

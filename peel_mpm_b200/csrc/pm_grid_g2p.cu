@@ -42,6 +42,32 @@ __global__ void k_set_clock_dev(Ctrl *c, const pm_clock *dev, int row, int ncol)
     }
 }
 
+// Batched clock: block s loads scene s's clock from dev[s]; block 0 also
+// resets the shared active-block counter.
+__global__ void k_set_clock_b(Ctrl *c, const pm_params *prms, const pm_clock *dev) {
+    const int sid = blockIdx.x, t = threadIdx.x;
+    const pm_clock *clk = dev + sid;
+    Ctrl *cs = c + sid;
+    if (t == 0) {
+        cs->time = clk->time;
+        cs->step = clk->step;
+        cs->any_allow = 0;
+        if (sid == 0) cs->n_active = 0;
+    }
+    if (t < prms[sid].n_colliders) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float o = (float)clk->col_origin[t][a], o2 = (float)clk->col_origin_next[t][a];
+            cs->col_origin[t][a] = o;
+            cs->col_vel[t][a] = __fdiv_rn(__fsub_rn(o2, o), 1e-4f);
+        }
+    }
+}
+
+void launch_set_clock_batch(const BatchScenes &sc, const WS &w, const pm_clock *dev, cudaStream_t s) {
+    k_set_clock_b<<<sc.n, 32, 0, s>>>(w.ctrl, sc.prms, dev);
+}
+
 void launch_set_clock(const pm_params &prm, const WS &w, const pm_clock &clk, cudaStream_t s) {
     k_set_clock<<<1, 32, 0, s>>>(w.ctrl, clk, prm.n_colliders);
 }
@@ -75,24 +101,28 @@ __device__ __forceinline__ void resolve(float v[3], const float vc[3], const flo
 // One thread per node of the active blocks.  Reads and clears the P2G
 // accumulators, writes grid velocity and the normalised damage field
 // (anisompm.py:727-746, 777-779).
-__global__ void __launch_bounds__(256) k_grid(const pm_params prm, const WS w) {
-    const Ctrl *ctrl = w.ctrl;
-    const long long nact = min((long long)ctrl->n_active, w.n_blocks);
+template <class SC>
+__global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
+    const long long nact = min((long long)w.ctrl->n_active, w.n_blocks);
     const long long items = nact * 64;
-    const int ng = prm.n_grid, nbs = w.nbs;
-    const float dt = (float)prm.dt;
-    const float gdt[3] = {dt * (float)prm.gravity[0], dt * (float)prm.gravity[1], dt * (float)prm.gravity[2]};
-    const float damp = (float)prm.grid_damp;
-    const bool do_damp = prm.grid_damp != 1.0;
-    const float dx = (float)prm.dx;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
          it += (long long)gridDim.x * blockDim.x) {
-        const int b = w.block_list[it >> 6];
+        const int gb = w.block_list[it >> 6];
+        const int sid = sc.of_gblock(gb);
+        const pm_params &prm = sc.params(sid);
+        const Ctrl *ctrl = w.ctrl + sid;
+        const int ng = prm.n_grid, nbs = (ng + kBlockEdge - 1) / kBlockEdge;
+        const float dt = (float)prm.dt;
+        const float gdt[3] = {dt * (float)prm.gravity[0], dt * (float)prm.gravity[1], dt * (float)prm.gravity[2]};
+        const float damp = (float)prm.grid_damp;
+        const bool do_damp = prm.grid_damp != 1.0;
+        const float dx = (float)prm.dx;
+        const int b = (int)(gb - sc.gblock_base(sid));
         const int l = (int)(it & 63);
         const int bx = b / (nbs * nbs), by = (b / nbs) % nbs, bz = b % nbs;
         const int ix = bx * kBlockEdge + (l >> 4), iy = by * kBlockEdge + ((l >> 2) & 3), iz = bz * kBlockEdge + (l & 3);
         if (ix >= ng || iy >= ng || iz >= ng) continue;
-        const long long node = ((long long)ix * ng + iy) * ng + iz;
+        const long long node = sc.node_base(sid) + ((long long)ix * ng + iy) * ng + iz;
         const float4 mom = w.g_mom[node];
         const float2 dmg = w.g_dmg[node];
         w.g_mom[node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -130,11 +160,14 @@ __global__ void __launch_bounds__(256) k_grid(const pm_params prm, const WS w) {
     }
 }
 
-void launch_grid(const pm_params &prm, const WS &w, cudaStream_t s) {
+template <class SC>
+void launch_grid(const SC &sc, const WS &w, cudaStream_t s) {
     const long long max_items = w.n_blocks * 64;
     const int blocks = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, 148LL * 8));
-    k_grid<<<blocks, 256, 0, s>>>(prm, w);
+    k_grid<SC><<<blocks, 256, 0, s>>>(sc, w);
 }
+template void launch_grid<PlainScenes>(const PlainScenes &, const WS &, cudaStream_t);
+template void launch_grid<BatchScenes>(const BatchScenes &, const WS &, cudaStream_t);
 
 // --------------------------------------------------------------------- G2P
 // One CTA per 256 particles in particle order (coalesced state reads and
@@ -149,14 +182,14 @@ void launch_grid(const pm_params &prm, const WS &w, cudaStream_t s) {
 // (anisompm.py:749-760, 781-803).  A footprint larger than the staging
 // buffers (incoherent particle order), or a particle whose stencil needs the
 // reference's edge clamping, gathers from global memory instead.
-constexpr int kG2PThreads = 256;
 constexpr int kGTQ = 1200;   // staged quadratic nodes (float4)
 constexpr int kGTC = 2400;   // staged cubic nodes (float)
 
 template <bool TILE>
-__device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &P, const WS &w, long long p,
-                                             const float xp[3], const float F[9], const int lo[3], const int qd[3],
-                                             const int cd[3], const float4 *sq, const float *sc) {
+__device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &P, const float4 *gvel,
+                                             const float *ggd, unsigned *nonfinite, long long p, const float xp[3],
+                                             const float F[9], const int lo[3], const int qd[3], const int cd[3],
+                                             const float4 *sq, const float *sc) {
     const long long ps = P.ps;
     const int ng = prm.n_grid;
     const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx, dt = (float)prm.dt;
@@ -192,7 +225,7 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
                 for (int oz = 0; oz < 3; ++oz) {
                     const float wk = wxy * q.w[oz][2];
                     const int node = NX[ox] + NY[oy] + NZ[oz];
-                    const float4 g = TILE ? sq[node] : __ldg(&w.g_vel[node]);
+                    const float4 g = TILE ? sq[node] : __ldg(&gvel[node]);
                     const float u0 = wk * g.x, u1 = wk * g.y, u2 = wk * g.z;
                     nv[0] += u0; nv[1] += u1; nv[2] += u2;
                     const float dp[3] = {DX[ox], DY[oy], DZ[oz]};
@@ -235,7 +268,7 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
 #pragma unroll
                 for (int oz = 0; oz < 4; ++oz) {
                     const int node = NX[ox] + NY[oy] + NZ[oz];
-                    lap += (ab * c.w[oz][2] + e * c.w2[oz][2]) * (TILE ? sc[node] : __ldg(&w.g_gd[node]));
+                    lap += (ab * c.w[oz][2] + e * c.w2[oz][2]) * (TILE ? sc[node] : __ldg(&ggd[node]));
                 }
             }
         lap *= (float)(prm.inv_dx * prm.inv_dx);
@@ -258,7 +291,7 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
     for (int a = 0; a < 3; ++a) finite = finite && isfinite(xn[a]);
 #pragma unroll
     for (int k = 0; k < 9; ++k) finite = finite && isfinite(Fn[k]);
-    if (!finite) atomicAdd(&w.ctrl->nonfinite, 1u);
+    if (!finite) atomicAdd(nonfinite, 1u);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         P.x[a * ps + p] = xn[a];
@@ -272,14 +305,19 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
     P.lap[p] = lap;
 }
 
-__global__ void __launch_bounds__(kG2PThreads, 3) k_g2p(const pm_params prm, const Parts P, const WS w) {
+template <class SC>
+__global__ void __launch_bounds__(kG2PThreads, 3) k_g2p(const SC scn, const Parts P, const WS w) {
     __shared__ float4 sq[kGTQ];
     __shared__ float sc[kGTC];
     __shared__ int s_box[6];
     const int tid = threadIdx.x;
-    // particle order: state reads and writes are coalesced
-    const long long p = (long long)blockIdx.x * kG2PThreads + tid;
-    const bool valid = p < P.n;
+    // particle order: state reads and writes are coalesced; a CTA never spans scenes
+    const int sid = scn.of_cta(blockIdx.x);
+    const pm_params &prm = scn.params(sid);
+    const long long p = scn.p_begin(sid) + ((long long)blockIdx.x - scn.cta_base(sid)) * kG2PThreads + tid;
+    const bool valid = p < scn.p_end(sid, P.n);
+    const float4 *gvel = w.g_vel + scn.node_base(sid);
+    const float *ggd = w.g_gd + scn.node_base(sid);
     const int ng = prm.n_grid;
     const long long ps = P.ps;
     const float inv_dx = (float)prm.inv_dx;
@@ -325,27 +363,32 @@ __global__ void __launch_bounds__(kG2PThreads, 3) k_g2p(const pm_params prm, con
     if (tile) {   // regular nodes lie inside the grid, so no bounds test is needed
         for (int i = tid; i < qn; i += kG2PThreads) {
             const int gx = lo[0] + i / (qd[1] * qd[2]), gy = lo[1] + (i / qd[2]) % qd[1], gz = lo[2] + i % qd[2];
-            sq[i] = w.g_vel[((long long)gx * ng + gy) * ng + gz];
+            sq[i] = gvel[((long long)gx * ng + gy) * ng + gz];
         }
         for (int i = tid; i < cn; i += kG2PThreads) {
             const int gx = lo[0] - 1 + i / (cd[1] * cd[2]), gy = lo[1] - 1 + (i / cd[2]) % cd[1],
                       gz = lo[2] - 1 + i % cd[2];
-            sc[i] = w.g_gd[((long long)gx * ng + gy) * ng + gz];
+            sc[i] = ggd[((long long)gx * ng + gy) * ng + gz];
         }
     }
     __syncthreads();
     if (!valid) return;
     if (reg && tile)
-        g2p_particle<true>(prm, P, w, p, xp, F, lo, qd, cd, sq, sc);
+        g2p_particle<true>(prm, P, gvel, ggd, &w.ctrl[sid].nonfinite, p, xp, F, lo, qd, cd, sq, sc);
     else
-        g2p_particle<false>(prm, P, w, p, xp, F, lo, qd, cd, sq, sc);
+        g2p_particle<false>(prm, P, gvel, ggd, &w.ctrl[sid].nonfinite, p, xp, F, lo, qd, cd, sq, sc);
 }
 
-void launch_g2p(const pm_params &prm, const Parts &P, const WS &w, cudaStream_t s) {
-    const long long blocks = (P.n + kG2PThreads - 1) / kG2PThreads;
+// n_ctas: CTAs over all scenes (each scene's particles start a new CTA); the
+// plain form derives it from P.n.
+template <class SC>
+void launch_g2p(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, long long n_ctas) {
+    const long long blocks = n_ctas >= 0 ? n_ctas : (P.n + kG2PThreads - 1) / kG2PThreads;
     if (blocks <= 0) return;
-    k_g2p<<<(unsigned)blocks, kG2PThreads, 0, s>>>(prm, P, w);
+    k_g2p<SC><<<(unsigned)blocks, kG2PThreads, 0, s>>>(sc, P, w);
 }
+template void launch_g2p<PlainScenes>(const PlainScenes &, const Parts &, const WS &, cudaStream_t, long long);
+template void launch_g2p<BatchScenes>(const BatchScenes &, const Parts &, const WS &, cudaStream_t, long long);
 
 // ---------------------------------------------------------------- sym_eig
 __global__ void __launch_bounds__(256) k_sym_eig(const float *__restrict__ A, long long n, int sweeps,

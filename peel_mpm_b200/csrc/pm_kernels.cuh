@@ -7,19 +7,28 @@
 
 namespace pm {
 
-void launch_keys(const WS &w, const Parts &P, int ng, float inv_dx, cudaStream_t s);
+template <class SC> void launch_keys(const SC &sc, const WS &w, const Parts &P, cudaStream_t s);
 void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv = nullptr);
 void launch_compact(const WS &w, cudaStream_t s);
 void prepare_p2g();
 void launch_keys_only(const float *x, long long n, long long ps, int ng, float inv_dx, bool blocked, const WS &w,
                       cudaStream_t s);
-void launch_p2g(const pm_params &prm, const Parts &P, const WS &w, cudaStream_t s, int range = 0);
-void launch_grid(const pm_params &prm, const WS &w, cudaStream_t s);
-void launch_g2p(const pm_params &prm, const Parts &P, const WS &w, cudaStream_t s);
+template <class SC> void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int range = 0);
+template <class SC> void launch_grid(const SC &sc, const WS &w, cudaStream_t s);
+template <class SC> void launch_g2p(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, long long n_ctas = -1);
 void launch_set_clock(const pm_params &prm, const WS &w, const pm_clock &clk, cudaStream_t s);
 void launch_set_clock_dev(const pm_params &prm, const WS &w, const pm_clock *dev, int row, cudaStream_t s);
+void launch_set_clock_batch(const BatchScenes &sc, const WS &w, const pm_clock *dev, cudaStream_t s);
 int balanced_range(long long n, int slots, int max_range);
 int resident_slots(const void *kernel, int threads, size_t smem);
 void launch_sym_eig(const float *A, long long n, int sweeps, float *ev, float *V, cudaStream_t s);
+
+// Argument checks and error reporting of the C ABI (pm_capi.cu), shared with
+// the other entry-point files.
+int report_error(int code, const char *msg);
+int api_check_device();
+int api_check_params(const pm_params *prm);
+int api_check_particles(const pm_particles *P, bool need_all);
+int api_cuda_check(const char *where);
 
 }  // namespace pm

@@ -211,16 +211,19 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
 //   {fx | x, m} {m v, d} {affine 0..3} {affine 4..7} {affine 8, regular, 0, 0}
 // with fx = X - floor(X - 0.5) per axis for particles whose stencil needs no
 // clamping (regular, base cell in [1, n_grid-4]) and the position x otherwise.
-__global__ void __launch_bounds__(256, 3) k_stress(const pm_params prm, const Parts P, const WS w) {
+template <class SC>
+__global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, const WS w) {
     // particle order: the state reads and writes are coalesced; the payload
     // goes to the particle's sorted position
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.n) return;
+    const int sid = sc.of_particle(p);
+    const pm_params &prm = sc.params(sid);
     const long long s = w.inv_perm[p];
     const long long ps = P.ps;
     const int ng = prm.n_grid;
     const float inv_dx = (float)prm.inv_dx;
-    const Ctrl *ctrl = w.ctrl;
+    const Ctrl *ctrl = w.ctrl + sid;
     const bool do_damage = ctrl->any_allow != 0 && (ctrl->step % (long long)prm.damage_every) == 0;
     float tau[9];
     constitutive(prm, P, p, do_damage, tau);
@@ -392,7 +395,8 @@ __device__ __forceinline__ int compact_flags(int flags, int *out_short_or_int, b
     return total;
 }
 
-__global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const pm_params prm, const WS w, long long n,
+template <class SC>
+__global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const WS w, long long n,
                                                              int range) {
     extern __shared__ float4 s_raw[];
     float *qt = (float *)s_raw;                                        // [4][kQN]
@@ -409,9 +413,6 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const pm_params prm,
     const int tid = threadIdx.x;
     const long long r0 = (long long)blockIdx.x * range;
     const int len = (int)min((long long)range, n - r0);
-    const int ng = prm.n_grid;
-    const int nb = sort_blocks_per_axis(ng);
-    const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
     const unsigned *keys = w.sorted_keys + r0;
 
     // ---- segments: runs of one sort block in [0, len)
@@ -434,7 +435,17 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const pm_params prm,
     for (int sg = 0; sg < nseg; ++sg) {
         const int a = seg[sg];
         const int b = (sg + 1 < nseg) ? seg[sg + 1] : len;
-        const unsigned blk = keys[a] >> kSortBlockBits;
+        const unsigned gblk = keys[a] >> kSortBlockBits;       // segments never span scenes
+        const int sid = sc.of_sblock(gblk);
+        const pm_params &prm = sc.params(sid);
+        const int ng = prm.n_grid;
+        const int nb = sort_blocks_per_axis(ng);
+        const int nbs = (ng + kBlockEdge - 1) / kBlockEdge;
+        const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
+        float4 *g_mom = w.g_mom + sc.node_base(sid);
+        float2 *g_dmg = w.g_dmg + sc.node_base(sid);
+        unsigned char *bmask = w.block_mask + sc.gblock_base(sid);
+        const unsigned blk = gblk - sc.sblock_base(sid);
         const int bz = (int)(blk % nb), by = (int)((blk / nb) % nb), bx = (int)(blk / ((unsigned)nb * nb));
         const int org[3] = {bx * kSortBlock, by * kSortBlock, bz * kSortBlock};   // quadratic tile origin
         {   // the segment's cell bounding box (inside the block): the flush visits only its footprint
@@ -507,8 +518,8 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const pm_params prm,
                 float aff[9];
 #pragma unroll
                 for (int k = 0; k < 9; ++k) aff[k] = pay[6 + k][t];
-                scatter_particle_global(xp, mv, aff, pay[15][t], pay[16][t], inv_dx, dx, ng, w.g_mom, w.g_dmg,
-                                        w.block_mask, w.nbs);
+                scatter_particle_global(xp, mv, aff, pay[15][t], pay[16][t], inv_dx, dx, ng, g_mom, g_dmg, bmask,
+                                        nbs);
             }
             // ---------------- phase 2b: (cell, slab) items into the tiles
             // items 0 .. 3*nruns-1 are quadratic x-slabs, then 5*nruns cubic x-slabs,
@@ -633,7 +644,7 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const pm_params prm,
                 if (a0 != 0.0f || a1 != 0.0f || a2 != 0.0f || a3 != 0.0f) {
                     qt[li] = 0.0f; qt[kQN + li] = 0.0f; qt[2 * kQN + li] = 0.0f; qt[3 * kQN + li] = 0.0f;
                     const int gx = org[0] + tx, gy = org[1] + ty, gz = org[2] + tz;   // in the grid: regular nodes only
-                    atomicAdd(&w.g_mom[((long long)gx * ng + gy) * ng + gz], make_float4(a0, a1, a2, a3));
+                    atomicAdd(&g_mom[((long long)gx * ng + gy) * ng + gz], make_float4(a0, a1, a2, a3));
                     s_bmark[(((tx >> 2) + 1) * 4 + ((ty >> 2) + 1)) * 4 + ((tz >> 2) + 1)] = 1;   // node 8b+t: block 2b+(t>>2)
                 }
             }
@@ -647,7 +658,7 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const pm_params prm,
                 if (a4 != 0.0f || a5 != 0.0f) {
                     ct[li] = 0.0f; ct[kCN + li] = 0.0f;
                     const int gx = org[0] - 1 + tx, gy = org[1] - 1 + ty, gz = org[2] - 1 + tz;
-                    atomicAdd(&w.g_dmg[((long long)gx * ng + gy) * ng + gz], make_float2(a4, a5));
+                    atomicAdd(&g_dmg[((long long)gx * ng + gy) * ng + gz], make_float2(a4, a5));
                     s_bmark[(((tx + 3) >> 2) * 4 + ((ty + 3) >> 2)) * 4 + ((tz + 3) >> 2)] = 1;   // node 8b-1+t: block 2b-1+((t+3)>>2)
                 }
             }
@@ -655,8 +666,8 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const pm_params prm,
         __syncthreads();
         if (tid < 64 && s_bmark[tid]) {
             const int bxx = 2 * bx - 1 + (tid >> 4), byy = 2 * by - 1 + ((tid >> 2) & 3), bzz = 2 * bz - 1 + (tid & 3);
-            if (bxx >= 0 && byy >= 0 && bzz >= 0 && bxx < w.nbs && byy < w.nbs && bzz < w.nbs)
-                w.block_mask[((long long)bxx * w.nbs + byy) * w.nbs + bzz] = 1;
+            if (bxx >= 0 && byy >= 0 && bzz >= 0 && bxx < nbs && byy < nbs && bzz < nbs)
+                bmask[((long long)bxx * nbs + byy) * nbs + bzz] = 1;
         }
         __syncthreads();
     }
@@ -687,21 +698,25 @@ void prepare_p2g() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        cudaFuncSetAttribute(k_scatter<PlainScenes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        cudaFuncSetAttribute(k_scatter<BatchScenes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
         done[dev] = 1;
     }
 }
 
-void launch_p2g(const pm_params &prm, const Parts &P, const WS &w, cudaStream_t s, int range) {
+template <class SC>
+void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int range) {
     if (P.n <= 0) return;
-    k_stress<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(prm, P, w);
+    k_stress<SC><<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(sc, P, w);
     prepare_p2g();
     // small fixed ranges let the hardware scheduler balance CTAs whose segment
     // structure differs (measured: 512 beats one balanced wave by 18% at 1M)
     if (range <= 0) range = kP2GDefaultRange;
     range = std::max(64, std::min(range, kP2GMaxRange)) / 32 * 32;
     const long long blocks = (P.n + range - 1) / range;
-    k_scatter<<<(unsigned)blocks, kP2GThreads, kP2GSmem, s>>>(prm, w, P.n, range);
+    k_scatter<SC><<<(unsigned)blocks, kP2GThreads, kP2GSmem, s>>>(sc, w, P.n, range);
 }
+template void launch_p2g<PlainScenes>(const PlainScenes &, const Parts &, const WS &, cudaStream_t, int);
+template void launch_p2g<BatchScenes>(const BatchScenes &, const Parts &, const WS &, cudaStream_t, int);
 
 }  // namespace pm

@@ -292,6 +292,46 @@ def interface_peel(seed: int = 0) -> Scene:
         interface=(band, normals))
 
 
+def batch_scenes(seed: int = 0, n_scenes: int = 64, n_lo: int = 4096, n_hi: int = 262144) -> list:
+    """Independent scenes of uneven size for the batched form.
+
+    Scene k: particle count log-uniform in [n_lo, n_hi] (8 per cell on a
+    jittered 2^3 sub-lattice, so the count is 8x the box's cell count), a box
+    of random aspect, a grid of 32^3-128^3 sized to the box (2x its longest
+    edge plus 8 cells, rounded up to 16), E log-uniform in [1e3, 1e5],
+    nu in [0.2, 0.45], one fiber direction uniform on the sphere, sigma_c in
+    [50, 500], bottom layer clamped and one top edge pulled up at a velocity
+    in [0.1, 2] m/s; dt = 5e-5, 300 substeps."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        target = math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))
+        cells = max(1.0, target / 8.0)
+        asp = np.exp(rng.uniform(-0.5, 0.5, 3)) * np.array([1.0, 0.5, 1.0])
+        unit = (cells / float(np.prod(asp))) ** (1.0 / 3.0)
+        ext = tuple(int(max(2, round(unit * a))) for a in asp)
+        ng = int(min(128, max(32, math.ceil((2.0 * max(ext) + 8) / 16.0) * 16)))
+        dx = 1.0 / ng
+        lo = tuple((ng - e) // 2 for e in ext)
+        x = jittered_lattice(lo, ext, dx, 2, 0.25, rng)
+        n = x.shape[0]
+        E = math.exp(rng.uniform(math.log(1e3), math.log(1e5)))
+        nu = float(rng.uniform(0.2, 0.45))
+        fib = np.tile(uniform_directions(1, rng), (n, 1))
+        sig = float(rng.uniform(50.0, 500.0))
+        pull = float(rng.uniform(0.1, 2.0))
+        ylo, yhi = lo[1] * dx, (lo[1] + ext[1]) * dx
+        bottom = x[:, 1] < ylo + dx
+        top_edge = (x[:, 1] > yhi - dx) & (x[:, 0] < lo[0] * dx + dx)
+        out.append(Scene(
+            name=f"batch{seed}_{k}", n_grid=ng, grid_lim=1.0, dt=5e-5, n_steps=300,
+            x=x, vol=np.full(n, (dx / 2) ** 3), rho=1000.0, E=np.full(n, E), nu=nu,
+            fibers=fib, alpha=-1.0, sigma_c=np.full(n, sig), l0_scale=1.0, eta=1e-3,
+            d0=rng.uniform(0.0, 0.05, n), allow=~(bottom | top_edge),
+            grips=[Grip(bottom, (0.0, 0.0, 0.0)), Grip(top_edge, (0.0, pull, 0.0))]))
+    return out
+
+
 SCENES = {
     "plain_small": plain_small,
     "plain_1m": plain_1m,

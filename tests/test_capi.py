@@ -59,3 +59,46 @@ def test_argument_errors_without_device():
     assert lib.pm_struct_size(99) == 0
     with pytest.raises(_lib.PeelMPMError):
         _lib.check(lib.pm_workspace_size(-5, 64, C.byref(out)), "size")
+
+
+def _bits(v):
+    b = 0
+    while (1 << b) < v:
+        b += 1
+    return b
+
+
+@pytest.mark.parametrize("ns,gs", [([1000, 0, 5000, 70000], [32, 64, 48, 128]), ([1], [4]),
+                                   ([4096] * 64, [32 + 16 * (k % 7) for k in range(64)])])
+def test_batch_layout_packs_scenes(ns, gs):
+    L = _lib.batch_workspace_layout(ns, gs)
+    assert L.n_total == sum(ns)
+    assert L.n_nodes == sum(g ** 3 for g in gs)
+    assert L.n_grid_blocks == sum(((g + 3) // 4) ** 3 for g in gs)
+    assert L.n_sort_blocks == sum(((g + 7) // 8) ** 3 for g in gs)
+    assert L.n_g2p_ctas == sum((n + 255) // 256 for n in ns)
+    assert L.ws.sort_passes == (_bits(L.n_sort_blocks) + 9 + 7) // 8
+    w = L.ws
+    offs = [w.ctrl, w.keys_a, w.keys_b, w.vals_a, w.vals_b, w.hist, w.block_mask, w.block_list, w.g_mom, w.g_dmg,
+            w.g_vel, w.g_gd, w.payload, w.inv_perm, L.params, L.tables, w.total]
+    assert all(o % 256 == 0 for o in offs)
+    assert offs == sorted(offs) and len(set(offs)) == len(offs)
+    assert w.keys_a - w.ctrl >= 224 * len(ns)                      # one control block per scene
+    assert w.g_dmg - w.g_mom >= 16 * L.n_nodes and w.block_list - w.block_mask >= L.n_grid_blocks
+    assert L.tables - L.params >= C.sizeof(_lib.pm_params) * len(ns)
+    assert w.total - L.tables >= 5 * 8 * (len(ns) + 1)
+    assert _lib.batch_workspace_size(ns, gs) == w.total
+
+
+def test_batch_argument_errors_without_device():
+    lib = _lib.load()
+    out = C.c_size_t(0)
+    n1, g1 = (C.c_int64 * 1)(10), (C.c_int32 * 1)(32)
+    assert lib.pm_batch_workspace_size(0, n1, g1, C.byref(out)) == _lib.PM_ERR_ARG
+    assert lib.pm_batch_workspace_size(_lib.PM_MAX_BATCH_SCENES + 1, n1, g1, C.byref(out)) == _lib.PM_ERR_ARG
+    assert lib.pm_batch_workspace_size(1, (C.c_int64 * 1)(-1), g1, C.byref(out)) == _lib.PM_ERR_ARG
+    assert lib.pm_batch_workspace_size(1, n1, (C.c_int32 * 1)(2), C.byref(out)) == _lib.PM_ERR_ARG
+    assert lib.pm_batch_workspace_size(2, (C.c_int64 * 2)(1 << 30, 1 << 30), (C.c_int32 * 2)(32, 32),
+                                       C.byref(out)) == _lib.PM_ERR_ARG
+    assert lib.pm_batch_workspace_size(1, None, g1, C.byref(out)) == _lib.PM_ERR_ARG
+    assert lib.pm_batch_workspace_size(1, n1, g1, C.byref(out)) == _lib.PM_OK and out.value > 0

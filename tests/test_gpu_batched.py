@@ -1,0 +1,113 @@
+"""BatchedAnisoMPM against the same scenes stepped one by one.
+
+The batch runs every kernel once over all scenes (one sort over all scenes'
+keys, per-scene grids, parameters, grips, colliders and clocks read from the
+workspace).  Each scene must evolve as the plain solver evolves it alone;
+atomic summation order differs between runs, so the comparison uses the
+float32-rounding bounds of the graph tests, not bit equality.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import gpu_state, make_gpu_sim, rel_l2
+from peel_mpm_b200 import BatchedAnisoMPM, _lib, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_scenes():
+    # uneven sizes and grids, plus the scenes that exercise colliders,
+    # f_clamp, damage_every=2, grid damping, ramps and interface normals
+    return scenes.batch_scenes(seed=1, n_scenes=5, n_lo=500, n_hi=20000) + [
+        scenes.knobs_drop(), scenes.tiny_bar(), scenes.interface_peel()]
+
+
+def compare(sa, sb, tight=1e-5, loose=1e-3):
+    for f in ("x", "v", "F", "C"):
+        assert rel_l2(sb[f], sa[f]) < tight, f
+    for f in ("d", "lap", "D_hist"):
+        assert rel_l2(sb[f], sa[f]) < loose, f
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_batch_matches_individual_scenes(graphs):
+    scs = mixed_scenes()
+    solo = [make_gpu_sim(sc) for sc in scs]
+    packed = [make_gpu_sim(sc) for sc in scs]
+    batch = BatchedAnisoMPM(packed, use_graphs=graphs)
+    n_sub, frames = 6, 3
+    for f in range(frames):
+        t0 = [f * n_sub * sc.dt for sc in scs]
+        batch.run_frame(n_sub, t0)
+        for sim, t in zip(solo, t0):
+            sim.run_frame(n_sub, t)
+    torch.cuda.synchronize()
+    for sim_a, sim_b in zip(solo, packed):
+        assert sim_b._step == sim_a._step == n_sub * frames
+        compare(gpu_state(sim_a), gpu_state(sim_b))
+    st = batch.check()
+    assert len(st) == len(scs) and all(s["nonfinite"] == 0 for s in st)
+    if graphs:
+        assert len(batch._graphs) == 1
+
+
+def test_batch_views_alias_the_batch_and_unpack_copies():
+    scs = scenes.batch_scenes(seed=2, n_scenes=3, n_lo=300, n_hi=3000)
+    sims = [make_gpu_sim(sc) for sc in scs]
+    x0 = [s.x.clone() for s in sims]
+    batch = BatchedAnisoMPM(sims)
+    for s, x in zip(sims, x0):
+        assert torch.equal(s.x, x)                      # packing kept the state
+    batch.run_frame(4, 0.0)
+    torch.cuda.synchronize()
+    moved = [s.x.clone() for s in sims]
+    assert any(not torch.equal(m, x) for m, x in zip(moved, x0))
+    with pytest.raises(RuntimeError):
+        sims[0].add_object(torch.zeros(1, 3) + 0.5, torch.ones(1) * 1e-6)
+    batch.unpack()
+    for s, m in zip(sims, moved):
+        assert torch.equal(s.x, m)
+        assert s._batch is None
+    sims[0].run_frame(2, 0.0)                         # standalone again
+    torch.cuda.synchronize()
+    assert np.isfinite(sims[0].x.cpu().numpy()).all()
+
+
+def test_batch_parameter_change_reaches_the_graph():
+    scs = scenes.batch_scenes(seed=3, n_scenes=2, n_lo=400, n_hi=2000)
+    a = [make_gpu_sim(sc) for sc in scs]
+    b = [make_gpu_sim(sc) for sc in scs]
+    batch = BatchedAnisoMPM(a)
+    batch.run_frame(3, 0.0)
+    for s in b:
+        s.run_frame(3, 0.0)
+    a[1].gravity = (0.0, -20.0, 0.0)
+    b[1].gravity = (0.0, -20.0, 0.0)
+    t0 = [3 * sc.dt for sc in scs]
+    batch.run_frame(3, t0)
+    for s, t in zip(b, t0):
+        s.run_frame(3, t)
+    torch.cuda.synchronize()
+    assert len(batch._graphs) == 1                   # parameters live in the workspace
+    for sa, sb in zip(b, a):
+        compare(gpu_state(sa), gpu_state(sb))
+
+
+def test_batch_rejects_a_workspace_of_another_batch():
+    lib = _lib.load()
+    scs = scenes.batch_scenes(seed=4, n_scenes=2, n_lo=300, n_hi=1000)
+    batch = BatchedAnisoMPM([make_gpu_sim(sc) for sc in scs])
+    batch.run_frame(1, 0.0)
+    torch.cuda.synchronize()
+    P = batch._sync_descriptors()
+    wrong_n = (C.c_int64 * 2)(batch.ns[1], batch.ns[0])
+    rc = lib.pm_batch_substep(2, wrong_n, batch._g_arr, C.byref(P), batch._ws.data_ptr(), batch._ws_bytes,
+                              batch._ws.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc in (_lib.PM_ERR_ARG, _lib.PM_ERR_WORKSPACE)
+    other = torch.empty(batch._ws_bytes, dtype=torch.uint8, device="cuda")
+    rc = lib.pm_batch_substep(2, batch._n_arr, batch._g_arr, C.byref(P), other.data_ptr(), batch._ws_bytes,
+                              other.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.PM_ERR_WORKSPACE
