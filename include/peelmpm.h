@@ -126,7 +126,7 @@ const char *pm_last_error(void);
 
 /* sizeof the ABI structs, for binding checks: 0 pm_params, 1 pm_particles,
  * 2 pm_clock, 3 pm_status_info, 4 pm_ws_layout, 5 pm_grip, 6 pm_collider,
- * 7 pm_batch_layout. */
+ * 7 pm_batch_layout, 8 pm_state_adj, 9 pm_param_adj. */
 size_t pm_struct_size(int32_t which);
 
 /* One-time set-up of the current device (kernel attributes).  Every entry
@@ -184,6 +184,50 @@ int pm_g2p(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
 /* Copies the status counters to host memory (synchronises `stream`). */
 int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, pm_status_info *out,
                    void *stream);
+
+/* ---------------------------------------------------------------- adjoint */
+
+/* Reverse mode of the plain substep for gradients of a loss on the final
+ * state with respect to per-particle parameters and the initial state.  The
+ * reference gets these from PyTorch autograd through substep()
+ * (anisompm.py:593-803); here the caller records each forward substep of a
+ * checkpoint segment into a tape slot and then runs pm_substep_adjoint from
+ * the last slot to the first.  Not supported (PM_ERR_ARG): f_clamp,
+ * colliders, interface particles. */
+
+/* Adjoints of the mutable state, same plane layout as pm_particles. */
+typedef struct pm_state_adj {
+    int64_t plane_stride;
+    float *x, *v, *F, *C;            /* 3, 3, 9, 9 planes */
+    float *d, *lap, *D_hist;
+} pm_state_adj;
+
+/* Per-particle parameter gradients, accumulated (+=) by every adjoint
+ * substep; a NULL plane is skipped. */
+typedef struct pm_param_adj {
+    int64_t plane_stride;
+    float *mu, *lam, *sigma_c;
+    float *A0;                       /* 9 planes */
+} pm_param_adj;
+
+/* Tape for `slots` recorded substeps of n particles on an n_grid^3 grid:
+ * 24 bytes per grid node and slot plus three shared adjoint grids (48 bytes
+ * per node).  Zeroed once by pm_tape_init. */
+int pm_tape_size(int64_t n, int32_t n_grid, int32_t slots, size_t *bytes);
+int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32_t slots, void *stream);
+
+/* pm_substep that also records the substep's grid state into tape slot
+ * `slot`.  The particle state P advances in place as in pm_substep. */
+int pm_substep_record(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, const pm_clock *clk,
+                      void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream);
+
+/* Adjoint of the substep recorded in `slot`: pre is the state before it and
+ * post the state after it (same material planes), adj_in the adjoint of the
+ * post state, adj_out (distinct from adj_in) receives the adjoint of the pre
+ * state, and grads accumulates the parameter gradients. */
+int pm_substep_adjoint(const pm_params *prm, const pm_particles *pre, const pm_particles *post,
+                       const pm_state_adj *adj_in, const pm_state_adj *adj_out, const pm_param_adj *grads,
+                       void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream);
 
 /* ---------------------------------------------------------------- batches */
 

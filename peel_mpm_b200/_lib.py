@@ -22,6 +22,7 @@ EXPORTS = (
     "pm_grid_update", "pm_g2p", "pm_read_status", "pm_sym_eig", "pm_bin_sort", "pm_bin_sort_static",
     "pm_batch_workspace_size", "pm_batch_workspace_layout", "pm_batch_workspace_init", "pm_batch_set_params",
     "pm_batch_workspace_release", "pm_batch_substep", "pm_batch_read_status",
+    "pm_tape_size", "pm_tape_init", "pm_substep_record", "pm_substep_adjoint",
 )
 PM_MAX_BATCH_SCENES = 4096
 PM_BIN_STATIC_MAX_N = 262144
@@ -79,7 +80,16 @@ class pm_batch_layout(C.Structure):
                [(f, C.c_int64) for f in ("n_total", "n_nodes", "n_grid_blocks", "n_sort_blocks", "n_g2p_ctas")]
 
 
-STRUCTS = (pm_params, pm_particles, pm_clock, pm_status_info, pm_ws_layout, pm_grip, pm_collider, pm_batch_layout)
+class pm_state_adj(C.Structure):
+    _fields_ = [("plane_stride", C.c_int64)] + [(f, C.c_void_p) for f in ("x", "v", "F", "C", "d", "lap", "D_hist")]
+
+
+class pm_param_adj(C.Structure):
+    _fields_ = [("plane_stride", C.c_int64)] + [(f, C.c_void_p) for f in ("mu", "lam", "sigma_c", "A0")]
+
+
+STRUCTS = (pm_params, pm_particles, pm_clock, pm_status_info, pm_ws_layout, pm_grip, pm_collider, pm_batch_layout,
+           pm_state_adj, pm_param_adj)
 
 _lib = None
 
@@ -124,6 +134,13 @@ def load():
         "pm_batch_workspace_release": (C.c_int, [vp]),
         "pm_batch_substep": (C.c_int, [i32, vp, vp, C.POINTER(pm_particles), vp, sz, vp, vp]),
         "pm_batch_read_status": (C.c_int, [vp, sz, i32, vp, vp, C.POINTER(pm_status_info), vp]),
+        "pm_tape_size": (C.c_int, [i64, i32, i32, C.POINTER(sz)]),
+        "pm_tape_init": (C.c_int, [vp, sz, i64, i32, i32, vp]),
+        "pm_substep_record": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), vp, sz, C.POINTER(pm_clock),
+                                        vp, sz, i32, i32, vp]),
+        "pm_substep_adjoint": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), C.POINTER(pm_particles),
+                                         C.POINTER(pm_state_adj), C.POINTER(pm_state_adj), C.POINTER(pm_param_adj),
+                                         vp, sz, i32, i32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -185,3 +202,10 @@ def batch_workspace_layout(ns, grids) -> pm_batch_layout:
     lay = pm_batch_layout()
     check(lib.pm_batch_workspace_layout(S, n_arr, g_arr, C.byref(lay)), "pm_batch_workspace_layout")
     return lay
+
+
+def tape_size(n: int, n_grid: int, slots: int) -> int:
+    lib = load()
+    out = C.c_size_t(0)
+    check(lib.pm_tape_size(int(n), int(n_grid), int(slots), C.byref(out)), "pm_tape_size")
+    return int(out.value)

@@ -1,0 +1,839 @@
+// Reverse-mode adjoint of one plain substep (anisompm.py:593-803) for the
+// differentiable form: given the adjoints of the state after substep t
+// (x', v', F', C', d', lap', D_hist'), produce the adjoints of the state
+// before it and accumulate the gradients of the per-particle parameters mu,
+// lam, sigma_c and A0.
+//
+// The forward substep t is first recorded (pm_substep_record) into a tape
+// slot: grid velocity and mass {v, m}, the normalised damage field gd, the
+// cubic weight sums, the active 4^3 block list and the step's clock.  The
+// adjoint then runs three kernels:
+//   k_adj_scatter   G2P adjoint as a scatter (particle order): the adjoint of
+//                   the grid velocity and damage field, accumulated with one
+//                   vector atomic per cubic-stencil node;
+//   k_adj_grid      grid-update adjoint over the recorded active blocks
+//                   (normalisation by mass and by the cubic weight sum);
+//   k_adj_particle  P2G adjoint as a gather plus the constitutive adjoint
+//                   (particle order): recomputes the particle's constitutive
+//                   update, gathers the grid adjoints, and runs the polar,
+//                   stress, damage and eigen-split adjoints.
+// Non-smooth operations take the branch the forward took (relu, max and clamp
+// pass the adjoint where the forward passed the value; base cells are
+// piecewise constant).  Unsupported in the adjoint (rejected by the host):
+// f_clamp, colliders and interface particles.
+#include "pm_kernels.cuh"
+
+namespace pm {
+
+namespace {
+
+__device__ __forceinline__ float relu_f(float v) { return v > 0.0f ? v : 0.0f; }
+
+// Tape header of one slot.
+struct TapeHead {
+    unsigned n_active;
+    int any_allow;
+    long long step;
+    double time;
+    double pad;
+};
+
+// Quadratic weights with their derivatives wrt the local coordinate fx.
+struct QuadD {
+    int b[3];
+    float fx[3];
+    float w[3][3], dw[3][3];
+};
+__device__ __forceinline__ void quad_weights_d(const float x[3], float inv_dx, int ng, QuadD &q) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float X = __fmul_rn(x[a], inv_dx);
+        const float fb = floorf(__fsub_rn(X, 0.5f));
+        q.b[a] = sat_base(fb, ng);
+        const float f = __fsub_rn(X, fb);
+        q.fx[a] = f;
+        const float t0 = 1.5f - f, t1 = f - 1.0f, t2 = f - 0.5f;
+        q.w[0][a] = 0.5f * (t0 * t0);
+        q.w[1][a] = 0.75f - t1 * t1;
+        q.w[2][a] = 0.5f * (t2 * t2);
+        q.dw[0][a] = -t0;
+        q.dw[1][a] = -2.0f * t1;
+        q.dw[2][a] = t2;
+    }
+}
+
+// Cubic weights, second derivatives and the derivatives of both wrt f.
+struct CubicD {
+    int b[3];
+    float w[4][3], w2[4][3], dw[4][3], dw2[4][3];
+};
+__device__ __forceinline__ void cubic_weights_d(const float x[3], float inv_dx, int ng, CubicD &c) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float X = __fmul_rn(x[a], inv_dx);
+        const float fb = floorf(X);
+        c.b[a] = sat_base(fb, ng) - 1;
+        const float f = __fsub_rn(X, fb);
+        const float one = 1.0f - f;
+        c.w[0][a] = (1.0f / 6.0f) * (one * one * one);
+        c.w[1][a] = (2.0f / 3.0f - f * f) + 0.5f * (f * f * f);
+        c.w[2][a] = (2.0f / 3.0f - one * one) + 0.5f * (one * one * one);
+        c.w[3][a] = (1.0f / 6.0f) * (f * f * f);
+        c.w2[0][a] = one;
+        c.w2[1][a] = 3.0f * f - 2.0f;
+        c.w2[2][a] = 1.0f - 3.0f * f;
+        c.w2[3][a] = f;
+        c.dw[0][a] = -0.5f * one * one;
+        c.dw[1][a] = -2.0f * f + 1.5f * f * f;
+        c.dw[2][a] = 2.0f * one - 1.5f * one * one;
+        c.dw[3][a] = 0.5f * f * f;
+        c.dw2[0][a] = -1.0f;
+        c.dw2[1][a] = 3.0f;
+        c.dw2[2][a] = -3.0f;
+        c.dw2[3][a] = 1.0f;
+    }
+}
+
+__device__ __forceinline__ int node_of(int x, int y, int z, int ng) {
+    return (clampi(x, 0, ng - 1) * ng + clampi(y, 0, ng - 1)) * ng + clampi(z, 0, ng - 1);
+}
+
+struct AdjIn {
+    float xb[3], vb[3], Cb[9], Fb[9], db, lapb, Dhb;
+};
+__device__ __forceinline__ void load_adj(const pm_state_adj &A, long long p, AdjIn &a) {
+    const long long s = A.plane_stride;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a.xb[k] = A.x[k * s + p];
+        a.vb[k] = A.v[k * s + p];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        a.Cb[k] = A.C[k * s + p];
+        a.Fb[k] = A.F[k * s + p];
+    }
+    a.db = A.d[p];
+    a.lapb = A.lap[p];
+    a.Dhb = A.D_hist[p];
+}
+
+// Adjoint of the end of G2P: x' = clamp(x + dt v'), F' = (I + dt C') F.
+// Returns the total adjoints of v' and C' and the pass-through mask of x.
+__device__ __forceinline__ void g2p_tail_adj(const pm_params &prm, const float xp[3], const float vpost[3],
+                                             const float Fpre[9], const AdjIn &a, float vt[3], float Ct[9],
+                                             bool inside[3]) {
+    const float dt = (float)prm.dt;
+    const float pad = (float)(2.0 * prm.dx), hi = (float)(prm.grid_lim - 2.0 * prm.dx);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float t = xp[k] + dt * vpost[k];
+        inside[k] = (t >= pad) && (t <= hi);
+        vt[k] = a.vb[k] + (inside[k] ? dt * a.xb[k] : 0.0f);
+    }
+    // C' enters F' = (I + dt C') F: Cbar += dt Fbar' F^T
+    float FbFt[9];
+    mmt3(a.Fb, Fpre, FbFt);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Ct[k] = a.Cb[k] + dt * FbFt[k];
+}
+
+// ---------------------------------------------------------------- k_adj_scatter
+// Adjoint of v' = sum w v_i, C' = K sum w v_i dpos^T and lap' = sum L gd_i:
+// acc[i].xyz += w (vbar + K Cbar dpos), acc[i].w += L lapbar.  The quadratic
+// stencil is contained in the cubic one (per axis the quadratic node o_q is
+// the cubic node o_c = o_q + s with s = 1 when frac(X) >= 0.5, else 0), so
+// one float4 atomic per cubic node carries both.
+__global__ void __launch_bounds__(256) k_adj_scatter(const pm_params prm, const Parts pre, const Parts post,
+                                                     const pm_state_adj ain, float4 *__restrict__ acc) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pre.n) return;
+    const long long ps = pre.ps;
+    const int ng = prm.n_grid;
+    const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
+    const float K = (float)(4.0 * prm.inv_dx * prm.inv_dx);
+    const float L2 = (float)(prm.inv_dx * prm.inv_dx);
+    float xp[3], vpost[3], F[9];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        xp[k] = pre.x[k * ps + p];
+        vpost[k] = post.v[k * ps + p];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = pre.F[k * ps + p];
+    AdjIn a;
+    load_adj(ain, p, a);
+    float vt[3], Ct[9];
+    bool inside[3];
+    g2p_tail_adj(prm, xp, vpost, F, a, vt, Ct, inside);
+    Quad q;
+    quad_weights(xp, inv_dx, ng, q);
+    Cubic c;
+    cubic_weights(xp, inv_dx, ng, c);
+    int sh[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) sh[k] = q.b[k] - c.b[k];   // 0 or 1
+    const float lb = a.lapb * L2;
+    for (int ox = 0; ox < 4; ++ox) {
+        const int qx = ox - sh[0];
+        for (int oy = 0; oy < 4; ++oy) {
+            const int qy = oy - sh[1];
+            const float ab = c.w2[ox][0] * c.w[oy][1] + c.w[ox][0] * c.w2[oy][1];
+            const float e = c.w[ox][0] * c.w[oy][1];
+#pragma unroll
+            for (int oz = 0; oz < 4; ++oz) {
+                const int qz = oz - sh[2];
+                const float Lw = ab * c.w[oz][2] + e * c.w2[oz][2];
+                float4 val = make_float4(0.0f, 0.0f, 0.0f, Lw * lb);
+                if (qx >= 0 && qx < 3 && qy >= 0 && qy < 3 && qz >= 0 && qz < 3) {
+                    const float wk = q.w[qx][0] * q.w[qy][1] * q.w[qz][2];
+                    const float dp[3] = {((float)qx - q.fx[0]) * dx, ((float)qy - q.fx[1]) * dx,
+                                         ((float)qz - q.fx[2]) * dx};
+                    val.x = wk * (vt[0] + K * (Ct[0] * dp[0] + Ct[1] * dp[1] + Ct[2] * dp[2]));
+                    val.y = wk * (vt[1] + K * (Ct[3] * dp[0] + Ct[4] * dp[1] + Ct[5] * dp[2]));
+                    val.z = wk * (vt[2] + K * (Ct[6] * dp[0] + Ct[7] * dp[1] + Ct[8] * dp[2]));
+                }
+                if (val.x != 0.0f || val.y != 0.0f || val.z != 0.0f || val.w != 0.0f)
+                    atomicAdd(&acc[node_of(c.b[0] + ox, c.b[1] + oy, c.b[2] + oz, ng)], val);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- k_adj_grid
+// Grid-update adjoint over the recorded active blocks.  Forward (active node,
+// m > 1e-12): v = (mv / m + dt g) * damp; gd = sum wd / sum w when sum w >
+// 1e-12.  Writes A = {mvbar, mbar}, B = {sumwd bar, sumw bar, gd, 0} and
+// clears acc.
+__global__ void __launch_bounds__(256) k_adj_grid(const pm_params prm, const int *__restrict__ blocks,
+                                                  const TapeHead *head, const float4 *__restrict__ gvel,
+                                                  const float *__restrict__ ggd, const float *__restrict__ gsw,
+                                                  float4 *__restrict__ acc, float4 *__restrict__ A,
+                                                  float4 *__restrict__ B, long long n_blocks) {
+    const long long nact = min((long long)head->n_active, n_blocks);
+    const long long items = nact * 64;
+    const int ng = prm.n_grid, nbs = (ng + kBlockEdge - 1) / kBlockEdge;
+    const float dt = (float)prm.dt, damp = (float)prm.grid_damp;
+    const float dg[3] = {damp * dt * (float)prm.gravity[0], damp * dt * (float)prm.gravity[1],
+                         damp * dt * (float)prm.gravity[2]};
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int b = blocks[it >> 6];
+        const int l = (int)(it & 63);
+        const int bx = b / (nbs * nbs), by = (b / nbs) % nbs, bz = b % nbs;
+        const int ix = bx * kBlockEdge + (l >> 4), iy = by * kBlockEdge + ((l >> 2) & 3), iz = bz * kBlockEdge + (l & 3);
+        if (ix >= ng || iy >= ng || iz >= ng) continue;
+        const long long node = ((long long)ix * ng + iy) * ng + iz;
+        const float4 ab = acc[node];
+        acc[node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float4 gv = gvel[node];
+        float4 ao = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (gv.w > 1e-12f) {
+            const float im = 1.0f / gv.w;
+            const float u0 = damp * ab.x, u1 = damp * ab.y, u2 = damp * ab.z;
+            ao.x = u0 * im; ao.y = u1 * im; ao.z = u2 * im;
+            // mv / m = v / damp - dt g:  mbar = -damp vbar . (mv/m) / m
+            ao.w = -(ab.x * (gv.x - dg[0]) + ab.y * (gv.y - dg[1]) + ab.z * (gv.z - dg[2])) * im;
+        }
+        A[node] = ao;
+        const float sw = gsw[node], gd = ggd[node];
+        float4 bo = make_float4(0.0f, 0.0f, gd, 0.0f);
+        if (sw > 1e-12f) {
+            bo.x = ab.w / sw;
+            bo.y = -ab.w * gd / sw;
+        }
+        B[node] = bo;
+    }
+}
+
+// ---------------------------------------------------------------- constitutive
+struct Cons {
+    float F[9], V[9], S[3], R[9], lamC[3];
+    float J, Jraw, tdev[9], tv;
+    bool dmg;
+    float sig[9], ev[3], Q[9], sp[9], A[9], M[9], A0[9];
+    float phi, drive, Dh0, Dh1, d0, lap, arg, cc, u, dn, d1, g, vdeg, res, sc, zeta, l0;
+    bool allow;
+};
+
+// Forward constitutive update without f_clamp and interface particles, as
+// the forward kernel computes it, keeping the intermediates.
+__device__ __forceinline__ void cons_forward(const pm_params &prm, const Parts &P, long long p, bool do_damage,
+                                             Cons &c, float tau[9]) {
+    const long long ps = P.ps;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) c.F[k] = P.F[k * ps + p];
+    float Cg[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Cg[3 * i + j] = c.F[i] * c.F[j] + c.F[3 + i] * c.F[3 + j] + c.F[6 + i] * c.F[6 + j];
+    sym_eig3<5>(Cg, c.lamC, c.V);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) c.S[i] = sqrtf(c.lamC[i] < 1e-12f ? 1e-12f : c.lamC[i]);
+    float W[9];
+    mm3(c.F, c.V, W);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float nr = sqrtf(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]) + 1e-12f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) W[3 * i + j] = W[3 * i + j] / nr;
+    }
+    mmt3(W, c.V, c.R);
+    c.Jraw = c.S[0] * c.S[1] * c.S[2];
+    c.J = c.Jraw < 1e-6f ? 1e-6f : c.Jraw;
+    const float mu = P.mu[p], lam = P.lam[p];
+    {
+        float FmR[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) FmR[k] = (2.0f * mu) * (c.F[k] - c.R[k]);
+        mmt3(FmR, c.F, c.tdev);
+    }
+    c.tv = lam * (c.J - 1.0f) * c.J;
+    c.dmg = do_damage;
+    c.d0 = P.d[p];
+    c.Dh0 = P.D_hist[p];
+    c.d1 = c.d0;
+    c.Dh1 = c.Dh0;
+    c.allow = P.allow[p] != 0;
+    if (do_damage) {
+        float sg[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sg[k] = (c.tdev[k] + ((k % 4 == 0) ? c.tv : 0.0f)) / c.J;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) c.sig[3 * i + j] = 0.5f * (sg[3 * i + j] + sg[3 * j + i]);
+        sym_eig3<5>(c.sig, c.ev, c.Q);
+        {
+            float ED[9];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float e = c.ev[j] < 0.0f ? 0.0f : c.ev[j];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) ED[3 * i + j] = c.Q[3 * i + j] * e;
+            }
+            mmt3(ED, c.Q, c.sp);
+        }
+        {
+            float RA[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) c.A0[k] = P.A0[k * ps + p];
+            mm3(c.R, c.A0, RA);
+            mmt3(RA, c.R, c.A);
+        }
+        mm3(c.A, c.sp, c.M);
+        const float trMM = (c.M[0] * c.M[0] + c.M[1] * c.M[3] + c.M[2] * c.M[6]) +
+                           (c.M[3] * c.M[1] + c.M[4] * c.M[4] + c.M[5] * c.M[7]) +
+                           (c.M[6] * c.M[2] + c.M[7] * c.M[5] + c.M[8] * c.M[8]);
+        c.sc = P.sigma_c[p];
+        c.phi = trMM / (c.sc * c.sc);
+        c.zeta = P.zeta[p];
+        c.drive = c.zeta * relu_f(c.phi - 1.0f);
+        c.Dh1 = c.drive > c.Dh0 ? c.drive : c.Dh0;
+        c.l0 = P.l0[p];
+        c.lap = P.lap[p];
+        const float resist = c.d0 - (c.l0 * c.l0) * c.lap;
+        c.arg = (1.0f - c.d0) * c.Dh1 - resist;
+        const float ddot = relu_f(c.arg);
+        const float dt_dmg = (float)(prm.dt * (double)prm.damage_every);
+        c.cc = dt_dmg / P.eta[p];
+        c.u = c.d0 + c.cc * ddot;
+        c.dn = c.u < 0.0f ? 0.0f : (c.u > 1.0f ? 1.0f : c.u);
+        if (c.allow) c.d1 = c.dn > c.d0 ? c.dn : c.d0;
+    }
+    c.res = P.residual[p];
+    const float omd = 1.0f - c.d1;
+    c.g = (omd * omd) * (1.0f - c.res) + c.res;
+    c.vdeg = (c.J >= 1.0f) ? c.g : 1.0f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) tau[k] = c.g * c.tdev[k] + ((k % 4 == 0) ? c.vdeg * c.tv : 0.0f);
+}
+
+// Adjoint of the eigen split sp = Q diag(relu(e)) Q^T of the symmetric sig:
+// sigbar = Q (Gam o (Q^T sym(spbar) Q)) Q^T with Gam_ii = [e_i > 0] and
+// Gam_ij = (relu(e_i) - relu(e_j)) / (e_i - e_j), guarded for near-equal
+// eigenvalues by the mean of the diagonal terms (Daleckii-Krein formula for
+// the isotropic matrix function relu).
+__device__ __forceinline__ void eigsplit_adj(const float ev[3], const float Q[9], const float spb[9], float sgb[9]) {
+    float Sy[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Sy[3 * i + j] = 0.5f * (spb[3 * i + j] + spb[3 * j + i]);
+    float T[9], Bq[9];
+    mm3(Sy, Q, T);                       // Sy Q
+    // Bq = Q^T (Sy Q)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Bq[3 * i + j] = Q[i] * T[j] + Q[3 + i] * T[3 + j] + Q[6 + i] * T[6 + j];
+    float gd[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) gd[i] = ev[i] >= 0.0f ? 1.0f : 0.0f;   // clamp(min=0) passes at 0
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            float gm;
+            if (i == j) {
+                gm = gd[i];
+            } else {
+                const float de = ev[i] - ev[j];
+                const float scale = fabsf(ev[i]) + fabsf(ev[j]);
+                if (fabsf(de) > 1e-6f * scale && fabsf(de) > 1e-30f)
+                    gm = (relu_f(ev[i]) - relu_f(ev[j])) / de;
+                else
+                    gm = 0.5f * (gd[i] + gd[j]);
+            }
+            Bq[3 * i + j] *= gm;
+        }
+    // sgb = Q Bq Q^T
+    mm3(Q, Bq, T);
+    mmt3(T, Q, sgb);
+}
+
+struct ConsAdj {
+    float Fb[9], mub, lamb, scb, A0b[9], d0b, lapb, Dh0b;
+};
+
+// Reverse of cons_forward given taubar, the adjoint of the updated damage d1
+// and of the updated history D_hist1.
+__device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, const float lam, const float taub[9],
+                                             float d1b, float Dh1b, ConsAdj &o) {
+    const float trt = taub[0] + taub[4] + taub[8];
+    float gb = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gb += taub[k] * c.tdev[k];
+    if (c.J >= 1.0f) gb += c.tv * trt;
+    float tdevb[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) tdevb[k] = c.g * taub[k];
+    float tvb = c.vdeg * trt;
+    d1b += gb * (-2.0f * (1.0f - c.d1) * (1.0f - c.res));
+    float Jb = 0.0f, Rb[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        Rb[k] = 0.0f;
+        o.A0b[k] = 0.0f;
+    }
+    o.d0b = 0.0f;
+    o.lapb = 0.0f;
+    o.Dh0b = 0.0f;
+    o.scb = 0.0f;
+    if (c.dmg) {
+        // torch.maximum sends half of the adjoint to each operand on a tie;
+        // clamp passes it on [lo, hi] inclusive; relu only where the input > 0
+        float dnb = 0.0f;
+        if (!c.allow || c.dn < c.d0) {
+            o.d0b += d1b;
+        } else if (c.dn > c.d0) {
+            dnb = d1b;
+        } else {
+            dnb = 0.5f * d1b;
+            o.d0b += 0.5f * d1b;
+        }
+        float ddotb = 0.0f;
+        if (c.u >= 0.0f && c.u <= 1.0f) {
+            o.d0b += dnb;
+            ddotb = c.cc * dnb;
+        }
+        float Dh1t = Dh1b;
+        if (c.arg > 0.0f) {
+            Dh1t += (1.0f - c.d0) * ddotb;
+            o.d0b += -(c.Dh1 + 1.0f) * ddotb;
+            o.lapb += (c.l0 * c.l0) * ddotb;
+        }
+        float driveb = 0.0f;
+        if (c.drive > c.Dh0) {
+            driveb = Dh1t;
+        } else if (c.drive < c.Dh0) {
+            o.Dh0b += Dh1t;
+        } else {
+            driveb = 0.5f * Dh1t;
+            o.Dh0b += 0.5f * Dh1t;
+        }
+        const float phib = (c.phi > 1.0f) ? c.zeta * driveb : 0.0f;
+        if (phib != 0.0f) {
+            const float isc2 = 1.0f / (c.sc * c.sc);
+            o.scb += -2.0f * c.phi / c.sc * phib;
+            float Mb[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) Mb[3 * i + j] = 2.0f * phib * isc2 * c.M[3 * j + i];
+            float Ab[9], spb[9];
+            mmt3(Mb, c.sp, Ab);                    // Mb sp^T
+            // spb = A^T Mb
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    spb[3 * i + j] = c.A[i] * Mb[j] + c.A[3 + i] * Mb[3 + j] + c.A[6 + i] * Mb[6 + j];
+            // A = R A0 R^T:  Rb += Ab R A0^T + Ab^T R A0;  A0b += R^T Ab R
+            {
+                float T1[9], T2[9], RA0t[9], RA0[9];
+                mmt3(c.R, c.A0, RA0t);             // R A0^T
+                mm3(c.R, c.A0, RA0);               // R A0
+                mm3(Ab, RA0t, T1);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        T2[3 * i + j] = Ab[i] * RA0[j] + Ab[3 + i] * RA0[3 + j] + Ab[6 + i] * RA0[6 + j];   // Ab^T RA0
+#pragma unroll
+                for (int k = 0; k < 9; ++k) Rb[k] += T1[k] + T2[k];
+                float AbR[9];
+                mm3(Ab, c.R, AbR);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        o.A0b[3 * i + j] = c.R[i] * AbR[j] + c.R[3 + i] * AbR[3 + j] + c.R[6 + i] * AbR[6 + j];
+            }
+            float sgb[9];
+            eigsplit_adj(c.ev, c.Q, spb, sgb);
+            // sig = sym(tdev + tv I) / J
+            const float iJ = 1.0f / c.J;
+            float dots = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                tdevb[k] += sgb[k] * iJ;
+                dots += sgb[k] * c.sig[k];
+            }
+            tvb += (sgb[0] + sgb[4] + sgb[8]) * iJ;
+            Jb += -dots * iJ;
+        }
+    } else {
+        o.d0b += d1b;
+        o.Dh0b += Dh1b;
+    }
+    // tv = lam (J - 1) J
+    o.lamb = tvb * (c.J - 1.0f) * c.J;
+    Jb += tvb * lam * (2.0f * c.J - 1.0f);
+    // tdev = 2 mu (F - R) F^T
+    float FmR[9], FmRFt[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) FmR[k] = c.F[k] - c.R[k];
+    mmt3(FmR, c.F, FmRFt);
+    float mub = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) mub += tdevb[k] * FmRFt[k];
+    o.mub = 2.0f * mub;
+    float TF[9], TtFmR[9];
+    mm3(tdevb, c.F, TF);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            TtFmR[3 * i + j] = tdevb[i] * FmR[j] + tdevb[3 + i] * FmR[3 + j] + tdevb[6 + i] * FmR[6 + j];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        o.Fb[k] = (2.0f * mu) * (TF[k] + TtFmR[k]);
+        Rb[k] += -(2.0f * mu) * TF[k];
+    }
+    // J = max(S0 S1 S2, 1e-6); S = sqrt(max(lamC, 1e-12))
+    float Sb[3] = {0.0f, 0.0f, 0.0f};
+    if (c.Jraw > 1e-6f) {
+        Sb[0] = Jb * c.S[1] * c.S[2];
+        Sb[1] = Jb * c.S[0] * c.S[2];
+        Sb[2] = Jb * c.S[0] * c.S[1];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (!(c.lamC[i] > 1e-12f)) Sb[i] = 0.0f;
+    // polar F = R U: Fbar += R V (G + diag(Sbar)) V^T with
+    // G_ij = (B_ij - B_ji) / (S_i + S_j), B = V^T R^T Rbar V
+    float RtRb[9], T[9], Bm[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            RtRb[3 * i + j] = c.R[i] * Rb[j] + c.R[3 + i] * Rb[3 + j] + c.R[6 + i] * Rb[6 + j];
+    mm3(RtRb, c.V, T);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Bm[3 * i + j] = c.V[i] * T[j] + c.V[3 + i] * T[3 + j] + c.V[6 + i] * T[6 + j];
+    float G[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            if (i == j) {
+                G[3 * i + j] = Sb[i];
+            } else {
+                float den = c.S[i] + c.S[j];
+                den = den < 1e-6f ? 1e-6f : den;
+                G[3 * i + j] = (Bm[3 * i + j] - Bm[3 * j + i]) / den;
+            }
+        }
+    float RV[9], RVG[9], Fp[9];
+    mm3(c.R, c.V, RV);
+    mm3(RV, G, RVG);
+    mmt3(RVG, c.V, Fp);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o.Fb[k] += Fp[k];
+}
+
+// ---------------------------------------------------------------- k_adj_particle
+__global__ void __launch_bounds__(128) k_adj_particle(const pm_params prm, const Parts pre, const Parts post,
+                                                      const pm_state_adj ain, const pm_state_adj aout,
+                                                      const pm_param_adj grads, const TapeHead *head,
+                                                      const float4 *__restrict__ gvel, const float4 *__restrict__ A,
+                                                      const float4 *__restrict__ B) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pre.n) return;
+    const long long ps = pre.ps;
+    const int ng = prm.n_grid;
+    const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx, dt = (float)prm.dt;
+    const float K = (float)(4.0 * prm.inv_dx * prm.inv_dx);
+    const float L2 = (float)(prm.inv_dx * prm.inv_dx);
+    float xp[3], vpost[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        xp[k] = pre.x[k * ps + p];
+        vpost[k] = post.v[k * ps + p];
+    }
+    AdjIn a;
+    load_adj(ain, p, a);
+    float xb[3] = {0.0f, 0.0f, 0.0f};
+    bool inside[3];
+    // ---- G2P adjoint, position part (weights and dpos depend on x)
+    {
+        float F[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) F[k] = pre.F[k * ps + p];
+        float vt[3], Ct[9];
+        g2p_tail_adj(prm, xp, vpost, F, a, vt, Ct, inside);
+        QuadD q;
+        quad_weights_d(xp, inv_dx, ng, q);
+        for (int ox = 0; ox < 3; ++ox)
+            for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) {
+                    const float4 g = __ldg(&gvel[node_of(q.b[0] + ox, q.b[1] + oy, q.b[2] + oz, ng)]);
+                    const float wx = q.w[ox][0], wy = q.w[oy][1], wz = q.w[oz][2];
+                    const float wk = wx * wy * wz;
+                    const float dp[3] = {((float)ox - q.fx[0]) * dx, ((float)oy - q.fx[1]) * dx,
+                                         ((float)oz - q.fx[2]) * dx};
+                    const float Cd0 = Ct[0] * dp[0] + Ct[1] * dp[1] + Ct[2] * dp[2];
+                    const float Cd1 = Ct[3] * dp[0] + Ct[4] * dp[1] + Ct[5] * dp[2];
+                    const float Cd2 = Ct[6] * dp[0] + Ct[7] * dp[1] + Ct[8] * dp[2];
+                    const float wbar = vt[0] * g.x + vt[1] * g.y + vt[2] * g.z + K * (g.x * Cd0 + g.y * Cd1 + g.z * Cd2);
+                    xb[0] += wbar * inv_dx * q.dw[ox][0] * wy * wz;
+                    xb[1] += wbar * inv_dx * wx * q.dw[oy][1] * wz;
+                    xb[2] += wbar * inv_dx * wx * wy * q.dw[oz][2];
+                    // dpos = node - x: xbar -= K w Cbar^T v_i
+                    xb[0] -= K * wk * (Ct[0] * g.x + Ct[3] * g.y + Ct[6] * g.z);
+                    xb[1] -= K * wk * (Ct[1] * g.x + Ct[4] * g.y + Ct[7] * g.z);
+                    xb[2] -= K * wk * (Ct[2] * g.x + Ct[5] * g.y + Ct[8] * g.z);
+                }
+    }
+    CubicD cw;
+    cubic_weights_d(xp, inv_dx, ng, cw);
+    {
+        const float lb = a.lapb * L2 * inv_dx;
+        for (int ox = 0; ox < 4; ++ox)
+            for (int oy = 0; oy < 4; ++oy)
+#pragma unroll
+                for (int oz = 0; oz < 4; ++oz) {
+                    const float gd = __ldg(&B[node_of(cw.b[0] + ox, cw.b[1] + oy, cw.b[2] + oz, ng)].z);
+                    const float wx = cw.w[ox][0], wy = cw.w[oy][1], wz = cw.w[oz][2];
+                    const float sx = cw.w2[ox][0], sy = cw.w2[oy][1], sz = cw.w2[oz][2];
+                    const float dwx = cw.dw[ox][0], dwy = cw.dw[oy][1], dwz = cw.dw[oz][2];
+                    const float tx = cw.dw2[ox][0], ty = cw.dw2[oy][1], tz = cw.dw2[oz][2];
+                    const float s = gd * lb;
+                    xb[0] += s * (tx * wy * wz + dwx * sy * wz + dwx * wy * sz);
+                    xb[1] += s * (sx * dwy * wz + wx * ty * wz + wx * dwy * sz);
+                    xb[2] += s * (sx * wy * dwz + wx * sy * dwz + wx * wy * tz);
+                }
+    }
+    // ---- constitutive recompute
+    const TapeHead h = *head;
+    const bool do_damage = h.any_allow != 0 && (h.step % (long long)prm.damage_every) == 0;
+    Cons c;
+    float tau[9];
+    cons_forward(prm, pre, p, do_damage, c, tau);
+    float v[3] = {pre.v[p], pre.v[ps + p], pre.v[2 * ps + p]};
+    bool gripped = false;
+    if (pre.grip_tag) {
+        const int gi = pre.grip_tag[p];
+        if (gi >= 0 && gi < prm.n_grips) {
+            gripped = true;
+            const double f = prm.grips[gi].ramp > 0.0 ? fmin(h.time / prm.grips[gi].ramp, 1.0) : 1.0;
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) v[ax] = (float)(prm.grips[gi].vel[ax] * f);
+        }
+    }
+    const float m = pre.mass[p];
+    const float coeff =
+        __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), pre.vol0[p]), 4.0f), inv_dx), inv_dx);
+    float aff[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) aff[k] = coeff * tau[k] + m * pre.C[k * ps + p];
+    const float mv[3] = {m * v[0], m * v[1], m * v[2]};
+    // ---- P2G adjoint (gather)
+    float mvb[3] = {0.0f, 0.0f, 0.0f}, affb[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) affb[k] = 0.0f;
+    {
+        QuadD q;
+        quad_weights_d(xp, inv_dx, ng, q);
+        for (int ox = 0; ox < 3; ++ox)
+            for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) {
+                    const float4 g = __ldg(&A[node_of(q.b[0] + ox, q.b[1] + oy, q.b[2] + oz, ng)]);
+                    const float wx = q.w[ox][0], wy = q.w[oy][1], wz = q.w[oz][2];
+                    const float wk = wx * wy * wz;
+                    const float dp[3] = {((float)ox - q.fx[0]) * dx, ((float)oy - q.fx[1]) * dx,
+                                         ((float)oz - q.fx[2]) * dx};
+                    mvb[0] += wk * g.x; mvb[1] += wk * g.y; mvb[2] += wk * g.z;
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        affb[j] += wk * g.x * dp[j];
+                        affb[3 + j] += wk * g.y * dp[j];
+                        affb[6 + j] += wk * g.z * dp[j];
+                    }
+                    const float c0 = mv[0] + aff[0] * dp[0] + aff[1] * dp[1] + aff[2] * dp[2];
+                    const float c1 = mv[1] + aff[3] * dp[0] + aff[4] * dp[1] + aff[5] * dp[2];
+                    const float c2 = mv[2] + aff[6] * dp[0] + aff[7] * dp[1] + aff[8] * dp[2];
+                    const float wbar = g.x * c0 + g.y * c1 + g.z * c2 + g.w * m;
+                    xb[0] += wbar * inv_dx * q.dw[ox][0] * wy * wz;
+                    xb[1] += wbar * inv_dx * wx * q.dw[oy][1] * wz;
+                    xb[2] += wbar * inv_dx * wx * wy * q.dw[oz][2];
+                    xb[0] -= wk * (aff[0] * g.x + aff[3] * g.y + aff[6] * g.z);
+                    xb[1] -= wk * (aff[1] * g.x + aff[4] * g.y + aff[7] * g.z);
+                    xb[2] -= wk * (aff[2] * g.x + aff[5] * g.y + aff[8] * g.z);
+                }
+    }
+    float d1b = a.db;
+    {
+        for (int ox = 0; ox < 4; ++ox)
+            for (int oy = 0; oy < 4; ++oy)
+#pragma unroll
+                for (int oz = 0; oz < 4; ++oz) {
+                    const float4 g = __ldg(&B[node_of(cw.b[0] + ox, cw.b[1] + oy, cw.b[2] + oz, ng)]);
+                    const float wx = cw.w[ox][0], wy = cw.w[oy][1], wz = cw.w[oz][2];
+                    const float wk = wx * wy * wz;
+                    d1b += wk * g.x;
+                    const float wbar = g.x * c.d1 + g.y;
+                    xb[0] += wbar * inv_dx * cw.dw[ox][0] * wy * wz;
+                    xb[1] += wbar * inv_dx * wx * cw.dw[oy][1] * wz;
+                    xb[2] += wbar * inv_dx * wx * wy * cw.dw[oz][2];
+                }
+    }
+    float taub[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) taub[k] = coeff * affb[k];
+    ConsAdj o;
+    cons_adjoint(c, pre.mu[p], pre.lam[p], taub, d1b, a.Dhb, o);
+    // ---- write the adjoints of the pre-step state
+    const long long os = aout.plane_stride;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        aout.x[k * os + p] = (inside[k] ? a.xb[k] : 0.0f) + xb[k];
+        aout.v[k * os + p] = gripped ? 0.0f : m * mvb[k];
+    }
+    {
+        float Cp[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Cp[k] = post.C[k * ps + p];
+        // F' = (I + dt C') F:  Fbar += (I + dt C')^T Fbar'
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float s = a.Fb[3 * i + j] + dt * (Cp[i] * a.Fb[j] + Cp[3 + i] * a.Fb[3 + j] + Cp[6 + i] * a.Fb[6 + j]);
+                aout.F[(3 * i + j) * os + p] = s + o.Fb[3 * i + j];
+            }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) aout.C[k * os + p] = m * affb[k];
+    aout.d[p] = o.d0b;
+    aout.lap[p] = o.lapb;
+    aout.D_hist[p] = o.Dh0b;
+    const long long gs = grads.plane_stride;
+    if (grads.mu) grads.mu[p] += o.mub;
+    if (grads.lam) grads.lam[p] += o.lamb;
+    if (grads.sigma_c) grads.sigma_c[p] += o.scb;
+    if (grads.A0) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) grads.A0[k * gs + p] += o.A0b[k];
+    }
+}
+
+__global__ void k_tape_head(const Ctrl *ctrl, TapeHead *head) {
+    if (threadIdx.x == 0) {
+        head->n_active = ctrl->n_active;
+        head->any_allow = ctrl->any_allow;
+        head->step = ctrl->step;
+        head->time = ctrl->time;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ tape layout
+TapeLayout make_tape_layout(long long n, int ng, int slots) {
+    TapeLayout T;
+    const size_t A = 256;
+    const long long G = (long long)ng * ng * ng;
+    const int nbs = (ng + kBlockEdge - 1) / kBlockEdge;
+    const long long nb = (long long)nbs * nbs * nbs;
+    (void)n;
+    size_t o = 0;
+    T.head = o;    o = align_up(o + sizeof(TapeHead) * (size_t)(slots > 0 ? slots : 1), A);
+    T.acc = o;     o = align_up(o + 16 * (size_t)G, A);
+    T.adj_q = o;   o = align_up(o + 16 * (size_t)G, A);
+    T.adj_c = o;   o = align_up(o + 16 * (size_t)G, A);
+    T.slot0 = o;
+    size_t s = 0;
+    T.vel = s;     s = align_up(s + 16 * (size_t)G, A);
+    T.gd = s;      s = align_up(s + 4 * (size_t)G, A);
+    T.sw = s;      s = align_up(s + 4 * (size_t)G, A);
+    T.blocks = s;  s = align_up(s + 4 * (size_t)nb, A);
+    T.slot_bytes = s;
+    T.total = o + s * (size_t)(slots > 0 ? slots : 1);
+    T.n_blocks = nb;
+    T.slots = slots;
+    return T;
+}
+
+void record_redirect(const TapeLayout &T, void *tape, int slot, WS &w) {
+    char *b = (char *)tape + T.slot0 + T.slot_bytes * (size_t)slot;
+    w.g_vel = (float4 *)(b + T.vel);
+    w.g_gd = (float *)(b + T.gd);
+    w.g_sw = (float *)(b + T.sw);
+    w.block_list = (int *)(b + T.blocks);
+}
+
+void launch_tape_head(const TapeLayout &T, void *tape, int slot, const WS &w, cudaStream_t s) {
+    TapeHead *h = (TapeHead *)((char *)tape + T.head) + slot;
+    k_tape_head<<<1, 32, 0, s>>>(w.ctrl, h);
+}
+
+void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, const pm_state_adj &ain,
+                    const pm_state_adj &aout, const pm_param_adj &grads, const TapeLayout &T, void *tape, int slot,
+                    cudaStream_t s) {
+    char *base = (char *)tape;
+    char *b = base + T.slot0 + T.slot_bytes * (size_t)slot;
+    const TapeHead *h = (const TapeHead *)(base + T.head) + slot;
+    float4 *acc = (float4 *)(base + T.acc);
+    float4 *Aq = (float4 *)(base + T.adj_q);
+    float4 *Bc = (float4 *)(base + T.adj_c);
+    const float4 *gvel = (const float4 *)(b + T.vel);
+    const float *ggd = (const float *)(b + T.gd);
+    const float *gsw = (const float *)(b + T.sw);
+    const int *blocks = (const int *)(b + T.blocks);
+    const long long n = pre.n;
+    if (n <= 0) return;
+    k_adj_scatter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prm, pre, post, ain, acc);
+    const long long max_items = T.n_blocks * 64;
+    const int gb = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, 148LL * 8));
+    k_adj_grid<<<gb, 256, 0, s>>>(prm, blocks, h, gvel, ggd, gsw, acc, Aq, Bc, T.n_blocks);
+    k_adj_particle<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(prm, pre, post, ain, aout, grads, h, gvel, Aq, Bc);
+}
+
+}  // namespace pm

@@ -98,6 +98,8 @@ size_t pm_struct_size(int32_t which) {
         case 5: return sizeof(pm_grip);
         case 6: return sizeof(pm_collider);
         case 7: return sizeof(pm_batch_layout);
+        case 8: return sizeof(pm_state_adj);
+        case 9: return sizeof(pm_param_adj);
         default: return 0;
     }
 }
@@ -223,6 +225,94 @@ int pm_substep_dev_clock(const pm_params *prm, const pm_particles *P, void *ws, 
                          const pm_clock *dev_clocks, int32_t row, void *stream) {
     if (!dev_clocks || row < 0) return fail(PM_ERR_ARG, "bad device clock table");
     return substep_common(prm, P, ws, ws_bytes, nullptr, dev_clocks, row, stream);
+}
+
+// ------------------------------------------------------------------ adjoint
+static int check_adjoint_params(const pm_params *prm, const pm_particles *P) {
+    if (prm->use_f_clamp) return fail(PM_ERR_ARG, "the adjoint does not support f_clamp");
+    if (prm->n_colliders > 0) return fail(PM_ERR_ARG, "the adjoint does not support colliders");
+    if (P && P->interface_mask) return fail(PM_ERR_ARG, "the adjoint does not support interface particles");
+    return PM_OK;
+}
+
+static int get_tape(void *tape, size_t bytes, long long n, int ng, int slots, int slot, pm::TapeLayout *T) {
+    if (!tape) return fail(PM_ERR_WORKSPACE, "tape is NULL");
+    if (((uintptr_t)tape & 255) != 0) return fail(PM_ERR_WORKSPACE, "tape must be 256-byte aligned");
+    if (slots < 1 || slot < 0 || slot >= slots) return fail(PM_ERR_ARG, "bad tape slot");
+    *T = pm::make_tape_layout(n, ng, slots);
+    if (bytes < T->total) return fail(PM_ERR_WORKSPACE, "tape too small for (n, n_grid, slots)");
+    return PM_OK;
+}
+
+int pm_tape_size(int64_t n, int32_t n_grid, int32_t slots, size_t *bytes) {
+    if (!bytes) return fail(PM_ERR_ARG, "bytes is NULL");
+    if (n < 0 || n_grid < 4 || n_grid > 1024 || slots < 1) return fail(PM_ERR_ARG, "bad n, n_grid or slots");
+    *bytes = pm::make_tape_layout(n, n_grid, slots).total;
+    return PM_OK;
+}
+
+int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32_t slots, void *stream) {
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (n < 0 || n_grid < 4 || n_grid > 1024) return fail(PM_ERR_ARG, "bad n or n_grid");
+    pm::TapeLayout T;
+    if ((rc = get_tape(tape, tape_bytes, n, n_grid, slots, 0, &T))) return rc;
+    if (cudaMemsetAsync(tape, 0, T.total, (cudaStream_t)stream) != cudaSuccess) return cuda_check("pm_tape_init");
+    return cuda_check("pm_tape_init");
+}
+
+int pm_substep_record(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, const pm_clock *clk,
+                      void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
+    if ((rc = check_adjoint_params(prm, P))) return rc;
+    if (!clk) return fail(PM_ERR_ARG, "clock is NULL");
+    pm::WS w;
+    if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
+    pm::TapeLayout T;
+    if ((rc = get_tape(tape, tape_bytes, P->n, prm->n_grid, slots, slot, &T))) return rc;
+    pm::record_redirect(T, tape, slot, w);
+    const pm::Parts parts = pm::make_parts(P);
+    cudaStream_t s = (cudaStream_t)stream;
+    pm::launch_set_clock(*prm, w, *clk, s);
+    if (P->n > 0) {
+        const pm::PlainScenes sc{*prm};
+        pm::launch_keys(sc, w, parts, s);
+        pm::launch_sort(w, P->n, s, w.inv_perm);
+        pm::launch_p2g(sc, parts, w, s);
+        pm::launch_compact(w, s);
+        pm::launch_grid(sc, w, s);
+        pm::launch_g2p(sc, parts, w, s);
+    }
+    pm::launch_tape_head(T, tape, slot, w, s);
+    return cuda_check("pm_substep_record");
+}
+
+static int check_adj(const pm_state_adj *a, long long n) {
+    if (!a) return fail(PM_ERR_ARG, "adjoint state is NULL");
+    if (a->plane_stride < n) return fail(PM_ERR_ARG, "adjoint plane_stride < n");
+    if (!a->x || !a->v || !a->F || !a->C || !a->d || !a->lap || !a->D_hist)
+        return fail(PM_ERR_ARG, "an adjoint state plane is NULL");
+    return PM_OK;
+}
+
+int pm_substep_adjoint(const pm_params *prm, const pm_particles *pre, const pm_particles *post,
+                       const pm_state_adj *adj_in, const pm_state_adj *adj_out, const pm_param_adj *grads,
+                       void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(pre, true)) ||
+        (rc = check_particles(post, true)))
+        return rc;
+    if ((rc = check_adjoint_params(prm, pre))) return rc;
+    if (pre->n != post->n) return fail(PM_ERR_ARG, "pre and post differ in n");
+    if ((rc = check_adj(adj_in, pre->n)) || (rc = check_adj(adj_out, pre->n))) return rc;
+    if (adj_in->x == adj_out->x) return fail(PM_ERR_ARG, "adj_in and adj_out must be distinct");
+    if (!grads || (grads->A0 && grads->plane_stride < pre->n)) return fail(PM_ERR_ARG, "bad parameter gradients");
+    pm::TapeLayout T;
+    if ((rc = get_tape(tape, tape_bytes, pre->n, prm->n_grid, slots, slot, &T))) return rc;
+    pm::launch_adjoint(*prm, pm::make_parts(pre), pm::make_parts(post), *adj_in, *adj_out, *grads, T, tape, slot,
+                       (cudaStream_t)stream);
+    return cuda_check("pm_substep_adjoint");
 }
 
 int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, pm_status_info *out, void *stream) {

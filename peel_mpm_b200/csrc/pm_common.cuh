@@ -114,6 +114,7 @@ struct WS {
     float2 *g_dmg;      // {sum w d, sum w}, zero between substeps
     float4 *g_vel;      // {v.x, v.y, v.z, unused}
     float *g_gd;        // normalised damage field
+    float *g_sw;        // cubic weight sums (recorded for the adjoint; NULL otherwise)
     float4 *payload;    // P2G payload, 5 float4 per particle in sorted order
     const unsigned *sorted_keys;
     const int *perm;
@@ -138,6 +139,7 @@ inline WS make_ws(void *base, const Layout &L) {
     w.g_dmg = (float2 *)(b + L.g_dmg);
     w.g_vel = (float4 *)(b + L.g_vel);
     w.g_gd = (float *)(b + L.g_gd);
+    w.g_sw = nullptr;
     w.payload = (float4 *)(b + L.payload);
     w.passes = L.passes;
     w.n_tiles = L.n_tiles;

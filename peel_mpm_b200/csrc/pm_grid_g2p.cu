@@ -155,8 +155,9 @@ __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
                 }
             }
         }
-        w.g_vel[node] = make_float4(v[0], v[1], v[2], 0.0f);
+        w.g_vel[node] = make_float4(v[0], v[1], v[2], mom.w);   // .w: node mass (read by the adjoint)
         w.g_gd[node] = dmg.y > 1e-12f ? dmg.x / dmg.y : 0.0f;
+        if (w.g_sw) w.g_sw[node] = dmg.y;
     }
 }
 

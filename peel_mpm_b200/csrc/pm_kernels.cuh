@@ -23,6 +23,21 @@ int balanced_range(long long n, int slots, int max_range);
 int resident_slots(const void *kernel, int threads, size_t smem);
 void launch_sym_eig(const float *A, long long n, int sweeps, float *ev, float *V, cudaStream_t s);
 
+// Tape of recorded substeps for the adjoint: a header per slot, three
+// adjoint grids shared by all slots, then per slot {v, m} grid, gd, cubic
+// weight sums and the active block list.
+struct TapeLayout {
+    size_t head, acc, adj_q, adj_c, slot0, vel, gd, sw, blocks, slot_bytes, total;
+    long long n_blocks;
+    int slots;
+};
+TapeLayout make_tape_layout(long long n, int ng, int slots);
+void record_redirect(const TapeLayout &T, void *tape, int slot, WS &w);
+void launch_tape_head(const TapeLayout &T, void *tape, int slot, const WS &w, cudaStream_t s);
+void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, const pm_state_adj &ain,
+                    const pm_state_adj &aout, const pm_param_adj &grads, const TapeLayout &T, void *tape, int slot,
+                    cudaStream_t s);
+
 // Argument checks and error reporting of the C ABI (pm_capi.cu), shared with
 // the other entry-point files.
 int report_error(int code, const char *msg);
