@@ -1,13 +1,30 @@
-"""Throughput of the AnisoMPM substep on B200: particle-steps/s.
+"""Throughput of the AnisoMPM substep on B200: particle-steps/s, for the plain,
+batched and differentiable forms.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--form all|plain|batched|adjoint] [--fd-dirs D]
 
-Workload: the 1,048,576-particle slab on a 128^3 grid (seeded synthetic
-scene: vMF fibers about x with kappa=20, log-normal E, sigma_c U(180,220),
-initial damage U(0,0.05), bottom clamped, top edge pulled at 1 m/s,
-dt = 5e-5).  A step is one substep of the whole scene.  The particle state
-(~290 MB with its grids) is larger than L2, so no flush is needed between
-steps.
+Headline workload (``value``): the plain form on the 1,048,576-particle slab on
+a 128^3 grid (seeded synthetic scene: vMF fibers about x with kappa=20,
+log-normal E, sigma_c U(180,220), initial damage U(0,0.05), bottom clamped,
+top edge pulled at 1 m/s, dt = 5e-5).  A step is one substep of the whole
+scene, replayed from a captured CUDA graph of up to 100 substeps.  The
+particle state (~290 MB with its grids) is larger than L2, so no flush is
+needed between steps.
+
+Beside it, in the same JSON line:
+  batched     -- 64 independent scenes (log-uniform 4k-256k particles, grids
+                 32^3-128^3, seeded) advanced by BatchedAnisoMPM.run_frame,
+                 against the same 64 scenes advanced one after another by
+                 AnisoMPM.run_frame (graph-captured too); aggregate
+                 particle-steps/s of both and their ratio.
+  fwd_adjoint -- differentiable.rollout on the 1M slab, 100 substeps with
+                 checkpoints every 10: forward time, forward+backward time and
+                 their ratio; gradients with respect to E, fibers, sigma_c and
+                 v0 of the mean squared distance to the final positions of a
+                 run with E*1.2, fibers rotated 15 degrees about z and
+                 sigma_c*0.8, with a central-difference check along random
+                 directions.
 
 Arms:
   ours       -- the sm_100a path.  ``value``: particle state resident in HBM,
@@ -53,8 +70,10 @@ BYTES_PER_NODE = 80
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--form", default="all", choices=["all", "plain", "batched", "adjoint"])
+    ap.add_argument("--fd-dirs", type=int, default=32, help="finite-difference directions of the adjoint check")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -80,6 +99,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0:   # sampling has started
+                time.sleep(0.02)
         except (OSError, ValueError):
             self.proc = None
         return self
@@ -218,6 +240,141 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_frames(sim, steps, t0, chunk=100):
+    """``steps`` substeps as graph replays of up to ``chunk`` substeps."""
+    done = 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        sim.run_frame(k, t0 + done * sim.dt)
+        done += k
+
+
+def bench_batched(torch, device, seed=0, n_sub=20, reps=3):
+    """BatchedAnisoMPM on 64 seeded scenes vs the same scenes one by one."""
+    import peel_mpm_b200 as pm
+    from peel_mpm_b200 import scenes
+    scs = scenes.batch_scenes(seed=seed)
+
+    def build(sc):
+        sim = pm.AnisoMPM(n_grid=sc.n_grid, grid_lim=sc.grid_lim, dt=sc.dt, gravity=tuple(sc.gravity),
+                          grid_damp=sc.grid_damp, f_clamp=sc.f_clamp, damage_every=sc.damage_every,
+                          device=device)
+        scenes.apply_scene(sim, sc, pm.grip_bc, None, torch)
+        return sim
+
+    solo = [build(sc) for sc in scs]
+    batch = pm.BatchedAnisoMPM([build(sc) for sc in scs])
+    total = sum(sc.n for sc in scs)
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(2):
+        batch.run_frame(n_sub, 0.0)
+        for sim in solo:
+            sim.run_frame(n_sub, 0.0)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for r in range(reps):
+        batch.run_frame(n_sub, [(2 + r) * n_sub * sc.dt for sc in scs])
+    e1.record(s)
+    torch.cuda.synchronize()
+    tb = e0.elapsed_time(e1) / reps
+    e0.record(s)
+    for r in range(reps):
+        for sim, sc in zip(solo, scs):
+            sim.run_frame(n_sub, (2 + r) * n_sub * sc.dt)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ts = e0.elapsed_time(e1) / reps
+    st = batch.status()
+    passes = _batch_passes(scs)
+    return {"value": total * n_sub / (tb * 1e-3), "unit": UNIT,
+            "sequential_value": total * n_sub / (ts * 1e-3), "speedup_vs_sequential": ts / tb,
+            "ms_per_substep": tb / n_sub, "sequential_ms_per_substep": ts / n_sub,
+            "scenes": len(scs), "particles": total, "grids": sorted({sc.n_grid for sc in scs}),
+            "substeps_per_frame": n_sub, "frames": reps,
+            "gpu_launches_per_substep": 7 + 3 * passes,
+            "nonfinite": sum(x["nonfinite"] for x in st),
+            "what": "64 scenes, log-uniform 4k-256k particles, one BatchedAnisoMPM.run_frame per frame (one CUDA "
+                    "graph) vs 64 AnisoMPM.run_frame calls (one CUDA graph each)"}
+
+
+def _batch_passes(scs):
+    from peel_mpm_b200 import _lib
+    return _lib.batch_workspace_layout([sc.n for sc in scs], [sc.n_grid for sc in scs]).ws.sort_passes
+
+
+def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
+    """Forward and forward+backward of differentiable.rollout on the 1M slab."""
+    import math
+    from peel_mpm_b200 import differentiable as dfx
+    sim, sc = build_sim(torch, device, seed=0)
+    dev = sim.device
+    f32 = torch.float32
+    S0 = sim._S.clone()
+    step0 = sim._step
+    t = math.radians(15.0)
+    rz = torch.tensor([[math.cos(t), -math.sin(t), 0.0], [math.sin(t), math.cos(t), 0.0], [0.0, 0.0, 1.0]],
+                      device=dev)
+    E0 = torch.tensor(sc.E, dtype=f32, device=dev)
+    fib0 = torch.tensor(sc.fibers, dtype=f32, device=dev)
+    sig0 = torch.tensor(sc.sigma_c, dtype=f32, device=dev)
+    v00 = torch.zeros(sc.n, 3, dtype=f32, device=dev)
+
+    def forward(E, fib, sig, v0):
+        sim._S.copy_(S0)
+        sim._step = step0
+        mu, lam, A0 = dfx.material(E, sc.nu, fib, sc.alpha)
+        return dfx.rollout(sim, n_steps, mu=mu, lam=lam, sigma_c=sig, A0=A0, v0=v0, checkpoint_every=every)
+
+    with torch.no_grad():
+        target = forward(E0 * 1.2, fib0 @ rz.t(), sig0 * 0.8, v00).clone()
+    s = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    res = None
+    for rep in range(3):                      # the first two warm up (graph capture, allocations)
+        E = E0.clone().requires_grad_(True)
+        fib = fib0.clone().requires_grad_(True)
+        sig = sig0.clone().requires_grad_(True)
+        v0 = v00.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        ev[0].record(s)
+        xT = forward(E, fib, sig, v0)
+        loss = ((xT - target) ** 2).sum(1).mean()
+        ev[1].record(s)
+        loss.backward()
+        ev[2].record(s)
+        torch.cuda.synchronize()
+        res = (ev[0].elapsed_time(ev[1]), ev[0].elapsed_time(ev[2]), E.grad, fib.grad, sig.grad, v0.grad,
+               float(loss.detach()))
+    fwd_ms, tot_ms, gE, gF, gS, gV, L0 = res
+    # central differences of the same float32 forward along random directions
+    gen = torch.Generator(device=dev).manual_seed(0)
+    errs = []
+    eps = 1e-3
+    with torch.no_grad():
+        for k in range(fd_dirs):
+            dE = E0 * torch.randn(E0.shape, device=dev, generator=gen)
+            dF = torch.randn(fib0.shape, device=dev, generator=gen)
+            dS = sig0 * torch.randn(sig0.shape, device=dev, generator=gen)
+            dV = torch.randn(v00.shape, device=dev, generator=gen)
+            lp = float(((forward(E0 + eps * dE, fib0 + eps * dF, sig0 + eps * dS, v00 + eps * dV) - target) ** 2)
+                       .sum(1).mean())
+            lm = float(((forward(E0 - eps * dE, fib0 - eps * dF, sig0 - eps * dS, v00 - eps * dV) - target) ** 2)
+                       .sum(1).mean())
+            fd = (lp - lm) / (2 * eps)
+            an = float((gE * dE).sum() + (gF * dF).sum() + (gS * dS).sum() + (gV * dV).sum())
+            errs.append(abs(an - fd) / max(abs(fd), 1e-30))
+    errs = np.array(errs) if errs else np.zeros(1)
+    return {"forward_ms": fwd_ms, "forward_backward_ms": tot_ms, "ratio": tot_ms / fwd_ms,
+            "value": sc.n * n_steps / (tot_ms * 1e-3), "unit": UNIT + " (forward+backward)",
+            "substeps": n_steps, "checkpoint_every": every, "particles": sc.n, "loss": L0,
+            "grad_norms": {"E": float(gE.norm()), "fibers": float(gF.norm()), "sigma_c": float(gS.norm()),
+                           "v0": float(gV.norm())},
+            "fd_check": {"directions": fd_dirs, "eps": eps, "median_rel_err": float(np.median(errs)),
+                         "max_rel_err": float(errs.max()), "frac_below_1e-3": float((errs < 1e-3).mean()),
+                         "forward": "the same float32 rollout"}}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -245,8 +402,9 @@ def run_ours(args):
     sim, sc = build_sim(torch, device, seed=rank)
     n = sim.n
     t0 = 0.0
+    chunk = min(100, args.steps)
     for i in range(args.warmup):
-        sim.substep(t0 + i * sim.dt)
+        sim.run_frame(chunk, t0)
     torch.cuda.synchronize()
     barrier()
 
@@ -256,8 +414,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         e0.record(s)
-        for i in range(args.steps):
-            sim.substep(t0 + (args.warmup + i) * sim.dt)
+        run_frames(sim, args.steps, t0, chunk)
         e1.record(s)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -301,7 +458,7 @@ def run_ours(args):
     alg = p2g_bytes if dom == "p2g" else g2p_bytes
     achieved = alg / (kt[dom] * 1e-3) / 1e9
     step_bytes = n * BYTES_PER_PARTICLE + n_active * BYTES_PER_NODE
-    roof = {"bound": "hbm", "kernel": "k_p2g (fused constitutive + P2G)" if dom == "p2g" else "k_g2p",
+    roof = {"bound": "hbm", "kernel": "k_stress + k_scatter (constitutive + P2G)" if dom == "p2g" else "k_g2p",
             "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
             "traffic": None, "algorithmic_bytes_per_launch": alg,
             "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
@@ -309,20 +466,28 @@ def run_ours(args):
                            "frac": step_bytes / (ms / args.steps * 1e-3) / 1e9 / hbm,
                            "bytes_per_step": step_bytes}}
 
+    forms = {}
+    if rank == 0 and args.form in ("all", "batched"):
+        forms["batched"] = bench_batched(torch, device)
+    if rank == 0 and args.form in ("all", "adjoint"):
+        forms["fwd_adjoint"] = bench_adjoint(torch, device, fd_dirs=args.fd_dirs)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
 
-    launches_per_step = 1 + 2 + 3 * sim_passes(sim) + 3
+    launches_per_step = 7 + 3 * sim_passes(sim)   # clock, keys, 3 per radix pass, stress, scatter, compact, grid, g2p
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "plain AnisoMPM substep, 1,048,576 particles, 128^3 grid (seeded slab)",
                            "particles": n, "n_grid": sim.n_grid, "dt": sim.dt, "parallelism": f"replicas{world}",
-                           "l2": "inputs larger than L2 (particle state ~290 MB)"},
+                           "l2": "inputs larger than L2 (particle state ~290 MB)",
+                           "graph_substeps": chunk},
                 "clocks": clocks.summary(), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches_per_step * args.steps, "status": st}
+        line.update(forms)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
