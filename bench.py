@@ -73,7 +73,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--form", default="all", choices=["all", "plain", "batched", "adjoint"])
-    ap.add_argument("--fd-dirs", type=int, default=32, help="finite-difference directions of the adjoint check")
+    ap.add_argument("--fd-dirs", type=int, default=0,
+                    help="central-difference directions of the adjoint check on the float32 forward (the 100-substep "
+                         "rollout crosses fracture, where the gradient is ill-conditioned; the float64 check at "
+                         "16k particles is in tests/test_gpu_adjoint.py)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -347,6 +350,18 @@ def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
         res = (ev[0].elapsed_time(ev[1]), ev[0].elapsed_time(ev[2]), E.grad, fib.grad, sig.grad, v0.grad,
                float(loss.detach()))
     fwd_ms, tot_ms, gE, gF, gS, gV, L0 = res
+    # the plain forward of the same 100 substeps (no checkpoints, no tape), for the ratio
+    plain = []
+    for rep in range(3):
+        sim._S.copy_(S0)
+        sim._step = step0
+        torch.cuda.synchronize()
+        ev[0].record(s)
+        run_frames(sim, n_steps, 0.0, chunk=n_steps)
+        ev[1].record(s)
+        torch.cuda.synchronize()
+        plain.append(ev[0].elapsed_time(ev[1]))
+    plain_ms = min(plain[1:])
     # central differences of the same float32 forward along random directions
     gen = torch.Generator(device=dev).manual_seed(0)
     errs = []
@@ -364,15 +379,19 @@ def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
             fd = (lp - lm) / (2 * eps)
             an = float((gE * dE).sum() + (gF * dF).sum() + (gS * dS).sum() + (gV * dV).sum())
             errs.append(abs(an - fd) / max(abs(fd), 1e-30))
-    errs = np.array(errs) if errs else np.zeros(1)
-    return {"forward_ms": fwd_ms, "forward_backward_ms": tot_ms, "ratio": tot_ms / fwd_ms,
+    fd = None
+    if errs:
+        errs = np.array(errs)
+        fd = {"directions": fd_dirs, "eps": eps, "median_rel_err": float(np.median(errs)),
+              "max_rel_err": float(errs.max()), "frac_below_1e-3": float((errs < 1e-3).mean()),
+              "forward": "the same float32 rollout"}
+    return {"plain_forward_ms": plain_ms, "forward_ms": fwd_ms, "forward_backward_ms": tot_ms,
+            "ratio": tot_ms / plain_ms, "ratio_vs_rollout_forward": tot_ms / fwd_ms,
             "value": sc.n * n_steps / (tot_ms * 1e-3), "unit": UNIT + " (forward+backward)",
             "substeps": n_steps, "checkpoint_every": every, "particles": sc.n, "loss": L0,
             "grad_norms": {"E": float(gE.norm()), "fibers": float(gF.norm()), "sigma_c": float(gS.norm()),
                            "v0": float(gV.norm())},
-            "fd_check": {"directions": fd_dirs, "eps": eps, "median_rel_err": float(np.median(errs)),
-                         "max_rel_err": float(errs.max()), "frac_below_1e-3": float((errs < 1e-3).mean()),
-                         "forward": "the same float32 rollout"}}
+            "fd_check": fd}
 
 
 def run_ours(args):

@@ -143,7 +143,10 @@ __device__ __forceinline__ void g2p_tail_adj(const pm_params &prm, const float x
 // acc[i].xyz += w (vbar + K Cbar dpos), acc[i].w += L lapbar.  The quadratic
 // stencil is contained in the cubic one (per axis the quadratic node o_q is
 // the cubic node o_c = o_q + s with s = 1 when frac(X) >= 0.5, else 0), so
-// one float4 atomic per cubic node carries both.
+// one float4 atomic per cubic node carries both.  Per axis the quadratic
+// weight, dpos and the K Cbar dpos column are tabulated over the 4 cubic
+// nodes (zero weight where the quadratic stencil does not reach), so a node
+// costs a few multiply-adds.
 __global__ void __launch_bounds__(256) k_adj_scatter(const pm_params prm, const Parts pre, const Parts post,
                                                      const pm_state_adj ain, float4 *__restrict__ acc) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,31 +173,50 @@ __global__ void __launch_bounds__(256) k_adj_scatter(const pm_params prm, const 
     quad_weights(xp, inv_dx, ng, q);
     Cubic c;
     cubic_weights(xp, inv_dx, ng, c);
-    int sh[3];
+    // per axis, over the 4 cubic nodes: quadratic weight (0 outside the
+    // quadratic stencil) and K Cbar[:, axis] dpos_axis
+    float wq[3][4], U[3][4][3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) sh[k] = q.b[k] - c.b[k];   // 0 or 1
+    for (int ax = 0; ax < 3; ++ax) {
+        const bool s1 = q.b[ax] != c.b[ax];   // quadratic base one node higher
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            float w = 0.0f, oq = 0.0f;
+            if (s1) {
+                if (o >= 1) { w = q.w[o - 1][ax]; oq = (float)(o - 1); }
+            } else {
+                if (o < 3) { w = q.w[o][ax]; oq = (float)o; }
+            }
+            wq[ax][o] = w;
+            const float dp = (oq - q.fx[ax]) * dx;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) U[ax][o][i] = K * Ct[3 * i + ax] * dp;
+        }
+    }
     const float lb = a.lapb * L2;
+#pragma unroll
     for (int ox = 0; ox < 4; ++ox) {
-        const int qx = ox - sh[0];
+#pragma unroll
         for (int oy = 0; oy < 4; ++oy) {
-            const int qy = oy - sh[1];
-            const float ab = c.w2[ox][0] * c.w[oy][1] + c.w[ox][0] * c.w2[oy][1];
-            const float e = c.w[ox][0] * c.w[oy][1];
+            const float ab = lb * (c.w2[ox][0] * c.w[oy][1] + c.w[ox][0] * c.w2[oy][1]);
+            const float e = lb * (c.w[ox][0] * c.w[oy][1]);
+            const float wxy = wq[0][ox] * wq[1][oy];
+            const float b0 = vt[0] + U[0][ox][0] + U[1][oy][0];
+            const float b1 = vt[1] + U[0][ox][1] + U[1][oy][1];
+            const float b2 = vt[2] + U[0][ox][2] + U[1][oy][2];
+            const int row = (clampi(c.b[0] + ox, 0, ng - 1) * ng + clampi(c.b[1] + oy, 0, ng - 1)) * ng;
 #pragma unroll
             for (int oz = 0; oz < 4; ++oz) {
-                const int qz = oz - sh[2];
-                const float Lw = ab * c.w[oz][2] + e * c.w2[oz][2];
-                float4 val = make_float4(0.0f, 0.0f, 0.0f, Lw * lb);
-                if (qx >= 0 && qx < 3 && qy >= 0 && qy < 3 && qz >= 0 && qz < 3) {
-                    const float wk = q.w[qx][0] * q.w[qy][1] * q.w[qz][2];
-                    const float dp[3] = {((float)qx - q.fx[0]) * dx, ((float)qy - q.fx[1]) * dx,
-                                         ((float)qz - q.fx[2]) * dx};
-                    val.x = wk * (vt[0] + K * (Ct[0] * dp[0] + Ct[1] * dp[1] + Ct[2] * dp[2]));
-                    val.y = wk * (vt[1] + K * (Ct[3] * dp[0] + Ct[4] * dp[1] + Ct[5] * dp[2]));
-                    val.z = wk * (vt[2] + K * (Ct[6] * dp[0] + Ct[7] * dp[1] + Ct[8] * dp[2]));
-                }
+                const float wk = wxy * wq[2][oz];
+                float4 val;
+                val.x = wk * (b0 + U[2][oz][0]);
+                val.y = wk * (b1 + U[2][oz][1]);
+                val.z = wk * (b2 + U[2][oz][2]);
+                val.w = ab * c.w[oz][2] + e * c.w2[oz][2];
+                // atomics are the cost here: skip the nodes this particle adds nothing to
+                // (outside its quadratic stencil when its lap adjoint is zero)
                 if (val.x != 0.0f || val.y != 0.0f || val.z != 0.0f || val.w != 0.0f)
-                    atomicAdd(&acc[node_of(c.b[0] + ox, c.b[1] + oy, c.b[2] + oz, ng)], val);
+                    atomicAdd(&acc[row + clampi(c.b[2] + oz, 0, ng - 1)], val);
             }
         }
     }
@@ -577,84 +599,63 @@ __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, cons
 }
 
 // ---------------------------------------------------------------- k_adj_particle
-__global__ void __launch_bounds__(128) k_adj_particle(const pm_params prm, const Parts pre, const Parts post,
-                                                      const pm_state_adj ain, const pm_state_adj aout,
-                                                      const pm_param_adj grads, const TapeHead *head,
-                                                      const float4 *__restrict__ gvel, const float4 *__restrict__ A,
-                                                      const float4 *__restrict__ B) {
+// The gathers come first, with the forward's APIC affine term read from the
+// tape, so the constitutive recompute and its adjoint run last with none of
+// the gather state live.  The output adjoint of F is written in two parts:
+// (I + dt C')^T Fbar' before the gathers, the constitutive part added at the
+// end (same thread, same address).
+__global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, const Parts pre, const Parts post,
+                                                         const pm_state_adj ain, const pm_state_adj aout,
+                                                         const pm_param_adj grads, const TapeHead *head,
+                                                         const float4 *__restrict__ gvel,
+                                                         const float4 *__restrict__ A, const float4 *__restrict__ B,
+                                                         const float *__restrict__ taff, long long taff_stride) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= pre.n) return;
-    const long long ps = pre.ps;
+    const long long ps = pre.ps, as = ain.plane_stride, os = aout.plane_stride;
     const int ng = prm.n_grid;
     const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx, dt = (float)prm.dt;
     const float K = (float)(4.0 * prm.inv_dx * prm.inv_dx);
     const float L2 = (float)(prm.inv_dx * prm.inv_dx);
-    float xp[3], vpost[3];
+    const TapeHead h = *head;
+    float xp[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        xp[k] = pre.x[k * ps + p];
-        vpost[k] = post.v[k * ps + p];
-    }
-    AdjIn a;
-    load_adj(ain, p, a);
+    for (int k = 0; k < 3; ++k) xp[k] = pre.x[k * ps + p];
     float xb[3] = {0.0f, 0.0f, 0.0f};
-    bool inside[3];
-    // ---- G2P adjoint, position part (weights and dpos depend on x)
+    float vt[3], Ct[9];
     {
-        float F[9];
+        float vpost[3], F[9];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) vpost[k] = post.v[k * ps + p];
 #pragma unroll
         for (int k = 0; k < 9; ++k) F[k] = pre.F[k * ps + p];
-        float vt[3], Ct[9];
+        AdjIn a;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            a.xb[k] = ain.x[k * as + p];
+            a.vb[k] = ain.v[k * as + p];
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            a.Cb[k] = ain.C[k * as + p];
+            a.Fb[k] = ain.F[k * as + p];
+        }
+        bool inside[3];
         g2p_tail_adj(prm, xp, vpost, F, a, vt, Ct, inside);
-        QuadD q;
-        quad_weights_d(xp, inv_dx, ng, q);
-        for (int ox = 0; ox < 3; ++ox)
-            for (int oy = 0; oy < 3; ++oy)
 #pragma unroll
-                for (int oz = 0; oz < 3; ++oz) {
-                    const float4 g = __ldg(&gvel[node_of(q.b[0] + ox, q.b[1] + oy, q.b[2] + oz, ng)]);
-                    const float wx = q.w[ox][0], wy = q.w[oy][1], wz = q.w[oz][2];
-                    const float wk = wx * wy * wz;
-                    const float dp[3] = {((float)ox - q.fx[0]) * dx, ((float)oy - q.fx[1]) * dx,
-                                         ((float)oz - q.fx[2]) * dx};
-                    const float Cd0 = Ct[0] * dp[0] + Ct[1] * dp[1] + Ct[2] * dp[2];
-                    const float Cd1 = Ct[3] * dp[0] + Ct[4] * dp[1] + Ct[5] * dp[2];
-                    const float Cd2 = Ct[6] * dp[0] + Ct[7] * dp[1] + Ct[8] * dp[2];
-                    const float wbar = vt[0] * g.x + vt[1] * g.y + vt[2] * g.z + K * (g.x * Cd0 + g.y * Cd1 + g.z * Cd2);
-                    xb[0] += wbar * inv_dx * q.dw[ox][0] * wy * wz;
-                    xb[1] += wbar * inv_dx * wx * q.dw[oy][1] * wz;
-                    xb[2] += wbar * inv_dx * wx * wy * q.dw[oz][2];
-                    // dpos = node - x: xbar -= K w Cbar^T v_i
-                    xb[0] -= K * wk * (Ct[0] * g.x + Ct[3] * g.y + Ct[6] * g.z);
-                    xb[1] -= K * wk * (Ct[1] * g.x + Ct[4] * g.y + Ct[7] * g.z);
-                    xb[2] -= K * wk * (Ct[2] * g.x + Ct[5] * g.y + Ct[8] * g.z);
-                }
-    }
-    CubicD cw;
-    cubic_weights_d(xp, inv_dx, ng, cw);
-    {
-        const float lb = a.lapb * L2 * inv_dx;
-        for (int ox = 0; ox < 4; ++ox)
-            for (int oy = 0; oy < 4; ++oy)
+        for (int k = 0; k < 3; ++k) xb[k] = inside[k] ? a.xb[k] : 0.0f;   // x' = clamp(x + dt v')
+        // F' = (I + dt C') F:  Fbar = (I + dt C')^T Fbar' (+ the constitutive part below)
+        float Cp[9];
 #pragma unroll
-                for (int oz = 0; oz < 4; ++oz) {
-                    const float gd = __ldg(&B[node_of(cw.b[0] + ox, cw.b[1] + oy, cw.b[2] + oz, ng)].z);
-                    const float wx = cw.w[ox][0], wy = cw.w[oy][1], wz = cw.w[oz][2];
-                    const float sx = cw.w2[ox][0], sy = cw.w2[oy][1], sz = cw.w2[oz][2];
-                    const float dwx = cw.dw[ox][0], dwy = cw.dw[oy][1], dwz = cw.dw[oz][2];
-                    const float tx = cw.dw2[ox][0], ty = cw.dw2[oy][1], tz = cw.dw2[oz][2];
-                    const float s = gd * lb;
-                    xb[0] += s * (tx * wy * wz + dwx * sy * wz + dwx * wy * sz);
-                    xb[1] += s * (sx * dwy * wz + wx * ty * wz + wx * dwy * sz);
-                    xb[2] += s * (sx * wy * dwz + wx * sy * dwz + wx * wy * tz);
-                }
+        for (int k = 0; k < 9; ++k) Cp[k] = post.C[k * ps + p];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                aout.F[(3 * i + j) * os + p] =
+                    a.Fb[3 * i + j] + dt * (Cp[i] * a.Fb[j] + Cp[3 + i] * a.Fb[3 + j] + Cp[6 + i] * a.Fb[6 + j]);
     }
-    // ---- constitutive recompute
-    const TapeHead h = *head;
-    const bool do_damage = h.any_allow != 0 && (h.step % (long long)prm.damage_every) == 0;
-    Cons c;
-    float tau[9];
-    cons_forward(prm, pre, p, do_damage, c, tau);
+    // ---- P2G inputs of the forward: velocity after the grips, mass, affine term
     float v[3] = {pre.v[p], pre.v[ps + p], pre.v[2 * ps + p]};
     bool gripped = false;
     if (pre.grip_tag) {
@@ -667,90 +668,111 @@ __global__ void __launch_bounds__(128) k_adj_particle(const pm_params prm, const
         }
     }
     const float m = pre.mass[p];
-    const float coeff =
-        __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), pre.vol0[p]), 4.0f), inv_dx), inv_dx);
+    const float mv[3] = {m * v[0], m * v[1], m * v[2]};
     float aff[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) aff[k] = coeff * tau[k] + m * pre.C[k * ps + p];
-    const float mv[3] = {m * v[0], m * v[1], m * v[2]};
-    // ---- P2G adjoint (gather)
-    float mvb[3] = {0.0f, 0.0f, 0.0f}, affb[9];
+    for (int k = 0; k < 9; ++k) aff[k] = taff[k * taff_stride + p];
+    // ---- quadratic gather: G2P adjoint (position part) and P2G adjoint
+    float vsum[3] = {0.0f, 0.0f, 0.0f}, mvb[3] = {0.0f, 0.0f, 0.0f}, affb[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) affb[k] = 0.0f;
     {
         QuadD q;
         quad_weights_d(xp, inv_dx, ng, q);
+#pragma unroll 1
         for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
             for (int oy = 0; oy < 3; ++oy)
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
-                    const float4 g = __ldg(&A[node_of(q.b[0] + ox, q.b[1] + oy, q.b[2] + oz, ng)]);
+                    const int node = node_of(q.b[0] + ox, q.b[1] + oy, q.b[2] + oz, ng);
+                    const float4 g = __ldg(&gvel[node]);
+                    const float4 an = __ldg(&A[node]);
                     const float wx = q.w[ox][0], wy = q.w[oy][1], wz = q.w[oz][2];
                     const float wk = wx * wy * wz;
-                    const float dp[3] = {((float)ox - q.fx[0]) * dx, ((float)oy - q.fx[1]) * dx,
-                                         ((float)oz - q.fx[2]) * dx};
-                    mvb[0] += wk * g.x; mvb[1] += wk * g.y; mvb[2] += wk * g.z;
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        affb[j] += wk * g.x * dp[j];
-                        affb[3 + j] += wk * g.y * dp[j];
-                        affb[6 + j] += wk * g.z * dp[j];
-                    }
-                    const float c0 = mv[0] + aff[0] * dp[0] + aff[1] * dp[1] + aff[2] * dp[2];
-                    const float c1 = mv[1] + aff[3] * dp[0] + aff[4] * dp[1] + aff[5] * dp[2];
-                    const float c2 = mv[2] + aff[6] * dp[0] + aff[7] * dp[1] + aff[8] * dp[2];
-                    const float wbar = g.x * c0 + g.y * c1 + g.z * c2 + g.w * m;
-                    xb[0] += wbar * inv_dx * q.dw[ox][0] * wy * wz;
-                    xb[1] += wbar * inv_dx * wx * q.dw[oy][1] * wz;
-                    xb[2] += wbar * inv_dx * wx * wy * q.dw[oz][2];
-                    xb[0] -= wk * (aff[0] * g.x + aff[3] * g.y + aff[6] * g.z);
-                    xb[1] -= wk * (aff[1] * g.x + aff[4] * g.y + aff[7] * g.z);
-                    xb[2] -= wk * (aff[2] * g.x + aff[5] * g.y + aff[8] * g.z);
+                    const float dp0 = ((float)ox - q.fx[0]) * dx, dp1 = ((float)oy - q.fx[1]) * dx,
+                                dp2 = ((float)oz - q.fx[2]) * dx;
+                    const float u0 = vt[0] + K * (Ct[0] * dp0 + Ct[1] * dp1 + Ct[2] * dp2);
+                    const float u1 = vt[1] + K * (Ct[3] * dp0 + Ct[4] * dp1 + Ct[5] * dp2);
+                    const float u2 = vt[2] + K * (Ct[6] * dp0 + Ct[7] * dp1 + Ct[8] * dp2);
+                    const float c0 = mv[0] + aff[0] * dp0 + aff[1] * dp1 + aff[2] * dp2;
+                    const float c1 = mv[1] + aff[3] * dp0 + aff[4] * dp1 + aff[5] * dp2;
+                    const float c2 = mv[2] + aff[6] * dp0 + aff[7] * dp1 + aff[8] * dp2;
+                    const float wbar = (g.x * u0 + g.y * u1 + g.z * u2) + (an.x * c0 + an.y * c1 + an.z * c2) + an.w * m;
+                    const float wb = wbar * inv_dx;
+                    xb[0] += wb * q.dw[ox][0] * wy * wz;
+                    xb[1] += wb * wx * q.dw[oy][1] * wz;
+                    xb[2] += wb * wx * wy * q.dw[oz][2];
+                    vsum[0] += wk * g.x; vsum[1] += wk * g.y; vsum[2] += wk * g.z;
+                    const float a0 = wk * an.x, a1 = wk * an.y, a2 = wk * an.z;
+                    mvb[0] += a0; mvb[1] += a1; mvb[2] += a2;
+                    affb[0] += a0 * dp0; affb[1] += a0 * dp1; affb[2] += a0 * dp2;
+                    affb[3] += a1 * dp0; affb[4] += a1 * dp1; affb[5] += a1 * dp2;
+                    affb[6] += a2 * dp0; affb[7] += a2 * dp1; affb[8] += a2 * dp2;
                 }
     }
-    float d1b = a.db;
+    // dpos = node - x:  xbar -= K Cbar^T sum(w v_i) + aff^T sum(w mvbar_i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        xb[j] -= K * (Ct[j] * vsum[0] + Ct[3 + j] * vsum[1] + Ct[6 + j] * vsum[2]) +
+                 (aff[j] * mvb[0] + aff[3 + j] * mvb[1] + aff[6 + j] * mvb[2]);
+    // ---- cubic gather: damage scatter adjoint and the Laplacian's position part
+    float d1b = ain.d[p];
     {
+        CubicD cw;
+        cubic_weights_d(xp, inv_dx, ng, cw);
+        const float d1 = post.d[p];
+        const float lb = ain.lap[p] * L2 * inv_dx;
+        float dsum = 0.0f;
+#pragma unroll 1
         for (int ox = 0; ox < 4; ++ox)
-            for (int oy = 0; oy < 4; ++oy)
+#pragma unroll
+            for (int oy = 0; oy < 4; ++oy) {
+                const int row = (clampi(cw.b[0] + ox, 0, ng - 1) * ng + clampi(cw.b[1] + oy, 0, ng - 1)) * ng;
+                float swd = 0.0f, swb = 0.0f, sdwb = 0.0f, g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
 #pragma unroll
                 for (int oz = 0; oz < 4; ++oz) {
-                    const float4 g = __ldg(&B[node_of(cw.b[0] + ox, cw.b[1] + oy, cw.b[2] + oz, ng)]);
-                    const float wx = cw.w[ox][0], wy = cw.w[oy][1], wz = cw.w[oz][2];
-                    const float wk = wx * wy * wz;
-                    d1b += wk * g.x;
-                    const float wbar = g.x * c.d1 + g.y;
-                    xb[0] += wbar * inv_dx * cw.dw[ox][0] * wy * wz;
-                    xb[1] += wbar * inv_dx * wx * cw.dw[oy][1] * wz;
-                    xb[2] += wbar * inv_dx * wx * wy * cw.dw[oz][2];
+                    const float4 bn = __ldg(&B[row + clampi(cw.b[2] + oz, 0, ng - 1)]);
+                    const float wz = cw.w[oz][2], dwz = cw.dw[oz][2];
+                    const float wbar = bn.x * d1 + bn.y;
+                    swd += wz * bn.x;
+                    swb += wz * wbar;
+                    sdwb += dwz * wbar;
+                    g0 += wz * bn.z;
+                    g1 += cw.w2[oz][2] * bn.z;
+                    g2 += dwz * bn.z;
+                    g3 += cw.dw2[oz][2] * bn.z;
                 }
+                const float wx = cw.w[ox][0], wy = cw.w[oy][1], dwx = cw.dw[ox][0], dwy = cw.dw[oy][1];
+                const float sx = cw.w2[ox][0], sy = cw.w2[oy][1], tx = cw.dw2[ox][0], ty = cw.dw2[oy][1];
+                dsum += wx * wy * swd;
+                xb[0] += inv_dx * dwx * wy * swb + lb * ((tx * wy + dwx * sy) * g0 + dwx * wy * g1);
+                xb[1] += inv_dx * wx * dwy * swb + lb * ((sx * dwy + wx * ty) * g0 + wx * dwy * g1);
+                xb[2] += inv_dx * wx * wy * sdwb + lb * ((sx * wy + wx * sy) * g2 + wx * wy * g3);
+            }
+        d1b += dsum;
     }
-    float taub[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) taub[k] = coeff * affb[k];
-    ConsAdj o;
-    cons_adjoint(c, pre.mu[p], pre.lam[p], taub, d1b, a.Dhb, o);
-    // ---- write the adjoints of the pre-step state
-    const long long os = aout.plane_stride;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        aout.x[k * os + p] = (inside[k] ? a.xb[k] : 0.0f) + xb[k];
+        aout.x[k * os + p] = xb[k];
         aout.v[k * os + p] = gripped ? 0.0f : m * mvb[k];
-    }
-    {
-        float Cp[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) Cp[k] = post.C[k * ps + p];
-        // F' = (I + dt C') F:  Fbar += (I + dt C')^T Fbar'
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const float s = a.Fb[3 * i + j] + dt * (Cp[i] * a.Fb[j] + Cp[3 + i] * a.Fb[3 + j] + Cp[6 + i] * a.Fb[6 + j]);
-                aout.F[(3 * i + j) * os + p] = s + o.Fb[3 * i + j];
-            }
     }
 #pragma unroll
     for (int k = 0; k < 9; ++k) aout.C[k * os + p] = m * affb[k];
+    // ---- constitutive recompute and adjoint
+    const bool do_damage = h.any_allow != 0 && (h.step % (long long)prm.damage_every) == 0;
+    const float coeff =
+        __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), pre.vol0[p]), 4.0f), inv_dx), inv_dx);
+    float taub[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) taub[k] = coeff * affb[k];
+    Cons c;
+    float tau[9];
+    cons_forward(prm, pre, p, do_damage, c, tau);
+    ConsAdj o;
+    cons_adjoint(c, pre.mu[p], pre.lam[p], taub, d1b, ain.D_hist[p], o);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) aout.F[k * os + p] += o.Fb[k];
     aout.d[p] = o.d0b;
     aout.lap[p] = o.lapb;
     aout.D_hist[p] = o.Dh0b;
@@ -782,7 +804,7 @@ TapeLayout make_tape_layout(long long n, int ng, int slots) {
     const long long G = (long long)ng * ng * ng;
     const int nbs = (ng + kBlockEdge - 1) / kBlockEdge;
     const long long nb = (long long)nbs * nbs * nbs;
-    (void)n;
+    const long long np = (n + 63) / 64 * 64 > 0 ? (n + 63) / 64 * 64 : 64;
     size_t o = 0;
     T.head = o;    o = align_up(o + sizeof(TapeHead) * (size_t)(slots > 0 ? slots : 1), A);
     T.acc = o;     o = align_up(o + 16 * (size_t)G, A);
@@ -794,6 +816,8 @@ TapeLayout make_tape_layout(long long n, int ng, int slots) {
     T.gd = s;      s = align_up(s + 4 * (size_t)G, A);
     T.sw = s;      s = align_up(s + 4 * (size_t)G, A);
     T.blocks = s;  s = align_up(s + 4 * (size_t)nb, A);
+    T.aff = s;     s = align_up(s + 36 * (size_t)np, A);
+    T.aff_stride = np;
     T.slot_bytes = s;
     T.total = o + s * (size_t)(slots > 0 ? slots : 1);
     T.n_blocks = nb;
@@ -807,6 +831,8 @@ void record_redirect(const TapeLayout &T, void *tape, int slot, WS &w) {
     w.g_gd = (float *)(b + T.gd);
     w.g_sw = (float *)(b + T.sw);
     w.block_list = (int *)(b + T.blocks);
+    w.tape_aff = (float *)(b + T.aff);
+    w.tape_aff_stride = T.aff_stride;
 }
 
 void launch_tape_head(const TapeLayout &T, void *tape, int slot, const WS &w, cudaStream_t s) {
@@ -833,7 +859,9 @@ void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, c
     const long long max_items = T.n_blocks * 64;
     const int gb = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, 148LL * 8));
     k_adj_grid<<<gb, 256, 0, s>>>(prm, blocks, h, gvel, ggd, gsw, acc, Aq, Bc, T.n_blocks);
-    k_adj_particle<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(prm, pre, post, ain, aout, grads, h, gvel, Aq, Bc);
+    const float *taff = (const float *)(b + T.aff);
+    k_adj_particle<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(prm, pre, post, ain, aout, grads, h, gvel, Aq, Bc,
+                                                               taff, T.aff_stride);
 }
 
 }  // namespace pm

@@ -115,6 +115,8 @@ struct WS {
     float4 *g_vel;      // {v.x, v.y, v.z, unused}
     float *g_gd;        // normalised damage field
     float *g_sw;        // cubic weight sums (recorded for the adjoint; NULL otherwise)
+    float *tape_aff;    // APIC affine term, 9 planes (recorded for the adjoint; NULL otherwise)
+    long long tape_aff_stride;
     float4 *payload;    // P2G payload, 5 float4 per particle in sorted order
     const unsigned *sorted_keys;
     const int *perm;
@@ -140,6 +142,8 @@ inline WS make_ws(void *base, const Layout &L) {
     w.g_vel = (float4 *)(b + L.g_vel);
     w.g_gd = (float *)(b + L.g_gd);
     w.g_sw = nullptr;
+    w.tape_aff = nullptr;
+    w.tape_aff_stride = 0;
     w.payload = (float4 *)(b + L.payload);
     w.passes = L.passes;
     w.n_tiles = L.n_tiles;

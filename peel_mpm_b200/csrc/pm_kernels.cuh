@@ -25,10 +25,10 @@ void launch_sym_eig(const float *A, long long n, int sweeps, float *ev, float *V
 
 // Tape of recorded substeps for the adjoint: a header per slot, three
 // adjoint grids shared by all slots, then per slot {v, m} grid, gd, cubic
-// weight sums and the active block list.
+// weight sums, the active block list and the particles' APIC affine term.
 struct TapeLayout {
-    size_t head, acc, adj_q, adj_c, slot0, vel, gd, sw, blocks, slot_bytes, total;
-    long long n_blocks;
+    size_t head, acc, adj_q, adj_c, slot0, vel, gd, sw, blocks, aff, slot_bytes, total;
+    long long n_blocks, aff_stride;
     int slots;
 };
 TapeLayout make_tape_layout(long long n, int ng, int slots);

@@ -259,6 +259,10 @@ __global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, c
     dst[2] = make_float4(aff[0], aff[1], aff[2], aff[3]);
     dst[3] = make_float4(aff[4], aff[5], aff[6], aff[7]);
     dst[4] = make_float4(aff[8], reg ? 1.0f : 0.0f, 0.0f, 0.0f);
+    if (w.tape_aff) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) w.tape_aff[k * w.tape_aff_stride + p] = aff[k];
+    }
 }
 
 // Scatter one particle straight into the global grid with the reference's

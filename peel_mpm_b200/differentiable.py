@@ -70,10 +70,43 @@ def _particles_at(sim: AnisoMPM, P, state: torch.Tensor):
     return Q
 
 
+class _Recorder:
+    """Tape and per-substep states of one checkpoint segment."""
+
+    def __init__(self, sim: AnisoMPM, slots: int):
+        lib = _lib.load()
+        self.sim, self.slots, self.lib = sim, slots, lib
+        dev = sim.device
+        n, stride = sim.n, sim._S.stride(0)
+        grips, _ = sim._descriptors()
+        sim._grip_tags(grips)
+        self.prm = sim._build_params(grips)
+        sim._ensure_ws()
+        P = sim._particles()
+        self.tape_bytes = _lib.tape_size(n, sim.n_grid, slots)
+        self.tape = torch.empty(self.tape_bytes, dtype=torch.uint8, device=dev)
+        self.stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(lib.pm_tape_init(self.tape.data_ptr(), self.tape_bytes, n, sim.n_grid, slots, self.stream),
+                   "pm_tape_init")
+        self.states = torch.empty((slots + 1, _MUTABLE, stride), device=dev, dtype=torch.float32)
+        self.descr = [_particles_at(sim, P, self.states[j]) for j in range(slots + 1)]
+
+    def record(self, state0, k: int, time0: float, step0: int):
+        """Run k substeps from state0 (recording slots 0..k-1); states[j] is
+        the state before substep j, states[k] the final one."""
+        sim, lib = self.sim, self.lib
+        self.states[0].copy_(state0)
+        for j in range(k):
+            self.states[j + 1].copy_(self.states[j])
+            clk = sim._clock(time0 + j * sim.dt, step0 + j)
+            _lib.check(lib.pm_substep_record(C.byref(self.prm), C.byref(self.descr[j + 1]), sim._ws.data_ptr(),
+                                             sim._ws_bytes, C.byref(clk), self.tape.data_ptr(), self.tape_bytes,
+                                             self.slots, j, self.stream), "pm_substep_record")
+
+
 class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, mu, lam, sigma_c, A0, v0, sim, n_steps, time0, every):
-        n = sim.n
         with torch.no_grad():
             sim.mu.copy_(mu)
             sim.lam.copy_(lam)
@@ -84,35 +117,33 @@ class _Rollout(torch.autograd.Function):
             raise NotImplementedError("the adjoint does not support colliders, f_clamp or interface particles")
         step0 = sim._step
         checkpoints = []
+        want_grad = any(ctx.needs_input_grad[:5])
+        rec = _Recorder(sim, min(every, n_steps)) if want_grad else None
         t = 0
         while t < n_steps:
             k = min(every, n_steps - t)
             checkpoints.append(sim._S[:_MUTABLE].clone())
-            sim.run_frame(k, time0 + t * sim.dt)
+            if rec is not None and t + k >= n_steps:
+                # the last segment is recorded now, so the backward starts without recomputing it
+                rec.record(sim._S[:_MUTABLE], k, time0 + t * sim.dt, step0 + t)
+                sim._S[:_MUTABLE].copy_(rec.states[k])
+                sim._step += k
+            else:
+                sim.run_frame(k, time0 + t * sim.dt)
             t += k
         ctx.sim = sim
         ctx.meta = (n_steps, time0, every, step0)
         ctx.checkpoints = checkpoints
+        ctx.rec = rec
         return sim.x.clone()
 
     @staticmethod
     def backward(ctx, gx):
-        sim = ctx.sim
+        sim, rec = ctx.sim, ctx.rec
         n_steps, time0, every, step0 = ctx.meta
-        lib = _lib.load()
+        lib = rec.lib
         dev = sim.device
         n, stride = sim.n, sim._S.stride(0)
-        grips, _ = sim._descriptors()
-        sim._grip_tags(grips)
-        prm = sim._build_params(grips)
-        sim._ensure_ws()
-        P = sim._particles()
-        slots = min(every, n_steps)
-        tape_bytes = _lib.tape_size(n, sim.n_grid, slots)
-        tape = torch.empty(tape_bytes, dtype=torch.uint8, device=dev)
-        st = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(lib.pm_tape_init(tape.data_ptr(), tape_bytes, n, sim.n_grid, slots, st), "pm_tape_init")
-        states = torch.empty((slots + 1, _MUTABLE, stride), device=dev, dtype=torch.float32)
         a_in = torch.zeros((_MUTABLE, stride), device=dev, dtype=torch.float32)
         a_out = torch.zeros_like(a_in)
         a_in[0:3, :n] = gx.t().to(torch.float32)
@@ -122,24 +153,17 @@ class _Rollout(torch.autograd.Function):
         pgb, pst = pg.data_ptr(), stride * 4
         grads.mu, grads.lam, grads.sigma_c, grads.A0 = pgb, pgb + pst, pgb + 2 * pst, pgb + 3 * pst
         seg_starts = list(range(0, n_steps, every))
+        last = len(seg_starts) - 1
         for si in reversed(range(len(seg_starts))):
             t0 = seg_starts[si]
             k = min(every, n_steps - t0)
-            states[0].copy_(ctx.checkpoints[si])
-            descr = []
-            for j in range(k + 1):
-                descr.append(_particles_at(sim, P, states[j]))
-            for j in range(k):
-                states[j + 1].copy_(states[j])
-                clk = sim._clock(time0 + (t0 + j) * sim.dt, step0 + t0 + j)
-                _lib.check(lib.pm_substep_record(C.byref(prm), C.byref(descr[j + 1]), sim._ws.data_ptr(),
-                                                 sim._ws_bytes, C.byref(clk), tape.data_ptr(), tape_bytes, slots, j,
-                                                 st), "pm_substep_record")
+            if si != last:   # the forward recorded the last segment
+                rec.record(ctx.checkpoints[si], k, time0 + t0 * sim.dt, step0 + t0)
             for j in reversed(range(k)):
                 ai, ao = _state_adj(a_in), _state_adj(a_out)
-                _lib.check(lib.pm_substep_adjoint(C.byref(prm), C.byref(descr[j]), C.byref(descr[j + 1]),
-                                                  C.byref(ai), C.byref(ao), C.byref(grads), tape.data_ptr(),
-                                                  tape_bytes, slots, j, st), "pm_substep_adjoint")
+                _lib.check(lib.pm_substep_adjoint(C.byref(rec.prm), C.byref(rec.descr[j]), C.byref(rec.descr[j + 1]),
+                                                  C.byref(ai), C.byref(ao), C.byref(grads), rec.tape.data_ptr(),
+                                                  rec.tape_bytes, rec.slots, j, rec.stream), "pm_substep_adjoint")
                 a_in, a_out = a_out, a_in
         o = _PLANES["v"][0]
         g_mu = pg[0, :n].clone()
@@ -148,6 +172,7 @@ class _Rollout(torch.autograd.Function):
         g_A0 = pg[3:12, :n].t().reshape(n, 3, 3).clone()
         g_v0 = a_in[o:o + 3, :n].t().clone()
         ctx.checkpoints = None
+        ctx.rec = None
         return g_mu, g_lam, g_sc, g_A0, g_v0, None, None, None, None
 
 
