@@ -269,14 +269,59 @@ __global__ void __launch_bounds__(256) k_adj_grid(const pm_params prm, const int
 }
 
 // ---------------------------------------------------------------- constitutive
+// What the adjoint keeps of the forward constitutive update.  The damage
+// driving geometry (Cauchy stress eigensystem, sigma+, A, M) is not kept: it
+// is needed only where the history drive is active, and is recomputed there.
 struct Cons {
     float F[9], V[9], S[3], R[9], lamC[3];
     float J, Jraw, tdev[9], tv;
     bool dmg;
-    float sig[9], ev[3], Q[9], sp[9], A[9], M[9], A0[9];
     float phi, drive, Dh0, Dh1, d0, lap, arg, cc, u, dn, d1, g, vdeg, res, sc, zeta, l0;
     bool allow;
 };
+
+// Damage driving geometry (anisompm.py:650-664): sig = sym(tdev + tv I) / J,
+// its eigensystem, sigma+ = Q relu(e) Q^T, A = R A0 R^T, M = A sigma+ and
+// phi = tr(M M) / sigma_c^2.
+struct DamageGeom {
+    float sig[9], ev[3], Q[9], sp[9], A[9], M[9], A0[9];
+    float phi;
+};
+__device__ __forceinline__ void damage_geom(const float R[9], const float tdev[9], float tv, float J, float sc,
+                                            const Parts &P, long long p, DamageGeom &g) {
+    const long long ps = P.ps;
+    float sg[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sg[k] = (tdev[k] + ((k % 4 == 0) ? tv : 0.0f)) / J;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) g.sig[3 * i + j] = 0.5f * (sg[3 * i + j] + sg[3 * j + i]);
+    sym_eig3<5>(g.sig, g.ev, g.Q);
+    {
+        float ED[9];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float e = g.ev[j] < 0.0f ? 0.0f : g.ev[j];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) ED[3 * i + j] = g.Q[3 * i + j] * e;
+        }
+        mmt3(ED, g.Q, g.sp);
+    }
+    {
+        float RA[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) g.A0[k] = P.A0[k * ps + p];
+        mm3(R, g.A0, RA);
+        mmt3(RA, R, g.A);
+    }
+    mm3(g.A, g.sp, g.M);
+    const float trMM = (g.M[0] * g.M[0] + g.M[1] * g.M[3] + g.M[2] * g.M[6]) +
+                       (g.M[3] * g.M[1] + g.M[4] * g.M[4] + g.M[5] * g.M[7]) +
+                       (g.M[6] * g.M[2] + g.M[7] * g.M[5] + g.M[8] * g.M[8]);
+    g.phi = trMM / (sc * sc);
+}
+
 
 // Forward constitutive update without f_clamp and interface particles, as
 // the forward kernel computes it, keeping the intermediates.
@@ -319,37 +364,12 @@ __device__ __forceinline__ void cons_forward(const pm_params &prm, const Parts &
     c.Dh1 = c.Dh0;
     c.allow = P.allow[p] != 0;
     if (do_damage) {
-        float sg[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) sg[k] = (c.tdev[k] + ((k % 4 == 0) ? c.tv : 0.0f)) / c.J;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) c.sig[3 * i + j] = 0.5f * (sg[3 * i + j] + sg[3 * j + i]);
-        sym_eig3<5>(c.sig, c.ev, c.Q);
-        {
-            float ED[9];
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const float e = c.ev[j] < 0.0f ? 0.0f : c.ev[j];
-#pragma unroll
-                for (int i = 0; i < 3; ++i) ED[3 * i + j] = c.Q[3 * i + j] * e;
-            }
-            mmt3(ED, c.Q, c.sp);
-        }
-        {
-            float RA[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) c.A0[k] = P.A0[k * ps + p];
-            mm3(c.R, c.A0, RA);
-            mmt3(RA, c.R, c.A);
-        }
-        mm3(c.A, c.sp, c.M);
-        const float trMM = (c.M[0] * c.M[0] + c.M[1] * c.M[3] + c.M[2] * c.M[6]) +
-                           (c.M[3] * c.M[1] + c.M[4] * c.M[4] + c.M[5] * c.M[7]) +
-                           (c.M[6] * c.M[2] + c.M[7] * c.M[5] + c.M[8] * c.M[8]);
         c.sc = P.sigma_c[p];
-        c.phi = trMM / (c.sc * c.sc);
+        {
+            DamageGeom dg;
+            damage_geom(c.R, c.tdev, c.tv, c.J, c.sc, P, p, dg);
+            c.phi = dg.phi;
+        }
         c.zeta = P.zeta[p];
         c.drive = c.zeta * relu_f(c.phi - 1.0f);
         c.Dh1 = c.drive > c.Dh0 ? c.drive : c.Dh0;
@@ -422,7 +442,7 @@ struct ConsAdj {
 // Reverse of cons_forward given taubar, the adjoint of the updated damage d1
 // and of the updated history D_hist1.
 __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, const float lam, const float taub[9],
-                                             float d1b, float Dh1b, ConsAdj &o) {
+                                             float d1b, float Dh1b, const Parts &P, long long p, ConsAdj &o) {
     const float trt = taub[0] + taub[4] + taub[8];
     float gb = 0.0f;
 #pragma unroll
@@ -477,26 +497,28 @@ __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, cons
         }
         const float phib = (c.phi > 1.0f) ? c.zeta * driveb : 0.0f;
         if (phib != 0.0f) {
+            DamageGeom dg;
+            damage_geom(c.R, c.tdev, c.tv, c.J, c.sc, P, p, dg);
             const float isc2 = 1.0f / (c.sc * c.sc);
             o.scb += -2.0f * c.phi / c.sc * phib;
             float Mb[9];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int j = 0; j < 3; ++j) Mb[3 * i + j] = 2.0f * phib * isc2 * c.M[3 * j + i];
+                for (int j = 0; j < 3; ++j) Mb[3 * i + j] = 2.0f * phib * isc2 * dg.M[3 * j + i];
             float Ab[9], spb[9];
-            mmt3(Mb, c.sp, Ab);                    // Mb sp^T
+            mmt3(Mb, dg.sp, Ab);                    // Mb sp^T
             // spb = A^T Mb
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
                 for (int j = 0; j < 3; ++j)
-                    spb[3 * i + j] = c.A[i] * Mb[j] + c.A[3 + i] * Mb[3 + j] + c.A[6 + i] * Mb[6 + j];
+                    spb[3 * i + j] = dg.A[i] * Mb[j] + dg.A[3 + i] * Mb[3 + j] + dg.A[6 + i] * Mb[6 + j];
             // A = R A0 R^T:  Rb += Ab R A0^T + Ab^T R A0;  A0b += R^T Ab R
             {
                 float T1[9], T2[9], RA0t[9], RA0[9];
-                mmt3(c.R, c.A0, RA0t);             // R A0^T
-                mm3(c.R, c.A0, RA0);               // R A0
+                mmt3(c.R, dg.A0, RA0t);             // R A0^T
+                mm3(c.R, dg.A0, RA0);               // R A0
                 mm3(Ab, RA0t, T1);
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
@@ -514,14 +536,14 @@ __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, cons
                         o.A0b[3 * i + j] = c.R[i] * AbR[j] + c.R[3 + i] * AbR[3 + j] + c.R[6 + i] * AbR[6 + j];
             }
             float sgb[9];
-            eigsplit_adj(c.ev, c.Q, spb, sgb);
+            eigsplit_adj(dg.ev, dg.Q, spb, sgb);
             // sig = sym(tdev + tv I) / J
             const float iJ = 1.0f / c.J;
             float dots = 0.0f;
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
                 tdevb[k] += sgb[k] * iJ;
-                dots += sgb[k] * c.sig[k];
+                dots += sgb[k] * dg.sig[k];
             }
             tvb += (sgb[0] + sgb[4] + sgb[8]) * iJ;
             Jb += -dots * iJ;
@@ -679,7 +701,7 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
     {
         QuadD q;
         quad_weights_d(xp, inv_dx, ng, q);
-#pragma unroll 1
+#pragma unroll
         for (int ox = 0; ox < 3; ++ox)
 #pragma unroll
             for (int oy = 0; oy < 3; ++oy)
@@ -724,7 +746,7 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
         const float d1 = post.d[p];
         const float lb = ain.lap[p] * L2 * inv_dx;
         float dsum = 0.0f;
-#pragma unroll 1
+#pragma unroll
         for (int ox = 0; ox < 4; ++ox)
 #pragma unroll
             for (int oy = 0; oy < 4; ++oy) {
@@ -770,7 +792,7 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
     float tau[9];
     cons_forward(prm, pre, p, do_damage, c, tau);
     ConsAdj o;
-    cons_adjoint(c, pre.mu[p], pre.lam[p], taub, d1b, ain.D_hist[p], o);
+    cons_adjoint(c, pre.mu[p], pre.lam[p], taub, d1b, ain.D_hist[p], pre, p, o);
 #pragma unroll
     for (int k = 0; k < 9; ++k) aout.F[k * os + p] += o.Fb[k];
     aout.d[p] = o.d0b;
