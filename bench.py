@@ -252,11 +252,16 @@ def run_frames(sim, steps, t0, chunk=100):
         done += k
 
 
-def bench_batched(torch, device, seed=0, n_sub=20, reps=3):
-    """BatchedAnisoMPM on 64 seeded scenes vs the same scenes one by one."""
+def bench_batched(torch, device, rank=0, world=1, max_over_ranks=lambda v: v, barrier=lambda: None, seed=0,
+                  n_sub=20, reps=3):
+    """BatchedAnisoMPM on 64 seeded scenes vs the same scenes one by one.
+    Under N ranks the scenes are bin-packed across ranks (no communication);
+    times are the max over ranks."""
     import peel_mpm_b200 as pm
-    from peel_mpm_b200 import scenes
-    scs = scenes.batch_scenes(seed=seed)
+    from peel_mpm_b200 import autotune, scenes
+    all_scs = scenes.batch_scenes(seed=seed)
+    mine = pm.partition_scenes([sc.n for sc in all_scs], world)[rank]
+    scs = [all_scs[k] for k in mine]
 
     def build(sc):
         sim = pm.AnisoMPM(n_grid=sc.n_grid, grid_lim=sc.grid_lim, dt=sc.dt, gravity=tuple(sc.gravity),
@@ -267,7 +272,8 @@ def bench_batched(torch, device, seed=0, n_sub=20, reps=3):
 
     solo = [build(sc) for sc in scs]
     batch = pm.BatchedAnisoMPM([build(sc) for sc in scs])
-    total = sum(sc.n for sc in scs)
+    tuned = autotune.tune(batch)
+    total = sum(sc.n for sc in all_scs)
     s = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for _ in range(2):
@@ -275,30 +281,32 @@ def bench_batched(torch, device, seed=0, n_sub=20, reps=3):
         for sim in solo:
             sim.run_frame(n_sub, 0.0)
     torch.cuda.synchronize()
+    barrier()
     e0.record(s)
     for r in range(reps):
         batch.run_frame(n_sub, [(2 + r) * n_sub * sc.dt for sc in scs])
     e1.record(s)
     torch.cuda.synchronize()
-    tb = e0.elapsed_time(e1) / reps
+    tb = max_over_ranks(e0.elapsed_time(e1) / reps)
+    barrier()
     e0.record(s)
     for r in range(reps):
         for sim, sc in zip(solo, scs):
             sim.run_frame(n_sub, (2 + r) * n_sub * sc.dt)
     e1.record(s)
     torch.cuda.synchronize()
-    ts = e0.elapsed_time(e1) / reps
+    ts = max_over_ranks(e0.elapsed_time(e1) / reps)
     st = batch.status()
     passes = _batch_passes(scs)
     return {"value": total * n_sub / (tb * 1e-3), "unit": UNIT,
             "sequential_value": total * n_sub / (ts * 1e-3), "speedup_vs_sequential": ts / tb,
             "ms_per_substep": tb / n_sub, "sequential_ms_per_substep": ts / n_sub,
-            "scenes": len(scs), "particles": total, "grids": sorted({sc.n_grid for sc in scs}),
-            "substeps_per_frame": n_sub, "frames": reps,
-            "gpu_launches_per_substep": 7 + 3 * passes,
+            "scenes": len(all_scs), "particles": total, "grids": sorted({sc.n_grid for sc in all_scs}),
+            "scenes_per_rank": len(scs), "substeps_per_frame": n_sub, "frames": reps,
+            "p2g_range": tuned, "gpu_launches_per_substep": 7 + 3 * passes,
             "nonfinite": sum(x["nonfinite"] for x in st),
             "what": "64 scenes, log-uniform 4k-256k particles, one BatchedAnisoMPM.run_frame per frame (one CUDA "
-                    "graph) vs 64 AnisoMPM.run_frame calls (one CUDA graph each)"}
+                    "graph) vs AnisoMPM.run_frame per scene (one CUDA graph each); scenes bin-packed across ranks"}
 
 
 def _batch_passes(scs):
@@ -486,8 +494,8 @@ def run_ours(args):
                            "bytes_per_step": step_bytes}}
 
     forms = {}
-    if rank == 0 and args.form in ("all", "batched"):
-        forms["batched"] = bench_batched(torch, device)
+    if args.form in ("all", "batched"):   # every rank takes its share of the scenes
+        forms["batched"] = bench_batched(torch, device, rank, world, max_over_ranks, barrier)
     if rank == 0 and args.form in ("all", "adjoint"):
         forms["fwd_adjoint"] = bench_adjoint(torch, device, fd_dirs=args.fd_dirs)
 

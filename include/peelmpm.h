@@ -77,6 +77,9 @@ typedef struct pm_params {
     double f_clamp_hi;
     int32_t n_grips;
     int32_t n_colliders;
+    int32_t p2g_range;          /* sorted particles per P2G block (64..4096); 0 = 512 (tuning knob, no
+                                   effect on results beyond float summation order) */
+    int32_t reserved;
     pm_grip grips[PM_MAX_GRIPS];
     pm_collider colliders[PM_MAX_COLLIDERS];
 } pm_params;

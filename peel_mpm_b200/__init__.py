@@ -9,7 +9,7 @@ device and the built library, and fails otherwise.
 """
 from .anisompm import (AnisoMPM, Collider, ParticleGrip, bin_particles, grip_bc, halfspace_collider,
                        sphere_collider, sym_eig)
-from .batched import BatchedAnisoMPM
+from .batched import BatchedAnisoMPM, partition_scenes
 
 __all__ = ["AnisoMPM", "BatchedAnisoMPM", "Collider", "ParticleGrip", "bin_particles", "grip_bc",
-           "halfspace_collider", "sphere_collider", "sym_eig"]
+           "halfspace_collider", "partition_scenes", "sphere_collider", "sym_eig"]

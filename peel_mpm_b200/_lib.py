@@ -44,7 +44,7 @@ class pm_params(C.Structure):
         ("gravity", C.c_double * 3), ("grid_damp", C.c_double),
         ("use_f_clamp", C.c_int32), ("record_stress", C.c_int32),
         ("f_clamp_lo", C.c_double), ("f_clamp_hi", C.c_double),
-        ("n_grips", C.c_int32), ("n_colliders", C.c_int32),
+        ("n_grips", C.c_int32), ("n_colliders", C.c_int32), ("p2g_range", C.c_int32), ("reserved", C.c_int32),
         ("grips", pm_grip * PM_MAX_GRIPS), ("colliders", pm_collider * PM_MAX_COLLIDERS),
     ]
 

@@ -44,6 +44,7 @@ class BatchedAnisoMPM:
         self.sims = sims
         self.device = dev
         self.use_graphs = use_graphs
+        self.p2g_range = 0        # sorted particles per P2G block for the whole batch; 0 = default
         self._lib = _lib.load()
         self._graphs = {}
         self._ws = None
@@ -140,9 +141,11 @@ class BatchedAnisoMPM:
             self._tag_keys = tag_keys
             self._P = None
         prms = [s._build_params(gs) for s, gs in zip(self.sims, grips_all)]
-        keys = tuple(s._params_key for s in self.sims)
+        keys = tuple(s._params_key for s in self.sims) + (int(self.p2g_range),)
         if keys != self._params_keys or not self._ws_ready:
             arr = (_lib.pm_params * len(prms))(*prms)
+            for k in range(len(prms)):
+                arr[k].p2g_range = int(self.p2g_range)
             st = torch.cuda.current_stream(self.device).cuda_stream
             if not self._ws_ready:
                 _lib.check(self._lib.pm_batch_workspace_init(self._ws.data_ptr(), self._ws_bytes, len(prms),
@@ -221,7 +224,7 @@ class BatchedAnisoMPM:
             # keep the pinned source and device table alive until the copy and kernels ran
             self._eager_keep = (host, table)
         else:
-            key = (n_sub, id(P), self._ws.data_ptr(), self._S.data_ptr())
+            key = (n_sub, id(P), self._ws.data_ptr(), self._S.data_ptr(), int(self.p2g_range))
             entry = self._graphs.get(key)
             if entry is None:
                 table = torch.empty(host.numel(), dtype=torch.uint8, device=self.device)
@@ -260,3 +263,19 @@ class BatchedAnisoMPM:
         if bad:
             raise FloatingPointError(f"scenes {bad} produced non-finite x or F")
         return st
+
+
+def partition_scenes(sizes, world: int):
+    """Assign scenes to ``world`` ranks by greedy bin packing on particle
+    counts (largest first onto the least-loaded rank).  Returns one list of
+    scene indices per rank, each in ascending order; scenes are independent,
+    so ranks need no communication while they run."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    loads = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i)):
+        r = min(range(world), key=lambda j: (loads[j], j))
+        parts[r].append(k)
+        loads[r] += int(sizes[k])
+    return [sorted(p) for p in parts]

@@ -109,7 +109,19 @@ pm::BatchScenes scenes_of(void *ws, const BatchPlan &bp) {
 
 // Host record of which batch each workspace was initialised for.
 std::mutex g_mu;
-std::unordered_map<uintptr_t, uint64_t> g_sig;
+struct WsRecord {
+    uint64_t sig;
+    int p2g_range;   // from the stored parameters of scene 0
+};
+std::unordered_map<uintptr_t, WsRecord> g_sig;
+
+// P2G range recorded for this workspace (0 when none).
+int recorded_range(const void *ws) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_sig.find((uintptr_t)ws);
+    return it == g_sig.end() ? 0 : it->second.p2g_range;
+}
+
 
 int check_ws(void *ws, size_t bytes, const BatchPlan &bp, bool require_record) {
     if (!ws) return report_error(PM_ERR_WORKSPACE, "workspace is NULL");
@@ -118,7 +130,7 @@ int check_ws(void *ws, size_t bytes, const BatchPlan &bp, bool require_record) {
     if (require_record) {
         std::lock_guard<std::mutex> lk(g_mu);
         auto it = g_sig.find((uintptr_t)ws);
-        if (it == g_sig.end() || it->second != bp.sig)
+        if (it == g_sig.end() || it->second.sig != bp.sig)
             return report_error(PM_ERR_WORKSPACE,
                                 "workspace was not initialised by pm_batch_workspace_init for these scenes");
     }
@@ -201,7 +213,7 @@ int pm_batch_workspace_init(void *ws, size_t ws_bytes, int32_t n_scenes, const i
     if ((rc = upload_tables(ws, bp, prms, s))) return rc;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        g_sig[(uintptr_t)ws] = bp.sig;
+        g_sig[(uintptr_t)ws] = WsRecord{bp.sig, prms[0].p2g_range};
     }
     return pm::api_cuda_check("pm_batch_workspace_init");
 }
@@ -219,6 +231,10 @@ int pm_batch_set_params(void *ws, size_t ws_bytes, int32_t n_scenes, const int64
             cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return pm::api_cuda_check("pm_batch_set_params");
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_sig[(uintptr_t)ws].p2g_range = prms[0].p2g_range;
+    }
     return PM_OK;
 }
 
@@ -239,7 +255,7 @@ int pm_batch_substep(int32_t n_scenes, const int64_t *n, const int32_t *n_grid, 
     if (bp.n_total > 0) {
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, bp.n_total, s, w.inv_perm);
-        pm::launch_p2g(sc, parts, w, s);
+        pm::launch_p2g(sc, parts, w, s, recorded_range(ws));
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s);
         pm::launch_g2p(sc, parts, w, s, bp.n_ctas);

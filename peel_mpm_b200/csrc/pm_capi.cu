@@ -44,6 +44,8 @@ int check_params(const pm_params *prm) {
     if (prm->damage_every < 1) return fail(PM_ERR_ARG, "damage_every must be >= 1");
     if (prm->n_grips < 0 || prm->n_grips > PM_MAX_GRIPS) return fail(PM_ERR_ARG, "too many grips");
     if (prm->n_colliders < 0 || prm->n_colliders > PM_MAX_COLLIDERS) return fail(PM_ERR_ARG, "too many colliders");
+    if (prm->p2g_range != 0 && (prm->p2g_range < 64 || prm->p2g_range > 4096))
+        return fail(PM_ERR_ARG, "p2g_range must be 0 or in [64, 4096]");
     if (!(prm->dx > 0.0) || !(prm->inv_dx > 0.0)) return fail(PM_ERR_ARG, "dx must be positive");
     return PM_OK;
 }
@@ -168,7 +170,7 @@ int pm_p2g(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
-    pm::launch_p2g(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream);
+    pm::launch_p2g(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream, prm->p2g_range);
     pm::launch_compact(w, (cudaStream_t)stream);
     return cuda_check("pm_p2g");
 }
@@ -207,7 +209,7 @@ static int substep_common(const pm_params *prm, const pm_particles *P, void *ws,
         const pm::PlainScenes sc{*prm};
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, P->n, s, w.inv_perm);
-        pm::launch_p2g(sc, parts, w, s);
+        pm::launch_p2g(sc, parts, w, s, prm->p2g_range);
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s);
         pm::launch_g2p(sc, parts, w, s);
@@ -279,7 +281,7 @@ int pm_substep_record(const pm_params *prm, const pm_particles *P, void *ws, siz
         const pm::PlainScenes sc{*prm};
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, P->n, s, w.inv_perm);
-        pm::launch_p2g(sc, parts, w, s);
+        pm::launch_p2g(sc, parts, w, s, prm->p2g_range);
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s);
         pm::launch_g2p(sc, parts, w, s);

@@ -25,7 +25,10 @@ def mixed_scenes():
         scenes.knobs_drop(), scenes.tiny_bar(), scenes.interface_peel()]
 
 
-def compare(sa, sb, tight=1e-5, loose=1e-3):
+# d, lap and D_hist fracture chaotically: any change of float summation order
+# moves them by up to ~3e-4 (the reference against itself with its particles
+# permuted), so they are held to 10x that; x, v, F, C to float32 rounding.
+def compare(sa, sb, tight=1e-5, loose=3e-3):
     for f in ("x", "v", "F", "C"):
         assert rel_l2(sb[f], sa[f]) < tight, f
     for f in ("d", "lap", "D_hist"):
@@ -111,3 +114,30 @@ def test_batch_rejects_a_workspace_of_another_batch():
     rc = lib.pm_batch_substep(2, batch._n_arr, batch._g_arr, C.byref(P), other.data_ptr(), batch._ws_bytes,
                               other.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert rc == _lib.PM_ERR_WORKSPACE
+
+
+def test_autotuned_p2g_range_keeps_results():
+    """The tuned P2G tile changes only the float summation order."""
+    from peel_mpm_b200 import autotune
+    scs = scenes.batch_scenes(seed=5, n_scenes=4, n_lo=500, n_hi=8000)
+    a = BatchedAnisoMPM([make_gpu_sim(sc) for sc in scs])
+    b = BatchedAnisoMPM([make_gpu_sim(sc) for sc in scs])
+    r = autotune.tune(a, substeps=2, reps=1, force=True)
+    assert r in autotune.CANDIDATES and a.p2g_range == r
+    assert autotune.bucket(a) in autotune._CACHE
+    a.run_frame(5, 0.0)
+    b.run_frame(5, 0.0)
+    torch.cuda.synchronize()
+    for sa, sb in zip(a.sims, b.sims):
+        compare(gpu_state(sb), gpu_state(sa))
+
+
+@pytest.mark.parametrize("rng", [64, 256, 4096])
+def test_plain_p2g_range_keeps_results(rng):
+    sc = scenes.knobs_drop()
+    a, b = make_gpu_sim(sc), make_gpu_sim(sc)
+    a.p2g_range = rng
+    a.run_frame(6, 0.0)
+    b.run_frame(6, 0.0)
+    torch.cuda.synchronize()
+    compare(gpu_state(b), gpu_state(a))

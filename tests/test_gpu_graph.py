@@ -34,7 +34,7 @@ def test_graph_frames_match_eager_substeps(name):
     for f in ("x", "v", "F", "C"):
         assert rel_l2(sb[f], sa[f]) < 1e-5, f
     for f in ("d", "lap", "D_hist"):
-        assert rel_l2(sb[f], sa[f]) < 1e-3, f
+        assert rel_l2(sb[f], sa[f]) < 3e-3, f   # 10x the reference's summation-order envelope
 
 
 def test_graph_recaptures_when_parameters_change():
