@@ -164,7 +164,11 @@ __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
 template <class SC>
 void launch_grid(const SC &sc, const WS &w, cudaStream_t s) {
     const long long max_items = w.n_blocks * 64;
-    const int blocks = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, 148LL * 8));
+    // a batch has many more active nodes than one scene and every item starts
+    // with a dependent chain of table loads (scene lookup, parameters): give
+    // each item its own thread rather than a grid-stride loop
+    const long long cap = SC::batched ? 148LL * 64 : 148LL * 8;
+    const int blocks = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, cap));
     k_grid<SC><<<blocks, 256, 0, s>>>(sc, w);
 }
 template void launch_grid<PlainScenes>(const PlainScenes &, const WS &, cudaStream_t);
@@ -307,7 +311,7 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
 }
 
 template <class SC>
-__global__ void __launch_bounds__(kG2PThreads, 3) k_g2p(const SC scn, const Parts P, const WS w) {
+__global__ void __launch_bounds__(kG2PThreads, 4) k_g2p(const SC scn, const Parts P, const WS w) {
     __shared__ float4 sq[kGTQ];
     __shared__ float sc[kGTC];
     __shared__ int s_box[6];

@@ -212,7 +212,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
 // with fx = X - floor(X - 0.5) per axis for particles whose stencil needs no
 // clamping (regular, base cell in [1, n_grid-4]) and the position x otherwise.
 template <class SC>
-__global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, const WS w) {
+__global__ void __launch_bounds__(256, 4) k_stress(const SC sc, const Parts P, const WS w) {
     // particle order: the state reads and writes are coalesced; the payload
     // goes to the particle's sorted position
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
