@@ -214,7 +214,7 @@ typedef struct pm_param_adj {
 } pm_param_adj;
 
 /* Tape for `slots` recorded substeps of n particles on an n_grid^3 grid:
- * per slot 24 bytes per grid node and 36 bytes per particle, plus three
+ * per slot 24 bytes per grid node and 124 bytes per particle, plus three
  * shared adjoint grids (48 bytes per node).  Zeroed once by pm_tape_init. */
 int pm_tape_size(int64_t n, int32_t n_grid, int32_t slots, size_t *bytes);
 int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32_t slots, void *stream);

@@ -324,29 +324,24 @@ __device__ __forceinline__ void damage_geom(const float R[9], const float tdev[9
 
 
 // Forward constitutive update without f_clamp and interface particles, as
-// the forward kernel computes it, keeping the intermediates.
+// the forward kernel computes it, keeping the intermediates.  The polar
+// decomposition (R, V, S) and, on damage steps, phi come from the tape that
+// the recorded forward wrote (pol[k * rs + p]: R 0..8, V 9..17, S 18..20,
+// phi 21), so neither eigensolve is repeated here.
 __device__ __forceinline__ void cons_forward(const pm_params &prm, const Parts &P, long long p, bool do_damage,
-                                             Cons &c, float tau[9]) {
+                                             Cons &c, float tau[9], const float *__restrict__ pol, long long rs) {
     const long long ps = P.ps;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) c.F[k] = P.F[k * ps + p];
-    float Cg[9];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) Cg[3 * i + j] = c.F[i] * c.F[j] + c.F[3 + i] * c.F[3 + j] + c.F[6 + i] * c.F[6 + j];
-    sym_eig3<5>(Cg, c.lamC, c.V);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) c.S[i] = sqrtf(c.lamC[i] < 1e-12f ? 1e-12f : c.lamC[i]);
-    float W[9];
-    mm3(c.F, c.V, W);
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        const float nr = sqrtf(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]) + 1e-12f;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) W[3 * i + j] = W[3 * i + j] / nr;
+    for (int k = 0; k < 9; ++k) {
+        c.F[k] = P.F[k * ps + p];
+        c.R[k] = pol[k * rs + p];
+        c.V[k] = pol[(9 + k) * rs + p];
     }
-    mmt3(W, c.V, c.R);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        c.S[i] = pol[(18 + i) * rs + p];
+        c.lamC[i] = c.S[i] > sqrtf(1e-12f) ? 1.0f : 0.0f;   // 0 where S = sqrt(max(lamC, 1e-12)) clamped
+    }
     c.Jraw = c.S[0] * c.S[1] * c.S[2];
     c.J = c.Jraw < 1e-6f ? 1e-6f : c.Jraw;
     const float mu = P.mu[p], lam = P.lam[p];
@@ -365,11 +360,7 @@ __device__ __forceinline__ void cons_forward(const pm_params &prm, const Parts &
     c.allow = P.allow[p] != 0;
     if (do_damage) {
         c.sc = P.sigma_c[p];
-        {
-            DamageGeom dg;
-            damage_geom(c.R, c.tdev, c.tv, c.J, c.sc, P, p, dg);
-            c.phi = dg.phi;
-        }
+        c.phi = pol[21 * rs + p];
         c.zeta = P.zeta[p];
         c.drive = c.zeta * relu_f(c.phi - 1.0f);
         c.Dh1 = c.drive > c.Dh0 ? c.drive : c.Dh0;
@@ -585,7 +576,7 @@ __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, cons
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i)
-        if (!(c.lamC[i] > 1e-12f)) Sb[i] = 0.0f;
+        if (c.lamC[i] == 0.0f) Sb[i] = 0.0f;
     // polar F = R U: Fbar += R V (G + diag(Sbar)) V^T with
     // G_ij = (B_ij - B_ji) / (S_i + S_j), B = V^T R^T Rbar V
     float RtRb[9], T[9], Bm[9];
@@ -631,7 +622,8 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
                                                          const pm_param_adj grads, const TapeHead *head,
                                                          const float4 *__restrict__ gvel,
                                                          const float4 *__restrict__ A, const float4 *__restrict__ B,
-                                                         const float *__restrict__ taff, long long taff_stride) {
+                                                         const float *__restrict__ taff, const float *__restrict__ tpol,
+                                                         long long taff_stride) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= pre.n) return;
     const long long ps = pre.ps, as = ain.plane_stride, os = aout.plane_stride;
@@ -790,7 +782,7 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
     for (int k = 0; k < 9; ++k) taub[k] = coeff * affb[k];
     Cons c;
     float tau[9];
-    cons_forward(prm, pre, p, do_damage, c, tau);
+    cons_forward(prm, pre, p, do_damage, c, tau, tpol, taff_stride);
     ConsAdj o;
     cons_adjoint(c, pre.mu[p], pre.lam[p], taub, d1b, ain.D_hist[p], pre, p, o);
 #pragma unroll
@@ -839,6 +831,7 @@ TapeLayout make_tape_layout(long long n, int ng, int slots) {
     T.sw = s;      s = align_up(s + 4 * (size_t)G, A);
     T.blocks = s;  s = align_up(s + 4 * (size_t)nb, A);
     T.aff = s;     s = align_up(s + 36 * (size_t)np, A);
+    T.pol = s;     s = align_up(s + 88 * (size_t)np, A);
     T.aff_stride = np;
     T.slot_bytes = s;
     T.total = o + s * (size_t)(slots > 0 ? slots : 1);
@@ -854,6 +847,7 @@ void record_redirect(const TapeLayout &T, void *tape, int slot, WS &w) {
     w.g_sw = (float *)(b + T.sw);
     w.block_list = (int *)(b + T.blocks);
     w.tape_aff = (float *)(b + T.aff);
+    w.tape_pol = (float *)(b + T.pol);
     w.tape_aff_stride = T.aff_stride;
 }
 
@@ -882,8 +876,9 @@ void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, c
     const int gb = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, 148LL * 8));
     k_adj_grid<<<gb, 256, 0, s>>>(prm, blocks, h, gvel, ggd, gsw, acc, Aq, Bc, T.n_blocks);
     const float *taff = (const float *)(b + T.aff);
+    const float *tpol = (const float *)(b + T.pol);
     k_adj_particle<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(prm, pre, post, ain, aout, grads, h, gvel, Aq, Bc,
-                                                               taff, T.aff_stride);
+                                                               taff, tpol, T.aff_stride);
 }
 
 }  // namespace pm

@@ -116,6 +116,7 @@ struct WS {
     float *g_gd;        // normalised damage field
     float *g_sw;        // cubic weight sums (recorded for the adjoint; NULL otherwise)
     float *tape_aff;    // APIC affine term, 9 planes (recorded for the adjoint; NULL otherwise)
+    float *tape_pol;    // polar R, V, S and phi, 22 planes (recorded for the adjoint; NULL otherwise)
     long long tape_aff_stride;
     float4 *payload;    // P2G payload, 5 float4 per particle in sorted order
     const unsigned *sorted_keys;
@@ -143,6 +144,7 @@ inline WS make_ws(void *base, const Layout &L) {
     w.g_gd = (float *)(b + L.g_gd);
     w.g_sw = nullptr;
     w.tape_aff = nullptr;
+    w.tape_pol = nullptr;
     w.tape_aff_stride = 0;
     w.payload = (float4 *)(b + L.payload);
     w.passes = L.passes;

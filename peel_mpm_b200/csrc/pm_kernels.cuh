@@ -25,9 +25,10 @@ void launch_sym_eig(const float *A, long long n, int sweeps, float *ev, float *V
 
 // Tape of recorded substeps for the adjoint: a header per slot, three
 // adjoint grids shared by all slots, then per slot {v, m} grid, gd, cubic
-// weight sums, the active block list and the particles' APIC affine term.
+// weight sums, the active block list, the particles' APIC affine term and
+// their polar decomposition (R, V, S) and damage drive phi.
 struct TapeLayout {
-    size_t head, acc, adj_q, adj_c, slot0, vel, gd, sw, blocks, aff, slot_bytes, total;
+    size_t head, acc, adj_q, adj_c, slot0, vel, gd, sw, blocks, aff, pol, slot_bytes, total;
     long long n_blocks, aff_stride;
     int slots;
 };

@@ -35,8 +35,11 @@ __device__ __forceinline__ float tmax(float a, float b) { return (a != a || b !=
 
 // Constitutive update of particle p (anisompm.py:614-706).  Writes tau and
 // updates F (f_clamp), d, D_hist and the diagnostics in place.
+// When `rec` is set (recording a substep for the adjoint) the polar
+// decomposition (R, V, S) and, on damage steps, phi are written to its planes:
+// rec[k * rs + p] for R (k 0..8), V (9..17), S (18..20), phi (21).
 __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &P, long long p, bool do_damage,
-                                             float tau[9]) {
+                                             float tau[9], float *rec = nullptr, long long rs = 0) {
     const long long ps = P.ps;
     float F[9];
 #pragma unroll
@@ -60,6 +63,15 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
         for (int i = 0; i < 3; ++i) W[3 * i + j] = W[3 * i + j] / nr;   // (620)
     }
     mmt3(W, V, R);                                                   // R = What V^T (621)
+    if (rec) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            rec[k * rs + p] = R[k];
+            rec[(9 + k) * rs + p] = V[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) rec[(18 + k) * rs + p] = S[k];
+    }
     if (prm.use_f_clamp) {                                           // (622-636)
         const float lo = (float)prm.f_clamp_lo, hi = (float)prm.f_clamp_hi;
         float D[9], corr[9];
@@ -124,6 +136,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
                            (M[6] * M[2] + M[7] * M[5] + M[8] * M[8]);
         const float sc = P.sigma_c[p];
         const float phi = trMM / (sc * sc);                          // (663-664)
+        if (rec) rec[21 * rs + p] = phi;
         if (P.phi) P.phi[p] = phi;
         if (P.phi_shear) {                                           // (670-673)
             float phs = 0.0f;
@@ -226,7 +239,7 @@ __global__ void __launch_bounds__(256, 4) k_stress(const SC sc, const Parts P, c
     const Ctrl *ctrl = w.ctrl + sid;
     const bool do_damage = ctrl->any_allow != 0 && (ctrl->step % (long long)prm.damage_every) == 0;
     float tau[9];
-    constitutive(prm, P, p, do_damage, tau);
+    constitutive(prm, P, p, do_damage, tau, w.tape_pol, w.tape_aff_stride);
     float v[3] = {P.v[p], P.v[ps + p], P.v[2 * ps + p]};
     if (P.grip_tag) {                                                // particle BCs (601-602)
         const int g = P.grip_tag[p];
