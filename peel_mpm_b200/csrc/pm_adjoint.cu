@@ -611,6 +611,96 @@ __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, cons
     for (int k = 0; k < 9; ++k) o.Fb[k] += Fp[k];
 }
 
+constexpr int kAQ = 512;    // staged quadratic nodes per CTA ({v, m} and {mvbar, mbar}: 32 B each)
+constexpr int kAC = 1024;   // staged cubic nodes per CTA (16 B each)
+
+// Gathers of k_adj_particle for one particle, from the CTA's shared-memory
+// tile (TILE) or from global memory with the reference's clamped indices.
+template <bool TILE>
+__device__ __forceinline__ void adj_gather(const float xp[3], float inv_dx, float dx, float K, int ng,
+                                           const float vt[3], const float Ct[9], const float mv[3], float m,
+                                           const float aff[9], float d1, float lb, const float4 *sv,
+                                           const float4 *sa, const float4 *sb, const int lo[3], const int qd[3],
+                                           const int cd[3], const float4 *__restrict__ gvel,
+                                           const float4 *__restrict__ A, const float4 *__restrict__ B,
+                                           float xb[3], float vsum[3], float mvb[3], float affb[9], float &d1b) {
+    {
+        QuadD q;
+        quad_weights_d(xp, inv_dx, ng, q);
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) {
+                    float4 g, an;
+                    if (TILE) {
+                        const int t = ((q.b[0] + ox - lo[0]) * qd[1] + (q.b[1] + oy - lo[1])) * qd[2] + q.b[2] + oz - lo[2];
+                        g = sv[t];
+                        an = sa[t];
+                    } else {
+                        const int node = node_of(q.b[0] + ox, q.b[1] + oy, q.b[2] + oz, ng);
+                        g = __ldg(&gvel[node]);
+                        an = __ldg(&A[node]);
+                    }
+                    const float wx = q.w[ox][0], wy = q.w[oy][1], wz = q.w[oz][2];
+                    const float wk = wx * wy * wz;
+                    const float dp0 = ((float)ox - q.fx[0]) * dx, dp1 = ((float)oy - q.fx[1]) * dx,
+                                dp2 = ((float)oz - q.fx[2]) * dx;
+                    const float u0 = vt[0] + K * (Ct[0] * dp0 + Ct[1] * dp1 + Ct[2] * dp2);
+                    const float u1 = vt[1] + K * (Ct[3] * dp0 + Ct[4] * dp1 + Ct[5] * dp2);
+                    const float u2 = vt[2] + K * (Ct[6] * dp0 + Ct[7] * dp1 + Ct[8] * dp2);
+                    const float c0 = mv[0] + aff[0] * dp0 + aff[1] * dp1 + aff[2] * dp2;
+                    const float c1 = mv[1] + aff[3] * dp0 + aff[4] * dp1 + aff[5] * dp2;
+                    const float c2 = mv[2] + aff[6] * dp0 + aff[7] * dp1 + aff[8] * dp2;
+                    const float wbar = (g.x * u0 + g.y * u1 + g.z * u2) + (an.x * c0 + an.y * c1 + an.z * c2) + an.w * m;
+                    const float wb = wbar * inv_dx;
+                    xb[0] += wb * q.dw[ox][0] * wy * wz;
+                    xb[1] += wb * wx * q.dw[oy][1] * wz;
+                    xb[2] += wb * wx * wy * q.dw[oz][2];
+                    vsum[0] += wk * g.x; vsum[1] += wk * g.y; vsum[2] += wk * g.z;
+                    const float a0 = wk * an.x, a1 = wk * an.y, a2 = wk * an.z;
+                    mvb[0] += a0; mvb[1] += a1; mvb[2] += a2;
+                    affb[0] += a0 * dp0; affb[1] += a0 * dp1; affb[2] += a0 * dp2;
+                    affb[3] += a1 * dp0; affb[4] += a1 * dp1; affb[5] += a1 * dp2;
+                    affb[6] += a2 * dp0; affb[7] += a2 * dp1; affb[8] += a2 * dp2;
+                }
+    }
+    {
+        CubicD cw;
+        cubic_weights_d(xp, inv_dx, ng, cw);
+        float dsum = 0.0f;
+#pragma unroll
+        for (int ox = 0; ox < 4; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 4; ++oy) {
+                const int row = TILE ? ((cw.b[0] + ox - lo[0] + 1) * cd[1] + (cw.b[1] + oy - lo[1] + 1)) * cd[2]
+                                     : (clampi(cw.b[0] + ox, 0, ng - 1) * ng + clampi(cw.b[1] + oy, 0, ng - 1)) * ng;
+                float swd = 0.0f, swb = 0.0f, sdwb = 0.0f, g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
+#pragma unroll
+                for (int oz = 0; oz < 4; ++oz) {
+                    const float4 bn = TILE ? sb[row + cw.b[2] + oz - lo[2] + 1] : __ldg(&B[row + clampi(cw.b[2] + oz, 0, ng - 1)]);
+                    const float wz = cw.w[oz][2], dwz = cw.dw[oz][2];
+                    const float wbar = bn.x * d1 + bn.y;
+                    swd += wz * bn.x;
+                    swb += wz * wbar;
+                    sdwb += dwz * wbar;
+                    g0 += wz * bn.z;
+                    g1 += cw.w2[oz][2] * bn.z;
+                    g2 += dwz * bn.z;
+                    g3 += cw.dw2[oz][2] * bn.z;
+                }
+                const float wx = cw.w[ox][0], wy = cw.w[oy][1], dwx = cw.dw[ox][0], dwy = cw.dw[oy][1];
+                const float sx = cw.w2[ox][0], sy = cw.w2[oy][1], tx = cw.dw2[ox][0], ty = cw.dw2[oy][1];
+                dsum += wx * wy * swd;
+                xb[0] += inv_dx * dwx * wy * swb + lb * ((tx * wy + dwx * sy) * g0 + dwx * wy * g1);
+                xb[1] += inv_dx * wx * dwy * swb + lb * ((sx * dwy + wx * ty) * g0 + wx * dwy * g1);
+                xb[2] += inv_dx * wx * wy * sdwb + lb * ((sx * wy + wx * sy) * g2 + wx * wy * g3);
+            }
+        d1b += dsum;
+    }
+}
+
 // ---------------------------------------------------------------- k_adj_particle
 // The gathers come first, with the forward's APIC affine term read from the
 // tape, so the constitutive recompute and its adjoint run last with none of
@@ -624,17 +714,65 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
                                                          const float4 *__restrict__ A, const float4 *__restrict__ B,
                                                          const float *__restrict__ taff, const float *__restrict__ tpol,
                                                          long long taff_stride) {
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= pre.n) return;
+    __shared__ float4 sv[kAQ], sa[kAQ], sb[kAC];
+    __shared__ int s_box[6];
+    const int tid = threadIdx.x;
+    const long long p = (long long)blockIdx.x * blockDim.x + tid;
+    const bool valid = p < pre.n;
     const long long ps = pre.ps, as = ain.plane_stride, os = aout.plane_stride;
     const int ng = prm.n_grid;
     const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx, dt = (float)prm.dt;
     const float K = (float)(4.0 * prm.inv_dx * prm.inv_dx);
     const float L2 = (float)(prm.inv_dx * prm.inv_dx);
-    const TapeHead h = *head;
-    float xp[3];
+    float xp[3] = {0.0f, 0.0f, 0.0f};
+    // ---- stage the CTA's grid footprint (as k_g2p does): {v, m} and the
+    // momentum adjoints of the quadratic nodes of the regular particles' base
+    // cells' bounding box, the damage adjoints of its cubic nodes
+    bool reg = valid;
+    int qb[3] = {0, 0, 0};
+    if (valid) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) xp[k] = pre.x[k * ps + p];
+        for (int k = 0; k < 3; ++k) {
+            xp[k] = pre.x[k * ps + p];
+            const float fb = floorf(__fsub_rn(__fmul_rn(xp[k], inv_dx), 0.5f));
+            reg = reg && (fb >= 1.0f) && (fb <= (float)(ng - 4));
+            qb[k] = reg ? (int)fb : 0;
+        }
+    }
+    if (tid < 6) s_box[tid] = tid < 3 ? 0x7fffffff : -0x7fffffff;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int mn = __reduce_min_sync(0xffffffffu, reg ? qb[k] : 0x7fffffff);
+        const int mx = __reduce_max_sync(0xffffffffu, reg ? qb[k] : -0x7fffffff);
+        if ((tid & 31) == 0) {
+            atomicMin(&s_box[k], mn);
+            atomicMax(&s_box[3 + k], mx);
+        }
+    }
+    __syncthreads();
+    const int lo[3] = {s_box[0], s_box[1], s_box[2]};
+    const bool any = s_box[3] >= lo[0];
+    const int qd[3] = {s_box[3] - lo[0] + 3, s_box[4] - lo[1] + 3, s_box[5] - lo[2] + 3};
+    const int cd[3] = {qd[0] + 2, qd[1] + 2, qd[2] + 2};
+    const int qn = any ? qd[0] * qd[1] * qd[2] : 0, cn = any ? cd[0] * cd[1] * cd[2] : 0;
+    const bool tile = any && qn <= kAQ && cn <= kAC;
+    if (tile) {   // regular nodes lie inside the grid
+        for (int i = tid; i < qn; i += blockDim.x) {
+            const int gx = lo[0] + i / (qd[1] * qd[2]), gy = lo[1] + (i / qd[2]) % qd[1], gz = lo[2] + i % qd[2];
+            const long long node = ((long long)gx * ng + gy) * ng + gz;
+            sv[i] = gvel[node];
+            sa[i] = A[node];
+        }
+        for (int i = tid; i < cn; i += blockDim.x) {
+            const int gx = lo[0] - 1 + i / (cd[1] * cd[2]), gy = lo[1] - 1 + (i / cd[2]) % cd[1],
+                      gz = lo[2] - 1 + i % cd[2];
+            sb[i] = B[((long long)gx * ng + gy) * ng + gz];
+        }
+    }
+    __syncthreads();
+    if (!valid) return;
+    const TapeHead h = *head;
     float xb[3] = {0.0f, 0.0f, 0.0f};
     float vt[3], Ct[9];
     {
@@ -686,86 +824,27 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
     float aff[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) aff[k] = taff[k * taff_stride + p];
-    // ---- quadratic gather: G2P adjoint (position part) and P2G adjoint
+    // ---- gathers (quadratic: G2P adjoint position part and P2G adjoint;
+    // cubic: damage scatter adjoint and the Laplacian's position part)
     float vsum[3] = {0.0f, 0.0f, 0.0f}, mvb[3] = {0.0f, 0.0f, 0.0f}, affb[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) affb[k] = 0.0f;
+    float d1b = ain.d[p];
     {
-        QuadD q;
-        quad_weights_d(xp, inv_dx, ng, q);
-#pragma unroll
-        for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-            for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                for (int oz = 0; oz < 3; ++oz) {
-                    const int node = node_of(q.b[0] + ox, q.b[1] + oy, q.b[2] + oz, ng);
-                    const float4 g = __ldg(&gvel[node]);
-                    const float4 an = __ldg(&A[node]);
-                    const float wx = q.w[ox][0], wy = q.w[oy][1], wz = q.w[oz][2];
-                    const float wk = wx * wy * wz;
-                    const float dp0 = ((float)ox - q.fx[0]) * dx, dp1 = ((float)oy - q.fx[1]) * dx,
-                                dp2 = ((float)oz - q.fx[2]) * dx;
-                    const float u0 = vt[0] + K * (Ct[0] * dp0 + Ct[1] * dp1 + Ct[2] * dp2);
-                    const float u1 = vt[1] + K * (Ct[3] * dp0 + Ct[4] * dp1 + Ct[5] * dp2);
-                    const float u2 = vt[2] + K * (Ct[6] * dp0 + Ct[7] * dp1 + Ct[8] * dp2);
-                    const float c0 = mv[0] + aff[0] * dp0 + aff[1] * dp1 + aff[2] * dp2;
-                    const float c1 = mv[1] + aff[3] * dp0 + aff[4] * dp1 + aff[5] * dp2;
-                    const float c2 = mv[2] + aff[6] * dp0 + aff[7] * dp1 + aff[8] * dp2;
-                    const float wbar = (g.x * u0 + g.y * u1 + g.z * u2) + (an.x * c0 + an.y * c1 + an.z * c2) + an.w * m;
-                    const float wb = wbar * inv_dx;
-                    xb[0] += wb * q.dw[ox][0] * wy * wz;
-                    xb[1] += wb * wx * q.dw[oy][1] * wz;
-                    xb[2] += wb * wx * wy * q.dw[oz][2];
-                    vsum[0] += wk * g.x; vsum[1] += wk * g.y; vsum[2] += wk * g.z;
-                    const float a0 = wk * an.x, a1 = wk * an.y, a2 = wk * an.z;
-                    mvb[0] += a0; mvb[1] += a1; mvb[2] += a2;
-                    affb[0] += a0 * dp0; affb[1] += a0 * dp1; affb[2] += a0 * dp2;
-                    affb[3] += a1 * dp0; affb[4] += a1 * dp1; affb[5] += a1 * dp2;
-                    affb[6] += a2 * dp0; affb[7] += a2 * dp1; affb[8] += a2 * dp2;
-                }
+        const float d1 = post.d[p];
+        const float lb = ain.lap[p] * L2 * inv_dx;
+        if (reg && tile)
+            adj_gather<true>(xp, inv_dx, dx, K, ng, vt, Ct, mv, m, aff, d1, lb, sv, sa, sb, lo, qd, cd, gvel, A, B,
+                             xb, vsum, mvb, affb, d1b);
+        else
+            adj_gather<false>(xp, inv_dx, dx, K, ng, vt, Ct, mv, m, aff, d1, lb, sv, sa, sb, lo, qd, cd, gvel, A, B,
+                              xb, vsum, mvb, affb, d1b);
     }
     // dpos = node - x:  xbar -= K Cbar^T sum(w v_i) + aff^T sum(w mvbar_i)
 #pragma unroll
     for (int j = 0; j < 3; ++j)
         xb[j] -= K * (Ct[j] * vsum[0] + Ct[3 + j] * vsum[1] + Ct[6 + j] * vsum[2]) +
                  (aff[j] * mvb[0] + aff[3 + j] * mvb[1] + aff[6 + j] * mvb[2]);
-    // ---- cubic gather: damage scatter adjoint and the Laplacian's position part
-    float d1b = ain.d[p];
-    {
-        CubicD cw;
-        cubic_weights_d(xp, inv_dx, ng, cw);
-        const float d1 = post.d[p];
-        const float lb = ain.lap[p] * L2 * inv_dx;
-        float dsum = 0.0f;
-#pragma unroll
-        for (int ox = 0; ox < 4; ++ox)
-#pragma unroll
-            for (int oy = 0; oy < 4; ++oy) {
-                const int row = (clampi(cw.b[0] + ox, 0, ng - 1) * ng + clampi(cw.b[1] + oy, 0, ng - 1)) * ng;
-                float swd = 0.0f, swb = 0.0f, sdwb = 0.0f, g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
-#pragma unroll
-                for (int oz = 0; oz < 4; ++oz) {
-                    const float4 bn = __ldg(&B[row + clampi(cw.b[2] + oz, 0, ng - 1)]);
-                    const float wz = cw.w[oz][2], dwz = cw.dw[oz][2];
-                    const float wbar = bn.x * d1 + bn.y;
-                    swd += wz * bn.x;
-                    swb += wz * wbar;
-                    sdwb += dwz * wbar;
-                    g0 += wz * bn.z;
-                    g1 += cw.w2[oz][2] * bn.z;
-                    g2 += dwz * bn.z;
-                    g3 += cw.dw2[oz][2] * bn.z;
-                }
-                const float wx = cw.w[ox][0], wy = cw.w[oy][1], dwx = cw.dw[ox][0], dwy = cw.dw[oy][1];
-                const float sx = cw.w2[ox][0], sy = cw.w2[oy][1], tx = cw.dw2[ox][0], ty = cw.dw2[oy][1];
-                dsum += wx * wy * swd;
-                xb[0] += inv_dx * dwx * wy * swb + lb * ((tx * wy + dwx * sy) * g0 + dwx * wy * g1);
-                xb[1] += inv_dx * wx * dwy * swb + lb * ((sx * dwy + wx * ty) * g0 + wx * dwy * g1);
-                xb[2] += inv_dx * wx * wy * sdwb + lb * ((sx * wy + wx * sy) * g2 + wx * wy * g3);
-            }
-        d1b += dsum;
-    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         aout.x[k * os + p] = xb[k];
@@ -793,10 +872,17 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
     const long long gs = grads.plane_stride;
     if (grads.mu) grads.mu[p] += o.mub;
     if (grads.lam) grads.lam[p] += o.lamb;
-    if (grads.sigma_c) grads.sigma_c[p] += o.scb;
+    // sigma_c and A0 enter only through an active damage drive: most
+    // particles add zero, so skip their read-modify-write
+    if (grads.sigma_c && o.scb != 0.0f) grads.sigma_c[p] += o.scb;
     if (grads.A0) {
+        bool nz = false;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) grads.A0[k * gs + p] += o.A0b[k];
+        for (int k = 0; k < 9; ++k) nz = nz || o.A0b[k] != 0.0f;
+        if (nz) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) grads.A0[k * gs + p] += o.A0b[k];
+        }
     }
 }
 
