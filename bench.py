@@ -296,17 +296,29 @@ def bench_batched(torch, device, rank=0, world=1, max_over_ranks=lambda v: v, ba
     e1.record(s)
     torch.cuda.synchronize()
     ts = max_over_ranks(e0.elapsed_time(e1) / reps)
+    # the same scenes with eager substeps (one C call per substep, no graphs)
+    for sim in solo:
+        sim.use_graphs = False
+    barrier()
+    e0.record(s)
+    for sim, sc in zip(solo, scs):
+        sim.run_frame(n_sub, 5 * n_sub * sc.dt)
+    e1.record(s)
+    torch.cuda.synchronize()
+    te = max_over_ranks(e0.elapsed_time(e1))
     st = batch.status()
     passes = _batch_passes(scs)
     return {"value": total * n_sub / (tb * 1e-3), "unit": UNIT,
             "sequential_value": total * n_sub / (ts * 1e-3), "speedup_vs_sequential": ts / tb,
+            "sequential_eager_value": total * n_sub / (te * 1e-3), "speedup_vs_sequential_eager": te / tb,
             "ms_per_substep": tb / n_sub, "sequential_ms_per_substep": ts / n_sub,
             "scenes": len(all_scs), "particles": total, "grids": sorted({sc.n_grid for sc in all_scs}),
             "scenes_per_rank": len(scs), "substeps_per_frame": n_sub, "frames": reps,
             "p2g_range": tuned, "gpu_launches_per_substep": 7 + 3 * passes,
             "nonfinite": sum(x["nonfinite"] for x in st),
             "what": "64 scenes, log-uniform 4k-256k particles, one BatchedAnisoMPM.run_frame per frame (one CUDA "
-                    "graph) vs AnisoMPM.run_frame per scene (one CUDA graph each); scenes bin-packed across ranks"}
+                    "graph) vs AnisoMPM.run_frame per scene (one CUDA graph each; and eager, one C call per "
+                    "substep); scenes bin-packed across ranks"}
 
 
 def _batch_passes(scs):
