@@ -115,44 +115,26 @@ def halfspace_collider(origin_fn, normal, mode="slip", friction=0.0) -> Collider
 def sym_eig(A: torch.Tensor, sweeps: int = 5):
     """Batched 3x3 symmetric eigendecomposition by cyclic Jacobi on the GPU
     (anisompm.py:48-95): ascending eigenvalues (N,3) and eigenvector columns
-    (N,3,3).  CUDA float32 tensors only."""
+    (N,3,3).  CUDA tensors only (computed in float32); runs as
+    ``torch.ops.peelmpm.sym_eig``."""
     if not A.is_cuda:
         raise ValueError("sym_eig runs on CUDA tensors only")
     if A.dim() != 3 or A.shape[1:] != (3, 3):
         raise ValueError("A must be (N,3,3)")
-    lib = _lib.load()
-    A = A.to(torch.float32).contiguous()
-    n = A.shape[0]
-    ev = torch.empty((n, 3), dtype=torch.float32, device=A.device)
-    V = torch.empty((n, 3, 3), dtype=torch.float32, device=A.device)
-    with torch.cuda.device(A.device):
-        s = torch.cuda.current_stream().cuda_stream
-        _lib.check(lib.pm_sym_eig(A.data_ptr(), n, int(sweeps), ev.data_ptr(), V.data_ptr(), s), "pm_sym_eig")
-    return ev, V
+    from . import ops  # noqa: F401  (registers torch.ops.peelmpm)
+    return torch.ops.peelmpm.sym_eig(A, int(sweeps))
 
 
-def bin_particles(x: torch.Tensor, n_grid: int, inv_dx: float, workspace: Optional[torch.Tensor] = None):
+def bin_particles(x: torch.Tensor, n_grid: int, inv_dx: float):
     """Cell key (``_node_index`` of the quadratic base cell, anisompm.py:544-548,
     586-590) of every particle, sorted, and the stable sorting permutation,
     on the GPU.  ``x`` is an (N,3) CUDA float32 tensor (any strides whose
-    component planes are equally spaced, e.g. ``AnisoMPM.x``)."""
-    lib = _lib.load()
+    component planes are equally spaced, e.g. ``AnisoMPM.x``); runs as
+    ``torch.ops.peelmpm.bin_sort``."""
     if not x.is_cuda or x.dtype != torch.float32 or x.dim() != 2 or x.shape[1] != 3:
         raise ValueError("x must be an (N,3) CUDA float32 tensor")
-    n = x.shape[0]
-    if x.stride(0) != 1:
-        x = x.t().contiguous().t()
-    ps = x.stride(1)
-    need = _lib.workspace_size(n, n_grid)
-    if workspace is None or workspace.numel() < need:
-        workspace = torch.empty(need, dtype=torch.uint8, device=x.device)
-    keys = torch.empty(n, dtype=torch.int32, device=x.device)
-    perm = torch.empty(n, dtype=torch.int32, device=x.device)
-    with torch.cuda.device(x.device):
-        s = torch.cuda.current_stream().cuda_stream
-        _lib.check(lib.pm_bin_sort(x.data_ptr(), n, ps, int(n_grid), float(inv_dx), keys.data_ptr(),
-                                   perm.data_ptr(), workspace.data_ptr(), need, s), "pm_bin_sort")
-    return keys.to(torch.int64), perm.to(torch.int64)
+    from . import ops  # noqa: F401
+    return torch.ops.peelmpm.bin_sort(x, int(n_grid), float(inv_dx))
 
 
 # --------------------------------------------------------------------------- solver
@@ -525,13 +507,10 @@ class AnisoMPM:
         self._grip_tags(grips)
         prm = self._build_params(grips)
         self._ensure_ws()
-        P = self._particles()
+        from . import ops
         clk = self._clock(time, self._step)
-        with torch.cuda.device(self.device):
-            s = torch.cuda.current_stream().cuda_stream
-            rc = self._lib.pm_substep(C.byref(prm), C.byref(P), self._ws.data_ptr(), self._ws_bytes,
-                                      C.byref(clk), s)
-        _lib.check(rc, "pm_substep")
+        torch.ops.peelmpm.substep(self._S, self._allow, self._imask if self._iface_used else None, self._tag,
+                                  self._ws, ops.struct_bytes(prm), ops.struct_bytes(clk), self.n)
         self._step += 1
 
     def run_frame(self, n_sub: int, time0: float = 0.0):

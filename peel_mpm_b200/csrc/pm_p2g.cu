@@ -38,12 +38,23 @@ __device__ __forceinline__ float tmax(float a, float b) { return (a != a || b !=
 // When `rec` is set (recording a substep for the adjoint) the polar
 // decomposition (R, V, S) and, on damage steps, phi are written to its planes:
 // rec[k * rs + p] for R (k 0..8), V (9..17), S (18..20), phi (21).
+// Per-particle inputs of k_stress, all loaded before any store: the state
+// planes share one buffer, so a store would otherwise keep later loads from
+// being issued early.
+struct StressIn {
+    float F[9], C[9], A0[9], v[3], x[3];
+    float d, lap, Dh, mu, lam, sc, eta, zeta, l0, res, vol0, m;
+    bool allow;
+    int grip;
+};
+
 __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &P, long long p, bool do_damage,
-                                             float tau[9], float *rec = nullptr, long long rs = 0) {
+                                             const StressIn &in, float tau[9], float &d_out, float *rec = nullptr,
+                                             long long rs = 0) {
     const long long ps = P.ps;
     float F[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = P.F[k * ps + p];
+    for (int k = 0; k < 9; ++k) F[k] = in.F[k];
     float Cg[9];   // C = F^T F (615)
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -90,7 +101,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
         for (int k = 0; k < 9; ++k) P.F[k * ps + p] = F[k];
     }
     const float J = clamp_min(S[0] * S[1] * S[2], 1e-6f);            // (637)
-    const float mu = P.mu[p], lam = P.lam[p];
+    const float mu = in.mu, lam = in.lam;
     float tdev[9];
     {
         float FmR[9];
@@ -126,7 +137,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
         {
             float A0[9], RA[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) A0[k] = P.A0[k * ps + p];
+            for (int k = 0; k < 9; ++k) A0[k] = in.A0[k];
             mm3(R, A0, RA);
             mmt3(RA, R, A);                                          // A = R A0 R^T (661)
         }
@@ -134,7 +145,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
         mm3(A, sp, M);
         const float trMM = (M[0] * M[0] + M[1] * M[3] + M[2] * M[6]) + (M[3] * M[1] + M[4] * M[4] + M[5] * M[7]) +
                            (M[6] * M[2] + M[7] * M[5] + M[8] * M[8]);
-        const float sc = P.sigma_c[p];
+        const float sc = in.sc;
         const float phi = trMM / (sc * sc);                          // (663-664)
         if (rec) rec[21 * rs + p] = phi;
         if (P.phi) P.phi[p] = phi;
@@ -152,22 +163,25 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
             }
             P.phi_shear[p] = phs;
         }
-        const float drive = P.zeta[p] * relu(phi - 1.0f);
-        const float dh0 = P.D_hist[p];
+        const float drive = in.zeta * relu(phi - 1.0f);
+        const float dh0 = in.Dh;
         const float Dh = tmax(dh0, drive);
         P.D_hist[p] = Dh;                                            // history max (679)
-        const float d = P.d[p];
-        const float l0 = P.l0[p];
-        const float resist = d - (l0 * l0) * P.lap[p];
+        const float d = in.d;
+        const float l0 = in.l0;
+        const float resist = d - (l0 * l0) * in.lap;
         const float ddot = relu((1.0f - d) * Dh - resist);           // (681-682)
         const float dt_dmg = (float)(prm.dt * (double)prm.damage_every);
-        float dn = d + (dt_dmg / P.eta[p]) * ddot;
+        float dn = d + (dt_dmg / in.eta) * ddot;
         dn = dn < 0.0f ? 0.0f : dn;
         dn = dn > 1.0f ? 1.0f : dn;                                  // (683-684)
-        if (P.allow[p]) P.d[p] = tmax(dn, d);                        // monotone, where allowed (685)
+        if (in.allow) {                                              // monotone, where allowed (685)
+            d_out = tmax(dn, d);
+            P.d[p] = d_out;
+        }
     }
-    const float d = P.d[p];
-    const float res = P.residual[p];
+    const float d = d_out;
+    const float res = in.res;
     const float omd = 1.0f - d;
     const float g = (omd * omd) * (1.0f - res) + res;                // (688)
     const float vdeg = (J >= 1.0f) ? g : 1.0f;                       // (690)
@@ -225,7 +239,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
 // with fx = X - floor(X - 0.5) per axis for particles whose stencil needs no
 // clamping (regular, base cell in [1, n_grid-4]) and the position x otherwise.
 template <class SC>
-__global__ void __launch_bounds__(256, 4) k_stress(const SC sc, const Parts P, const WS w) {
+__global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, const WS w) {
     // particle order: the state reads and writes are coalesced; the payload
     // goes to the particle's sorted position
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -238,29 +252,56 @@ __global__ void __launch_bounds__(256, 4) k_stress(const SC sc, const Parts P, c
     const float inv_dx = (float)prm.inv_dx;
     const Ctrl *ctrl = w.ctrl + sid;
     const bool do_damage = ctrl->any_allow != 0 && (ctrl->step % (long long)prm.damage_every) == 0;
+    StressIn in;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        in.F[k] = P.F[k * ps + p];
+        in.C[k] = P.C[k * ps + p];
+        in.A0[k] = do_damage ? P.A0[k * ps + p] : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        in.v[k] = P.v[k * ps + p];
+        in.x[k] = P.x[k * ps + p];
+    }
+    in.d = P.d[p];
+    in.lap = P.lap[p];
+    in.Dh = P.D_hist[p];
+    in.mu = P.mu[p];
+    in.lam = P.lam[p];
+    in.sc = P.sigma_c[p];
+    in.eta = P.eta[p];
+    in.zeta = P.zeta[p];
+    in.l0 = P.l0[p];
+    in.res = P.residual[p];
+    in.vol0 = P.vol0[p];
+    in.m = P.mass[p];
+    in.allow = P.allow[p] != 0;
+    in.grip = P.grip_tag ? P.grip_tag[p] : -1;
     float tau[9];
-    constitutive(prm, P, p, do_damage, tau, w.tape_pol, w.tape_aff_stride);
-    float v[3] = {P.v[p], P.v[ps + p], P.v[2 * ps + p]};
-    if (P.grip_tag) {                                                // particle BCs (601-602)
-        const int g = P.grip_tag[p];
+    float d_new = in.d;
+    constitutive(prm, P, p, do_damage, in, tau, d_new, w.tape_pol, w.tape_aff_stride);
+    float v[3] = {in.v[0], in.v[1], in.v[2]};
+    {                                                                // particle BCs (601-602)
+        const int g = in.grip;
         if (g >= 0 && g < prm.n_grips) {
             const double f = prm.grips[g].ramp > 0.0 ? fmin(ctrl->time / prm.grips[g].ramp, 1.0) : 1.0;
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) v[ax] = (float)(prm.grips[g].vel[ax] * f);
         }
     }
-    const float m = P.mass[p];
+    const float m = in.m;
     // stress_coeff = -dt*vol0*4*inv_dx*inv_dx; affine = coeff*tau + m*C (711-713)
     const float coeff =
-        __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), P.vol0[p]), 4.0f), inv_dx), inv_dx);
+        __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), in.vol0), 4.0f), inv_dx), inv_dx);
     float aff[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) aff[k] = coeff * tau[k] + m * P.C[k * ps + p];
+    for (int k = 0; k < 9; ++k) aff[k] = coeff * tau[k] + m * in.C[k];
     float xp[3], fx[3];
     bool reg = true;
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        xp[ax] = P.x[ax * ps + p];
+        xp[ax] = in.x[ax];
         const float X = __fmul_rn(xp[ax], inv_dx);
         const float fb = floorf(__fsub_rn(X, 0.5f));
         reg = reg && (fb >= 1.0f) && (fb <= (float)(ng - 4));
@@ -268,7 +309,7 @@ __global__ void __launch_bounds__(256, 4) k_stress(const SC sc, const Parts P, c
     }
     float4 *dst = w.payload + 5 * s;
     dst[0] = reg ? make_float4(fx[0], fx[1], fx[2], m) : make_float4(xp[0], xp[1], xp[2], m);
-    dst[1] = make_float4(m * v[0], m * v[1], m * v[2], P.d[p]);
+    dst[1] = make_float4(m * v[0], m * v[1], m * v[2], d_new);
     dst[2] = make_float4(aff[0], aff[1], aff[2], aff[3]);
     dst[3] = make_float4(aff[4], aff[5], aff[6], aff[7]);
     dst[4] = make_float4(aff[8], reg ? 1.0f : 0.0f, 0.0f, 0.0f);
