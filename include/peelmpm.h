@@ -279,6 +279,25 @@ int pm_batch_substep(int32_t n_scenes, const int64_t *n, const int32_t *n_grid, 
 int pm_batch_read_status(const void *ws, size_t ws_bytes, int32_t n_scenes, const int64_t *n, const int32_t *n_grid,
                          pm_status_info *out, void *stream);
 
+/* ---------------------------------------------------------------- observables */
+
+/* Per-frame reductions of the reference's experiment loop (peel_test.py:263-307)
+ * on the device, without a host synchronisation per frame.  Particles carry a
+ * group id (group[p] in [0, n_groups), -1 = none; group NULL = all in group 0).
+ * For each group g, row[g * PM_OBS_VALUES + k] accumulates (row zeroed by the
+ * caller; one row per frame): k = 0 max phi, 1 max phi_shear, 2 sum of d,
+ * 3 max d, 4 count of d > d_threshold, 5 count, 6 sum of y.  phi_peak /
+ * phi_shear_peak (NULL to skip) keep per-particle running maxima.  status[1]
+ * counts particles with non-finite x or d; status[0] (initialise to -1)
+ * becomes the first frame whose group `onset_group` has a broken fraction
+ * (k4 / k5) above onset_fraction, and at that frame d and x are copied to
+ * snap_d / snap_x (3 planes of snap_stride; NULL to skip). */
+#define PM_OBS_MAX_GROUPS 8
+#define PM_OBS_VALUES 8
+int pm_observe(const pm_particles *P, const int8_t *group, int32_t n_groups, float d_threshold, float *row,
+               float *phi_peak, float *phi_shear_peak, int32_t *status, int32_t onset_group, float onset_fraction,
+               int32_t frame, float *snap_d, float *snap_x, int64_t snap_stride, void *stream);
+
 /* ---------------------------------------------------------------- helpers */
 
 /* Batched 3x3 symmetric eigendecomposition by 5-sweep cyclic Jacobi, A

@@ -22,8 +22,9 @@ EXPORTS = (
     "pm_grid_update", "pm_g2p", "pm_read_status", "pm_sym_eig", "pm_bin_sort", "pm_bin_sort_static",
     "pm_batch_workspace_size", "pm_batch_workspace_layout", "pm_batch_workspace_init", "pm_batch_set_params",
     "pm_batch_workspace_release", "pm_batch_substep", "pm_batch_read_status",
-    "pm_tape_size", "pm_tape_init", "pm_substep_record", "pm_substep_adjoint",
+    "pm_tape_size", "pm_tape_init", "pm_substep_record", "pm_substep_adjoint", "pm_observe",
 )
+PM_OBS_MAX_GROUPS, PM_OBS_VALUES = 8, 8
 PM_MAX_BATCH_SCENES = 4096
 PM_BIN_STATIC_MAX_N = 262144
 
@@ -138,6 +139,8 @@ def load():
         "pm_tape_init": (C.c_int, [vp, sz, i64, i32, i32, vp]),
         "pm_substep_record": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), vp, sz, C.POINTER(pm_clock),
                                         vp, sz, i32, i32, vp]),
+        "pm_observe": (C.c_int, [C.POINTER(pm_particles), vp, i32, C.c_float, vp, vp, vp, vp, i32, C.c_float, i32,
+                                 vp, vp, i64, vp]),
         "pm_substep_adjoint": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), C.POINTER(pm_particles),
                                          C.POINTER(pm_state_adj), C.POINTER(pm_state_adj), C.POINTER(pm_param_adj),
                                          vp, sz, i32, i32, vp]),

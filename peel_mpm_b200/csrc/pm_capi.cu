@@ -317,6 +317,21 @@ int pm_substep_adjoint(const pm_params *prm, const pm_particles *pre, const pm_p
     return cuda_check("pm_substep_adjoint");
 }
 
+int pm_observe(const pm_particles *P, const int8_t *group, int32_t n_groups, float d_threshold, float *row,
+               float *phi_peak, float *phi_shear_peak, int32_t *status, int32_t onset_group, float onset_fraction,
+               int32_t frame, float *snap_d, float *snap_x, int64_t snap_stride, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_particles(P, false))) return rc;
+    if (!P->d) return fail(PM_ERR_ARG, "d is NULL");
+    if (n_groups < 1 || n_groups > PM_OBS_MAX_GROUPS) return fail(PM_ERR_ARG, "n_groups must be in [1, 8]");
+    if (!row || !status) return fail(PM_ERR_ARG, "row or status is NULL");
+    if (onset_group >= n_groups) return fail(PM_ERR_ARG, "onset_group out of range");
+    if (snap_x && snap_stride < P->n) return fail(PM_ERR_ARG, "snap_stride < n");
+    pm::launch_observe(pm::make_parts(P), group, n_groups, d_threshold, row, phi_peak, phi_shear_peak, status,
+                       onset_group, onset_fraction, frame, snap_d, snap_x, snap_stride, (cudaStream_t)stream);
+    return cuda_check("pm_observe");
+}
+
 int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, pm_status_info *out, void *stream) {
     int rc;
     if ((rc = check_device())) return rc;

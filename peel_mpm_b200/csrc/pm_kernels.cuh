@@ -39,6 +39,12 @@ void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, c
                     const pm_state_adj &aout, const pm_param_adj &grads, const TapeLayout &T, void *tape, int slot,
                     cudaStream_t s);
 
+// Per-frame observables (pm_observe.cu): values per group per frame row.
+constexpr int kObsValues = 8;   // phi max, phi_shear max, d sum, d max, n(d > thr), count, y sum, unused
+int launch_observe(const Parts &P, const int8_t *group, int n_groups, float thr, float *row, float *phi_pp,
+                   float *psh_pp, int *status, int onset_group, float onset_frac, int frame, float *snap_d,
+                   float *snap_x, long long snap_stride, cudaStream_t s);
+
 // Argument checks and error reporting of the C ABI (pm_capi.cu), shared with
 // the other entry-point files.
 int report_error(int code, const char *msg);
