@@ -440,6 +440,8 @@ def run_ours(args):
 
     sim, sc = build_sim(torch, device, seed=rank)
     n = sim.n
+    from peel_mpm_b200 import autotune
+    tuned = autotune.tune(sim)       # P2G tile for this size bucket (state restored afterwards)
     t0 = 0.0
     chunk = min(100, args.steps)
     for i in range(args.warmup):
@@ -523,7 +525,8 @@ def run_ours(args):
                 "config": {"workload": "plain AnisoMPM substep, 1,048,576 particles, 128^3 grid (seeded slab)",
                            "particles": n, "n_grid": sim.n_grid, "dt": sim.dt, "parallelism": f"replicas{world}",
                            "l2": "inputs larger than L2 (particle state ~290 MB)",
-                           "graph_substeps": chunk},
+                           "graph_substeps": chunk, "p2g_range": tuned,
+                           "p2g_range_ms": autotune._CACHE[autotune.bucket(sim)]["ms"]},
                 "clocks": clocks.summary(), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches_per_step * args.steps, "status": st}
         line.update(forms)
