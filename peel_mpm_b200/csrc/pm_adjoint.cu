@@ -758,15 +758,18 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
     const int qn = any ? qd[0] * qd[1] * qd[2] : 0, cn = any ? cd[0] * cd[1] * cd[2] : 0;
     const bool tile = any && qn <= kAQ && cn <= kAC;
     if (tile) {   // regular nodes lie inside the grid
+        const FastDiv qyz = make_fastdiv(qd[1] * qd[2]), qz = make_fastdiv(qd[2]);
         for (int i = tid; i < qn; i += blockDim.x) {
-            const int gx = lo[0] + i / (qd[1] * qd[2]), gy = lo[1] + (i / qd[2]) % qd[1], gz = lo[2] + i % qd[2];
+            const int ix = fdiv(i, qyz), r = i - ix * qyz.d, iy = fdiv(r, qz);
+            const int gx = lo[0] + ix, gy = lo[1] + iy, gz = lo[2] + r - iy * qz.d;
             const long long node = ((long long)gx * ng + gy) * ng + gz;
             sv[i] = gvel[node];
             sa[i] = A[node];
         }
+        const FastDiv cyz = make_fastdiv(cd[1] * cd[2]), cz = make_fastdiv(cd[2]);
         for (int i = tid; i < cn; i += blockDim.x) {
-            const int gx = lo[0] - 1 + i / (cd[1] * cd[2]), gy = lo[1] - 1 + (i / cd[2]) % cd[1],
-                      gz = lo[2] - 1 + i % cd[2];
+            const int ix = fdiv(i, cyz), r = i - ix * cyz.d, iy = fdiv(r, cz);
+            const int gx = lo[0] - 1 + ix, gy = lo[1] - 1 + iy, gz = lo[2] - 1 + r - iy * cz.d;
             sb[i] = B[((long long)gx * ng + gy) * ng + gz];
         }
     }

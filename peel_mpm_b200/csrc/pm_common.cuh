@@ -237,6 +237,18 @@ struct BatchScenes {
     __device__ __forceinline__ long long cta_base(int s) const { return ctab[s]; }
 };
 
+// Division of a small non-negative int by a runtime divisor through a float
+// reciprocal (tile index -> coordinates in the staging loops): with
+// y = (i + 0.5) / d the fraction of y is at least 0.5/d from an integer and
+// the two float roundings move y by at most y * 2^-23, which stays below
+// 0.5/d for i < 2^22, so the truncation is floor(i / d) exactly.
+struct FastDiv {
+    int d;
+    float r;
+};
+__device__ __forceinline__ FastDiv make_fastdiv(int d) { return FastDiv{d, __frcp_rn((float)d)}; }
+__device__ __forceinline__ int fdiv(int i, const FastDiv &f) { return __float2int_rz(((float)i + 0.5f) * f.r); }
+
 // ------------------------------------------------------------------ cells
 // floor(v).to(long) then clamp, as the reference forms base cells: NaN or a
 // value outside int64 becomes INT64_MIN in torch and clamps to node 0; values

@@ -366,13 +366,16 @@ __global__ void __launch_bounds__(kG2PThreads, 4) k_g2p(const SC scn, const Part
     const long long qn = any ? (long long)qd[0] * qd[1] * qd[2] : 0, cn = any ? (long long)cd[0] * cd[1] * cd[2] : 0;
     const bool tile = any && qn <= kGTQ && cn <= kGTC;
     if (tile) {   // regular nodes lie inside the grid, so no bounds test is needed
+        const FastDiv qyz = make_fastdiv(qd[1] * qd[2]), qz = make_fastdiv(qd[2]);
         for (int i = tid; i < qn; i += kG2PThreads) {
-            const int gx = lo[0] + i / (qd[1] * qd[2]), gy = lo[1] + (i / qd[2]) % qd[1], gz = lo[2] + i % qd[2];
+            const int ix = fdiv(i, qyz), r = i - ix * qyz.d, iy = fdiv(r, qz);
+            const int gx = lo[0] + ix, gy = lo[1] + iy, gz = lo[2] + r - iy * qz.d;
             sq[i] = gvel[((long long)gx * ng + gy) * ng + gz];
         }
+        const FastDiv cyz = make_fastdiv(cd[1] * cd[2]), cz = make_fastdiv(cd[2]);
         for (int i = tid; i < cn; i += kG2PThreads) {
-            const int gx = lo[0] - 1 + i / (cd[1] * cd[2]), gy = lo[1] - 1 + (i / cd[2]) % cd[1],
-                      gz = lo[2] - 1 + i % cd[2];
+            const int ix = fdiv(i, cyz), r = i - ix * cyz.d, iy = fdiv(r, cz);
+            const int gx = lo[0] - 1 + ix, gy = lo[1] - 1 + iy, gz = lo[2] - 1 + r - iy * cz.d;
             sc[i] = ggd[((long long)gx * ng + gy) * ng + gz];
         }
     }

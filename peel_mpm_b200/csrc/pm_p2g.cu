@@ -695,8 +695,10 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const W
         __syncthreads();
         {   // quadratic footprint: local nodes [cmin, cmin + cext + 2) per axis
             const int ex = cext[0] + 2, ey = cext[1] + 2, ez = cext[2] + 2;
+            const FastDiv fyz = make_fastdiv(ey * ez), fz = make_fastdiv(ez);
             for (int i = tid; i < ex * ey * ez; i += kP2GThreads) {
-                const int tx = cmin[0] + i / (ey * ez), ty = cmin[1] + (i / ez) % ey, tz = cmin[2] + i % ez;
+                const int ix = fdiv(i, fyz), r = i - ix * fyz.d, iy = fdiv(r, fz);
+                const int tx = cmin[0] + ix, ty = cmin[1] + iy, tz = cmin[2] + r - iy * fz.d;
                 const int li = (tx * kQE + ty) * kQE + tz;
                 const float a0 = qt[li], a1 = qt[kQN + li], a2 = qt[2 * kQN + li], a3 = qt[3 * kQN + li];
                 if (a0 != 0.0f || a1 != 0.0f || a2 != 0.0f || a3 != 0.0f) {
@@ -709,8 +711,10 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const W
         }
         {   // cubic footprint: local nodes [cmin, cmin + cext + 4) per axis (tile origin 8b-1)
             const int ex = cext[0] + 4, ey = cext[1] + 4, ez = cext[2] + 4;
+            const FastDiv fyz = make_fastdiv(ey * ez), fz = make_fastdiv(ez);
             for (int i = tid; i < ex * ey * ez; i += kP2GThreads) {
-                const int tx = cmin[0] + i / (ey * ez), ty = cmin[1] + (i / ez) % ey, tz = cmin[2] + i % ez;
+                const int ix = fdiv(i, fyz), r = i - ix * fyz.d, iy = fdiv(r, fz);
+                const int tx = cmin[0] + ix, ty = cmin[1] + iy, tz = cmin[2] + r - iy * fz.d;
                 const int li = (tx * kCE + ty) * kCE + tz;
                 const float a4 = ct[li], a5 = ct[kCN + li];
                 if (a4 != 0.0f || a5 != 0.0f) {
