@@ -129,7 +129,7 @@ const char *pm_last_error(void);
 
 /* sizeof the ABI structs, for binding checks: 0 pm_params, 1 pm_particles,
  * 2 pm_clock, 3 pm_status_info, 4 pm_ws_layout, 5 pm_grip, 6 pm_collider,
- * 7 pm_batch_layout, 8 pm_state_adj, 9 pm_param_adj. */
+ * 7 pm_batch_layout, 8 pm_state_adj, 9 pm_param_adj, 10 pm_camera, 11 pm_render_params. */
 size_t pm_struct_size(int32_t which);
 
 /* One-time set-up of the current device (kernel attributes).  Every entry
@@ -297,6 +297,45 @@ int pm_batch_read_status(const void *ws, size_t ws_bytes, int32_t n_scenes, cons
 int pm_observe(const pm_particles *P, const int8_t *group, int32_t n_groups, float d_threshold, float *row,
                float *phi_peak, float *phi_shear_peak, int32_t *status, int32_t onset_group, float onset_fraction,
                int32_t frame, float *snap_d, float *snap_x, int64_t snap_stride, void *stream);
+
+/* ---------------------------------------------------------------- renderer */
+
+/* Gaussian-splat renderer of the reference's orange demo (render.py:71-162),
+ * as CUDA kernels writing a headless (height, width, 3) float image in
+ * [0, 1].  Camera: X_cam = X_world R + T (row vectors; the 3DGS convention of
+ * Camera.world_to_cam), pinhole fx, fy, principal point at the image centre. */
+typedef struct pm_camera {
+    float R[9];                      /* row-major */
+    float T[3];
+    float fx, fy;
+    int32_t width, height;
+} pm_camera;
+
+typedef struct pm_render_params {
+    float bg[3];                     /* background colour */
+    float scale_modifier;
+    int32_t r_max;                   /* footprint radius cap in pixels */
+    float tau;                       /* soft z-buffer depth scale; <= 0: 0.02 x median depth of the drawn splats */
+    float near;                      /* splats with camera depth <= near are dropped */
+    float max_raw_radius;            /* splats whose unclamped radius reaches this are dropped */
+} pm_render_params;
+
+int pm_render_workspace_size(int64_t n, int32_t width, int32_t height, size_t *bytes);
+/* xyz (n,3), cov3d (n,3,3) row-major, color (n,3): device float arrays.  The
+ * reference's per-splat opacity does not enter its compositing, so it is not
+ * an argument. */
+int pm_render_gaussians(const pm_camera *cam, const pm_render_params *rp, const float *xyz, const float *cov3d,
+                        const float *color, int64_t n, float *image, void *ws, size_t ws_bytes, void *stream);
+
+/* Gaussian carrying (run_orange.py:116-133): gaussian i, bound to particle
+ * bind[i] (device int32, out-of-range ids are skipped), gets position
+ * affine (x) + F off0_i, covariance F cov0_i F^T and colour
+ * color0_i (1 - crack_tint d) from its particle's current state; affine is a
+ * device 3x4 row-major [A | t] (the demo's sim-to-world map); off0 (n,3),
+ * cov0 (n,3,3), color0 (n,3), outputs pos (n,3), cov (n,3,3), color (n,3). */
+int pm_carry_gaussians(const pm_particles *P, const int32_t *bind, const float *off0, const float *cov0,
+                       const float *color0, int64_t g_n, const float *affine, float crack_tint, float *pos, float *cov,
+                       float *color, void *stream);
 
 /* ---------------------------------------------------------------- helpers */
 

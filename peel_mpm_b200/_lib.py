@@ -23,6 +23,7 @@ EXPORTS = (
     "pm_batch_workspace_size", "pm_batch_workspace_layout", "pm_batch_workspace_init", "pm_batch_set_params",
     "pm_batch_workspace_release", "pm_batch_substep", "pm_batch_read_status",
     "pm_tape_size", "pm_tape_init", "pm_substep_record", "pm_substep_adjoint", "pm_observe",
+    "pm_render_workspace_size", "pm_render_gaussians", "pm_carry_gaussians",
 )
 PM_OBS_MAX_GROUPS, PM_OBS_VALUES = 8, 8
 PM_MAX_BATCH_SCENES = 4096
@@ -89,8 +90,18 @@ class pm_param_adj(C.Structure):
     _fields_ = [("plane_stride", C.c_int64)] + [(f, C.c_void_p) for f in ("mu", "lam", "sigma_c", "A0")]
 
 
+class pm_camera(C.Structure):
+    _fields_ = [("R", C.c_float * 9), ("T", C.c_float * 3), ("fx", C.c_float), ("fy", C.c_float),
+                ("width", C.c_int32), ("height", C.c_int32)]
+
+
+class pm_render_params(C.Structure):
+    _fields_ = [("bg", C.c_float * 3), ("scale_modifier", C.c_float), ("r_max", C.c_int32), ("tau", C.c_float),
+                ("near", C.c_float), ("max_raw_radius", C.c_float)]
+
+
 STRUCTS = (pm_params, pm_particles, pm_clock, pm_status_info, pm_ws_layout, pm_grip, pm_collider, pm_batch_layout,
-           pm_state_adj, pm_param_adj)
+           pm_state_adj, pm_param_adj, pm_camera, pm_render_params)
 
 _lib = None
 
@@ -139,6 +150,11 @@ def load():
         "pm_tape_init": (C.c_int, [vp, sz, i64, i32, i32, vp]),
         "pm_substep_record": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), vp, sz, C.POINTER(pm_clock),
                                         vp, sz, i32, i32, vp]),
+        "pm_render_workspace_size": (C.c_int, [i64, i32, i32, C.POINTER(sz)]),
+        "pm_carry_gaussians": (C.c_int, [C.POINTER(pm_particles), vp, vp, vp, vp, i64, vp, C.c_float, vp, vp, vp,
+                                         vp]),
+        "pm_render_gaussians": (C.c_int, [C.POINTER(pm_camera), C.POINTER(pm_render_params), vp, vp, vp, i64, vp, vp,
+                                          sz, vp]),
         "pm_observe": (C.c_int, [C.POINTER(pm_particles), vp, i32, C.c_float, vp, vp, vp, vp, i32, C.c_float, i32,
                                  vp, vp, i64, vp]),
         "pm_substep_adjoint": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), C.POINTER(pm_particles),

@@ -102,6 +102,8 @@ size_t pm_struct_size(int32_t which) {
         case 7: return sizeof(pm_batch_layout);
         case 8: return sizeof(pm_state_adj);
         case 9: return sizeof(pm_param_adj);
+        case 10: return sizeof(pm_camera);
+        case 11: return sizeof(pm_render_params);
         default: return 0;
     }
 }
@@ -330,6 +332,44 @@ int pm_observe(const pm_particles *P, const int8_t *group, int32_t n_groups, flo
     pm::launch_observe(pm::make_parts(P), group, n_groups, d_threshold, row, phi_peak, phi_shear_peak, status,
                        onset_group, onset_fraction, frame, snap_d, snap_x, snap_stride, (cudaStream_t)stream);
     return cuda_check("pm_observe");
+}
+
+// ------------------------------------------------------------------ renderer
+int pm_render_workspace_size(int64_t n, int32_t width, int32_t height, size_t *bytes) {
+    if (!bytes) return fail(PM_ERR_ARG, "bytes is NULL");
+    if (n < 0 || n >= (1LL << 31) || width < 1 || height < 1 || (int64_t)width * height > (1LL << 30))
+        return fail(PM_ERR_ARG, "bad n, width or height");
+    *bytes = pm::render_workspace_bytes(n, (long long)width * height);
+    return PM_OK;
+}
+
+int pm_render_gaussians(const pm_camera *cam, const pm_render_params *rp, const float *xyz, const float *cov3d,
+                        const float *color, int64_t n, float *image, void *ws, size_t ws_bytes, void *stream) {
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (!cam || !rp || !image) return fail(PM_ERR_ARG, "camera, parameters or image is NULL");
+    if (n > 0 && (!xyz || !cov3d || !color)) return fail(PM_ERR_ARG, "NULL gaussian array");
+    if (rp->r_max < 1) return fail(PM_ERR_ARG, "r_max must be >= 1");
+    size_t need = 0;
+    if ((rc = pm_render_workspace_size(n, cam->width, cam->height, &need))) return rc;
+    if (!ws || ((uintptr_t)ws & 255) != 0 || ws_bytes < need)
+        return fail(PM_ERR_WORKSPACE, "render workspace missing, misaligned or too small");
+    pm::launch_render(*cam, *rp, xyz, cov3d, color, n, image, ws, (cudaStream_t)stream);
+    return cuda_check("pm_render_gaussians");
+}
+
+int pm_carry_gaussians(const pm_particles *P, const int32_t *bind, const float *off0, const float *cov0,
+                       const float *color0, int64_t g_n, const float *affine, float crack_tint, float *pos, float *cov,
+                       float *color, void *stream) {
+    int rc;
+    if ((rc = check_device()) || (rc = check_particles(P, false))) return rc;
+    if (!P->F || (crack_tint > 0.0f && !P->d)) return fail(PM_ERR_ARG, "F (and d for the crack tint) required");
+    if (g_n < 0) return fail(PM_ERR_ARG, "g_n < 0");
+    if (g_n > 0 && (!bind || !off0 || !cov0 || !color0 || !affine || !pos || !cov || !color))
+        return fail(PM_ERR_ARG, "NULL array");
+    pm::launch_carry(pm::make_parts(P), bind, off0, cov0, color0, g_n, affine, crack_tint, pos, cov, color,
+                     (cudaStream_t)stream);
+    return cuda_check("pm_carry_gaussians");
 }
 
 int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, pm_status_info *out, void *stream) {

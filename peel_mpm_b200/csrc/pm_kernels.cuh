@@ -45,6 +45,14 @@ int launch_observe(const Parts &P, const int8_t *group, int n_groups, float thr,
                    float *psh_pp, int *status, int onset_group, float onset_frac, int frame, float *snap_d,
                    float *snap_x, long long snap_stride, cudaStream_t s);
 
+// Gaussian-splat renderer (pm_render.cu).
+size_t render_workspace_bytes(long long n, long long npix);
+void launch_render(const pm_camera &cam, const pm_render_params &rp, const float *xyz, const float *cov,
+                   const float *color, long long n, float *img, void *ws, cudaStream_t s);
+void launch_carry(const Parts &P, const int *bind, const float *off0, const float *cov0, const float *color0,
+                  long long g_n, const float *affine, float tint, float *pos, float *cov, float *color,
+                  cudaStream_t s);
+
 // Argument checks and error reporting of the C ABI (pm_capi.cu), shared with
 // the other entry-point files.
 int report_error(int code, const char *msg);
