@@ -2,7 +2,7 @@
 batched and differentiable forms.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--form all|plain|batched|adjoint] [--fd-dirs D]
+                    [--form all|plain|batched|adjoint|render] [--fd-dirs D]
 
 Headline workload (``value``): the plain form on the 1,048,576-particle slab on
 a 128^3 grid (seeded synthetic scene: vMF fibers about x with kappa=20,
@@ -25,6 +25,10 @@ Beside it, in the same JSON line:
                  run with E*1.2, fibers rotated 15 degrees about z and
                  sigma_c*0.8, with a central-difference check along random
                  directions.
+  render      -- the 1M slab's particles carrying one gaussian each
+                 (positions x + F off0, covariances F cov0 F^T, damage tint)
+                 and EWA-splatted to a 1280x720 image: median carry and
+                 render times per frame.
 
 Arms:
   ours       -- the sm_100a path.  ``value``: particle state resident in HBM,
@@ -72,7 +76,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--form", default="all", choices=["all", "plain", "batched", "adjoint"])
+    ap.add_argument("--form", default="all", choices=["all", "plain", "batched", "adjoint", "render"])
     ap.add_argument("--fd-dirs", type=int, default=0,
                     help="central-difference directions of the adjoint check on the float32 forward (the 100-substep "
                          "rollout crosses fracture, where the gradient is ill-conditioned; the float64 check at "
@@ -414,6 +418,50 @@ def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
             "fd_check": fd}
 
 
+def bench_render(torch, device, sim, frames=10, warmup=3, width=1280, height=720):
+    """Gaussian carrying + EWA splat rendering of the 1M slab: one gaussian per
+    particle (isotropic, radius dx/2, coloured by height, tinted by damage),
+    a 1280x720 camera facing the slab, tau from the median depth."""
+    from peel_mpm_b200.render import Camera, carry_gaussians, render_gaussians
+    dev = sim.device
+    x = sim.x
+    n = sim.n
+    lo, hi = x.min(0).values, x.max(0).values
+    c = (0.5 * (lo + hi)).cpu().numpy()
+    ext = float((hi - lo).max())
+    cam = Camera(R=np.eye(3), T=-c + np.array([0.0, 0.0, 2.0 * ext]), fx=1.6 * width, fy=1.6 * width,
+                 width=width, height=height, device=dev)
+    bind = torch.arange(n, dtype=torch.int32, device=dev)
+    off0 = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+    r = 0.5 * sim.dx
+    cov0 = (torch.eye(3, device=dev) * r * r).expand(n, 3, 3).contiguous()
+    h = (x[:, 1] - lo[1]) / max(float(hi[1] - lo[1]), 1e-6)
+    col0 = torch.stack([0.9 - 0.5 * h, 0.5 + 0.3 * h, 0.2 + 0.6 * h], 1).contiguous()
+    s = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    carry, render = [], []
+    for f in range(warmup + frames):
+        ev[0].record(s)
+        pos, cov, col = carry_gaussians(sim, bind, off0, cov0, col0, crack_tint=0.6)
+        ev[1].record(s)
+        img = render_gaussians(cam, pos, cov, col, None, bg=(1.0, 1.0, 1.0), r_max=12)
+        ev[2].record(s)
+        torch.cuda.synchronize()
+        if f >= warmup:
+            carry.append(ev[0].elapsed_time(ev[1]))
+            render.append(ev[1].elapsed_time(ev[2]))
+    carry_ms, render_ms = statistics.median(carry), statistics.median(render)
+    hbm, kind = peaks()
+    carry_bytes = n * (4 + 48 + 4 + 12 + 36 + 12 + 12 + 60)   # bind, F x d, off0 cov0 color0 in; pos cov color out
+    return {"gaussians": n, "width": width, "height": height, "r_max": 12,
+            "carry_ms": carry_ms, "render_ms": render_ms, "frame_ms": carry_ms + render_ms,
+            "value": n / ((carry_ms + render_ms) * 1e-3), "unit": "gaussians/s (carry + render)",
+            "carry_roofline": {"bound": "hbm", "achieved": carry_bytes / (carry_ms * 1e-3) / 1e9, "peak": hbm,
+                               "frac": carry_bytes / (carry_ms * 1e-3) / 1e9 / hbm, "unit": "GB/s",
+                               "peak_kind": kind, "algorithmic_bytes": carry_bytes},
+            "image_mean": float(img.mean())}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -510,6 +558,8 @@ def run_ours(args):
     forms = {}
     if args.form in ("all", "batched"):   # every rank takes its share of the scenes
         forms["batched"] = bench_batched(torch, device, rank, world, max_over_ranks, barrier)
+    if rank == 0 and args.form in ("all", "render"):
+        forms["render"] = bench_render(torch, device, sim)
     if rank == 0 and args.form in ("all", "adjoint"):
         forms["fwd_adjoint"] = bench_adjoint(torch, device, fd_dirs=args.fd_dirs)
 

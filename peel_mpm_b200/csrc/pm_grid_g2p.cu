@@ -98,75 +98,90 @@ __device__ __forceinline__ void resolve(float v[3], const float vc[3], const flo
     v[2] = vc[2] + t2 + keep * nn[2];
 }
 
-// One thread per node of the active blocks.  Reads and clears the P2G
-// accumulators, writes grid velocity and the normalised damage field
-// (anisompm.py:727-746, 777-779).
+// One thread per z-row of 4 nodes of an active 4^3 block: the row's scene,
+// parameters and node address are resolved once and its 4 nodes' loads are
+// independent.  Reads and clears the P2G accumulators, writes grid velocity
+// and the normalised damage field (anisompm.py:727-746, 777-779).
 template <class SC>
 __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
     const long long nact = min((long long)w.ctrl->n_active, w.n_blocks);
-    const long long items = nact * 64;
+    const long long items = nact * 16;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
          it += (long long)gridDim.x * blockDim.x) {
-        const int gb = w.block_list[it >> 6];
+        const int gb = w.block_list[it >> 4];
         const int sid = sc.of_gblock(gb);
         const pm_params &prm = sc.params(sid);
         const Ctrl *ctrl = w.ctrl + sid;
         const int ng = prm.n_grid, nbs = (ng + kBlockEdge - 1) / kBlockEdge;
+        const int b = (int)(gb - sc.gblock_base(sid));
+        const int l = (int)(it & 15);
+        const int bx = b / (nbs * nbs), by = (b / nbs) % nbs, bz = b % nbs;
+        const int ix = bx * kBlockEdge + (l >> 2), iy = by * kBlockEdge + (l & 3), iz0 = bz * kBlockEdge;
+        if (ix >= ng || iy >= ng) continue;
+        const int nz = min(kBlockEdge, ng - iz0);
+        const long long row = sc.node_base(sid) + ((long long)ix * ng + iy) * ng + iz0;
+        float4 mom[kBlockEdge];
+        float2 dmg[kBlockEdge];
+#pragma unroll
+        for (int k = 0; k < kBlockEdge; ++k) {
+            if (k < nz) {
+                mom[k] = w.g_mom[row + k];
+                dmg[k] = w.g_dmg[row + k];
+            }
+        }
         const float dt = (float)prm.dt;
         const float gdt[3] = {dt * (float)prm.gravity[0], dt * (float)prm.gravity[1], dt * (float)prm.gravity[2]};
         const float damp = (float)prm.grid_damp;
         const bool do_damp = prm.grid_damp != 1.0;
         const float dx = (float)prm.dx;
-        const int b = (int)(gb - sc.gblock_base(sid));
-        const int l = (int)(it & 63);
-        const int bx = b / (nbs * nbs), by = (b / nbs) % nbs, bz = b % nbs;
-        const int ix = bx * kBlockEdge + (l >> 4), iy = by * kBlockEdge + ((l >> 2) & 3), iz = bz * kBlockEdge + (l & 3);
-        if (ix >= ng || iy >= ng || iz >= ng) continue;
-        const long long node = sc.node_base(sid) + ((long long)ix * ng + iy) * ng + iz;
-        const float4 mom = w.g_mom[node];
-        const float2 dmg = w.g_dmg[node];
-        w.g_mom[node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        w.g_dmg[node] = make_float2(0.0f, 0.0f);
-        const bool active = mom.w > 1e-12f;
-        const float inv_m = active ? 1.0f / mom.w : 0.0f;
-        float v[3] = {mom.x * inv_m + gdt[0], mom.y * inv_m + gdt[1], mom.z * inv_m + gdt[2]};
-        if (do_damp) {
-            v[0] *= damp; v[1] *= damp; v[2] *= damp;
-        }
-        if (!active) v[0] = v[1] = v[2] = 0.0f;
-        if (active && prm.n_colliders > 0) {
-            const float pos[3] = {(float)ix * dx, (float)iy * dx, (float)iz * dx};
-            for (int c = 0; c < prm.n_colliders; ++c) {
-                const pm_collider col = prm.colliders[c];
-                const float *o = ctrl->col_origin[c];
-                const float *vc = ctrl->col_vel[c];
-                if (col.kind == 0) {   // halfspace_collider (847-867)
-                    const float nn[3] = {(float)col.normal[0], (float)col.normal[1], (float)col.normal[2]};
-                    const float sd = (pos[0] - o[0]) * nn[0] + (pos[1] - o[1]) * nn[1] + (pos[2] - o[2]) * nn[2];
-                    if (sd < 0.0f) resolve(v, vc, nn, col.mode == 1, (float)col.friction);
-                } else {               // sphere_collider (828-844)
-                    const float r0 = pos[0] - o[0], r1 = pos[1] - o[1], r2 = pos[2] - o[2];
-                    const float dist = sqrtf(r0 * r0 + r1 * r1 + r2 * r2);
-                    if (dist < (float)col.radius) {
-                        const float den = dist + 1e-9f;
-                        const float nn[3] = {r0 / den, r1 / den, r2 / den};
-                        resolve(v, vc, nn, col.mode == 1, (float)col.friction);
+        const int ncol = prm.n_colliders;
+#pragma unroll
+        for (int k = 0; k < kBlockEdge; ++k) {
+            if (k >= nz) continue;
+            const long long node = row + k;
+            w.g_mom[node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            w.g_dmg[node] = make_float2(0.0f, 0.0f);
+            const bool active = mom[k].w > 1e-12f;
+            const float inv_m = active ? 1.0f / mom[k].w : 0.0f;
+            float v[3] = {mom[k].x * inv_m + gdt[0], mom[k].y * inv_m + gdt[1], mom[k].z * inv_m + gdt[2]};
+            if (do_damp) {
+                v[0] *= damp; v[1] *= damp; v[2] *= damp;
+            }
+            if (!active) v[0] = v[1] = v[2] = 0.0f;
+            if (active && ncol > 0) {
+                const float pos[3] = {(float)ix * dx, (float)iy * dx, (float)(iz0 + k) * dx};
+                for (int c = 0; c < ncol; ++c) {
+                    const pm_collider col = prm.colliders[c];
+                    const float *o = ctrl->col_origin[c];
+                    const float *vc = ctrl->col_vel[c];
+                    if (col.kind == 0) {   // halfspace_collider (847-867)
+                        const float nn[3] = {(float)col.normal[0], (float)col.normal[1], (float)col.normal[2]};
+                        const float sd = (pos[0] - o[0]) * nn[0] + (pos[1] - o[1]) * nn[1] + (pos[2] - o[2]) * nn[2];
+                        if (sd < 0.0f) resolve(v, vc, nn, col.mode == 1, (float)col.friction);
+                    } else {               // sphere_collider (828-844)
+                        const float r0 = pos[0] - o[0], r1 = pos[1] - o[1], r2 = pos[2] - o[2];
+                        const float dist = sqrtf(r0 * r0 + r1 * r1 + r2 * r2);
+                        if (dist < (float)col.radius) {
+                            const float den = dist + 1e-9f;
+                            const float nn[3] = {r0 / den, r1 / den, r2 / den};
+                            resolve(v, vc, nn, col.mode == 1, (float)col.friction);
+                        }
                     }
                 }
             }
+            w.g_vel[node] = make_float4(v[0], v[1], v[2], mom[k].w);   // .w: node mass (read by the adjoint)
+            w.g_gd[node] = dmg[k].y > 1e-12f ? dmg[k].x / dmg[k].y : 0.0f;
+            if (w.g_sw) w.g_sw[node] = dmg[k].y;
         }
-        w.g_vel[node] = make_float4(v[0], v[1], v[2], mom.w);   // .w: node mass (read by the adjoint)
-        w.g_gd[node] = dmg.y > 1e-12f ? dmg.x / dmg.y : 0.0f;
-        if (w.g_sw) w.g_sw[node] = dmg.y;
     }
 }
 
 template <class SC>
 void launch_grid(const SC &sc, const WS &w, cudaStream_t s) {
-    const long long max_items = w.n_blocks * 64;
-    // a batch has many more active nodes than one scene and every item starts
+    const long long max_items = w.n_blocks * 16;
+    // a batch has many more active nodes than one scene and every row starts
     // with a dependent chain of table loads (scene lookup, parameters): give
-    // each item its own thread rather than a grid-stride loop
+    // each row its own thread rather than a grid-stride loop
     const long long cap = SC::batched ? 148LL * 64 : 148LL * 8;
     const int blocks = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, cap));
     k_grid<SC><<<blocks, 256, 0, s>>>(sc, w);

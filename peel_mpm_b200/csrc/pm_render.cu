@@ -26,7 +26,8 @@ struct RenderWS {
     int *list;        // compacted drawn splats
     unsigned *count;  // [0] drawn splats
     float *tau;       // [0] tau, [1] 1 / tau
-    float *zmin, *csum, *wsum, *logrev;
+    float *zmin, *logrev;
+    float4 *csum;     // per pixel: colour sums (x, y, z) and weight sum (w)
     WS sort;          // key / value buffers of the median sort
 };
 
@@ -35,10 +36,7 @@ __global__ void __launch_bounds__(256) k_splat_clear(RenderWS r, long long npix,
     if (i == 0) *count = 0;
     if (i < npix) {
         r.zmin[i] = __int_as_float(0x7f800000);   // +inf
-        r.csum[3 * i] = 0.0f;
-        r.csum[3 * i + 1] = 0.0f;
-        r.csum[3 * i + 2] = 0.0f;
-        r.wsum[i] = 0.0f;
+        r.csum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         r.logrev[i] = 0.0f;
     }
 }
@@ -125,25 +123,52 @@ __global__ void k_splat_tau(RenderWS r, float tau_given, const unsigned *sorted)
     r.tau[1] = 1.0f / (tau > 1e-6f ? tau : 1e-6f);
 }
 
-__device__ __forceinline__ float splat_alpha(const RenderWS &r, int g, int px, int py) {
-    const float dx = (float)px + 0.5f - r.u[g], dy = (float)py + 0.5f - r.v[g];
-    const float power = -0.5f * (r.c00[g] * dx * dx + r.c11[g] * dy * dy) - r.c01[g] * dx * dy;
-    return expf(power < 0.0f ? power : 0.0f);
+// One drawn splat, held in registers for its footprint loop.
+struct SplatR {
+    float u, v, z, c00, c01, c11;
+    int u0, v0, rad, side;
+    FastDiv fside;
+};
+
+__device__ __forceinline__ SplatR load_splat(const RenderWS &r, int g) {
+    SplatR q;
+    q.u = r.u[g]; q.v = r.v[g]; q.z = r.z[g];
+    q.c00 = r.c00[g]; q.c01 = r.c01[g]; q.c11 = r.c11[g];
+    q.u0 = r.u0[g]; q.v0 = r.v0[g]; q.rad = r.rad[g];
+    q.side = 2 * q.rad + 1;
+    q.fside = make_fastdiv(q.side);
+    return q;
+}
+
+// Footprint pixel k of the splat: its screen coordinates and alpha
+// exp(min(power, 0)), or false when the pixel is off screen or its alpha is
+// not above 1/255.  A power below -6 gives exp(power) < 0.0025 < 1/255, so
+// those pixels are dropped before the exponential with the same outcome.
+__device__ __forceinline__ bool splat_pixel(const SplatR &q, int k, int W, int H, int &px, int &py, float &ga) {
+    const int ky = fdiv(k, q.fside), kx = k - ky * q.side;
+    px = q.u0 + kx - q.rad;
+    py = q.v0 + ky - q.rad;
+    if (px < 0 || px >= W || py < 0 || py >= H) return false;
+    const float dx = (float)px + 0.5f - q.u, dy = (float)py + 0.5f - q.v;
+    const float power = -0.5f * (q.c00 * dx * dx + q.c11 * dy * dy) - q.c01 * dx * dy;
+    if (power < -6.0f) return false;
+    ga = expf(power < 0.0f ? power : 0.0f);
+    return ga > (1.0f / 255.0f);
 }
 
 // pass 1: nearest depth per pixel (z > 0: int ordering of the bits)
 __global__ void __launch_bounds__(256) k_splat_zmin(const pm_camera cam, RenderWS r) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (warp >= (int)*r.count) return;
-    const int g = r.list[warp];
-    const int rad = r.rad[g], side = 2 * rad + 1, u0 = r.u0[g], v0 = r.v0[g];
-    const int zb = __float_as_int(r.z[g]);
-    for (int k = lane; k < side * side; k += 32) {
-        const int ky = k / side, kx = k - ky * side;
-        const int px = u0 + kx - rad, py = v0 + ky - rad;
-        if (px < 0 || px >= cam.width || py < 0 || py >= cam.height) continue;
-        if (splat_alpha(r, g, px, py) > (1.0f / 255.0f))
-            atomicMin(reinterpret_cast<int *>(&r.zmin[(long long)py * cam.width + px]), zb);
+    const SplatR q = load_splat(r, r.list[warp]);
+    const int zb = __float_as_int(q.z), W = cam.width, H = cam.height, nk = q.side * q.side;
+    int *zmin = reinterpret_cast<int *>(r.zmin);
+    for (int k = lane; k < nk; k += 32) {
+        int px, py;
+        float ga;
+        if (!splat_pixel(q, k, W, H, px, py, ga)) continue;
+        int *zp = zmin + (long long)py * W + px;
+        if (zb < __ldcg(zp)) atomicMin(zp, zb);   // the stored depth only decreases: skip the atomic when nearer
     }
 }
 
@@ -152,21 +177,17 @@ __global__ void __launch_bounds__(256) k_splat_blend(const pm_camera cam, Render
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (warp >= (int)*r.count) return;
     const int g = r.list[warp];
-    const int rad = r.rad[g], side = 2 * rad + 1, u0 = r.u0[g], v0 = r.v0[g];
-    const float z = r.z[g], inv_tau = r.tau[1];
+    const SplatR q = load_splat(r, g);
+    const float inv_tau = r.tau[1];
     const float c0 = color[3 * g], c1 = color[3 * g + 1], c2 = color[3 * g + 2];
-    for (int k = lane; k < side * side; k += 32) {
-        const int ky = k / side, kx = k - ky * side;
-        const int px = u0 + kx - rad, py = v0 + ky - rad;
-        if (px < 0 || px >= cam.width || py < 0 || py >= cam.height) continue;
-        const float ga = splat_alpha(r, g, px, py);
-        if (!(ga > (1.0f / 255.0f))) continue;
-        const long long pix = (long long)py * cam.width + px;
-        const float w = ga * expf(-(z - r.zmin[pix]) * inv_tau);
-        atomicAdd(&r.csum[3 * pix], c0 * w);
-        atomicAdd(&r.csum[3 * pix + 1], c1 * w);
-        atomicAdd(&r.csum[3 * pix + 2], c2 * w);
-        atomicAdd(&r.wsum[pix], w);
+    const int W = cam.width, H = cam.height, nk = q.side * q.side;
+    for (int k = lane; k < nk; k += 32) {
+        int px, py;
+        float ga;
+        if (!splat_pixel(q, k, W, H, px, py, ga)) continue;
+        const long long pix = (long long)py * W + px;
+        const float w = ga * expf(-(q.z - __ldcg(&r.zmin[pix])) * inv_tau);
+        atomicAdd(&r.csum[pix], make_float4(c0 * w, c1 * w, c2 * w, w));
         const float om = 1.0f - ga;
         atomicAdd(&r.logrev[pix], logf(om > 1e-6f ? om : 1e-6f));
     }
@@ -177,10 +198,11 @@ __global__ void __launch_bounds__(256) k_splat_compose(const pm_render_params rp
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npix) return;
     const float cover = 1.0f - expf(r.logrev[i]);
-    const float ws = r.wsum[i];
+    const float4 cs = r.csum[i];
+    const float ws = cs.w, csum[3] = {cs.x, cs.y, cs.z};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float rgb = ws > 1e-8f ? r.csum[3 * i + c] / (ws > 1e-8f ? ws : 1e-8f) : rp.bg[c];
+        const float rgb = ws > 1e-8f ? csum[c] / (ws > 1e-8f ? ws : 1e-8f) : rp.bg[c];
         float o = rgb * cover + rp.bg[c] * (1.0f - cover);
         o = o < 0.0f ? 0.0f : (o > 1.0f ? 1.0f : o);
         img[3 * i + c] = o;
@@ -189,7 +211,7 @@ __global__ void __launch_bounds__(256) k_splat_compose(const pm_render_params rp
 
 struct RenderLayout {
     Layout sort;
-    size_t u, v, z, c00, c01, c11, u0, v0, rad, list, count, tau, zmin, csum, wsum, logrev, total;
+    size_t u, v, z, c00, c01, c11, u0, v0, rad, list, count, tau, zmin, csum, logrev, total;
 };
 
 RenderLayout make_render_layout(long long n, long long npix) {
@@ -210,8 +232,7 @@ RenderLayout make_render_layout(long long n, long long npix) {
     R.count = o;  o = align_up(o + 16, A);
     R.tau = o;    o = align_up(o + 16, A);
     R.zmin = o;   o = align_up(o + 4 * np, A);
-    R.csum = o;   o = align_up(o + 12 * np, A);
-    R.wsum = o;   o = align_up(o + 4 * np, A);
+    R.csum = o;   o = align_up(o + 16 * np, A);
     R.logrev = o; o = align_up(o + 4 * np, A);
     R.total = o;
     return R;
@@ -278,8 +299,8 @@ void launch_render(const pm_camera &cam, const pm_render_params &rp, const float
     r.list = (int *)(b + L.list);
     r.count = (unsigned *)(b + L.count);
     r.tau = (float *)(b + L.tau);
-    r.zmin = (float *)(b + L.zmin); r.csum = (float *)(b + L.csum);
-    r.wsum = (float *)(b + L.wsum); r.logrev = (float *)(b + L.logrev);
+    r.zmin = (float *)(b + L.zmin); r.csum = (float4 *)(b + L.csum);
+    r.logrev = (float *)(b + L.logrev);
     r.sort = make_ws(ws, L.sort);
     const unsigned pb = (unsigned)((npix + 255) / 256);
     k_splat_clear<<<pb > 0 ? pb : 1, 256, 0, s>>>(r, npix, r.count);
