@@ -18,12 +18,14 @@ Beside it, in the same JSON line:
                  against the same 64 scenes advanced one after another by
                  AnisoMPM.run_frame (graph-captured too); aggregate
                  particle-steps/s of both and their ratio.
-  fwd_adjoint -- differentiable.rollout on the 1M slab, 100 substeps with
-                 checkpoints every 10: forward time, forward+backward time and
-                 their ratio; gradients with respect to E, fibers, sigma_c and
-                 v0 of the mean squared distance to the final positions of a
-                 run with E*1.2, fibers rotated 15 degrees about z and
-                 sigma_c*0.8, with a central-difference check along random
+  fwd_adjoint -- differentiable.rollout on the 1M slab, 100 substeps as one
+                 recorded segment sized to device memory (checkpoint_every
+                 "auto": no recompute in the backward), and with checkpoints
+                 every 10 (segments re-run in the backward): forward time,
+                 forward+backward time and their ratio to the plain forward;
+                 gradients with respect to E, fibers, sigma_c and v0 of a
+                 fixed random linear functional of the final positions, with
+                 an optional central-difference check along random
                  directions.
   render      -- the 1M slab's particles carrying one gaussian each
                  (positions x + F off0, covariances F cov0 F^T, damage tint)
@@ -331,49 +333,66 @@ def _batch_passes(scs):
 
 
 def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
-    """Forward and forward+backward of differentiable.rollout on the 1M slab."""
-    import math
+    """Forward and forward+backward of differentiable.rollout on the 1M slab,
+    with checkpoints every ``every`` substeps (the backward re-runs the
+    segments) and with one segment sized to device memory (every substep
+    recorded during the forward: nothing re-run)."""
     from peel_mpm_b200 import differentiable as dfx
     sim, sc = build_sim(torch, device, seed=0)
     dev = sim.device
     f32 = torch.float32
     S0 = sim._S.clone()
     step0 = sim._step
-    t = math.radians(15.0)
-    rz = torch.tensor([[math.cos(t), -math.sin(t), 0.0], [math.sin(t), math.cos(t), 0.0], [0.0, 0.0, 1.0]],
-                      device=dev)
     E0 = torch.tensor(sc.E, dtype=f32, device=dev)
     fib0 = torch.tensor(sc.fibers, dtype=f32, device=dev)
     sig0 = torch.tensor(sc.sigma_c, dtype=f32, device=dev)
     v00 = torch.zeros(sc.n, 3, dtype=f32, device=dev)
 
-    def forward(E, fib, sig, v0):
+    def forward(E, fib, sig, v0, k=every):
         sim._S.copy_(S0)
         sim._step = step0
         mu, lam, A0 = dfx.material(E, sc.nu, fib, sc.alpha)
-        return dfx.rollout(sim, n_steps, mu=mu, lam=lam, sigma_c=sig, A0=A0, v0=v0, checkpoint_every=every)
+        return dfx.rollout(sim, n_steps, mu=mu, lam=lam, sigma_c=sig, A0=A0, v0=v0, checkpoint_every=k)
 
-    with torch.no_grad():
-        target = forward(E0 * 1.2, fib0 @ rz.t(), sig0 * 0.8, v00).clone()
+    # loss: a fixed random linear functional of the final positions, so the
+    # gradient's seed does not depend on float32 noise of the forward
+    wgen = torch.Generator(device=dev).manual_seed(1)
+    Wt = torch.randn((sc.n, 3), device=dev, generator=wgen)
+
+    def loss_of(xT):
+        return (xT * Wt).sum() / sc.n
+
     s = torch.cuda.current_stream()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    res = None
-    for rep in range(3):                      # the first two warm up (graph capture, allocations)
-        E = E0.clone().requires_grad_(True)
-        fib = fib0.clone().requires_grad_(True)
-        sig = sig0.clone().requires_grad_(True)
-        v0 = v00.clone().requires_grad_(True)
-        torch.cuda.synchronize()
-        ev[0].record(s)
-        xT = forward(E, fib, sig, v0)
-        loss = ((xT - target) ** 2).sum(1).mean()
-        ev[1].record(s)
-        loss.backward()
-        ev[2].record(s)
-        torch.cuda.synchronize()
-        res = (ev[0].elapsed_time(ev[1]), ev[0].elapsed_time(ev[2]), E.grad, fib.grad, sig.grad, v0.grad,
-               float(loss.detach()))
-    fwd_ms, tot_ms, gE, gF, gS, gV, L0 = res
+
+    def timed(k):
+        res = prev = None
+        for rep in range(3):                      # the first two warm up (graph capture, allocations)
+            E = E0.clone().requires_grad_(True)
+            fib = fib0.clone().requires_grad_(True)
+            sig = sig0.clone().requires_grad_(True)
+            v0 = v00.clone().requires_grad_(True)
+            torch.cuda.synchronize()
+            ev[0].record(s)
+            xT = forward(E, fib, sig, v0, k)
+            loss = loss_of(xT)
+            ev[1].record(s)
+            loss.backward()
+            ev[2].record(s)
+            torch.cuda.synchronize()
+            prev = None if res is None else res[2:6]
+            res = (ev[0].elapsed_time(ev[1]), ev[0].elapsed_time(ev[2]), E.grad, fib.grad, sig.grad, v0.grad,
+                   float(loss.detach()))
+        return res, prev
+
+    def rel(ga, gb):   # largest relative difference over the four gradients
+        return max(float((a - b).norm() / max(float(b.norm()), 1e-30)) for a, b in zip(ga, gb))
+
+    (fwd_k, tot_k, *g_k, _), _ = timed(every)
+    k_auto = dfx.auto_segment(sim, n_steps)
+    (fwd_ms, tot_ms, gE, gF, gS, gV, L0), g_prev = timed(k_auto)
+    gdiff = rel((gE, gF, gS, gV), g_k)
+    gspread = rel((gE, gF, gS, gV), g_prev)   # the same computation run twice (float atomics reorder sums)
     # the plain forward of the same 100 substeps (no checkpoints, no tape), for the ratio
     plain = []
     for rep in range(3):
@@ -396,10 +415,8 @@ def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
             dF = torch.randn(fib0.shape, device=dev, generator=gen)
             dS = sig0 * torch.randn(sig0.shape, device=dev, generator=gen)
             dV = torch.randn(v00.shape, device=dev, generator=gen)
-            lp = float(((forward(E0 + eps * dE, fib0 + eps * dF, sig0 + eps * dS, v00 + eps * dV) - target) ** 2)
-                       .sum(1).mean())
-            lm = float(((forward(E0 - eps * dE, fib0 - eps * dF, sig0 - eps * dS, v00 - eps * dV) - target) ** 2)
-                       .sum(1).mean())
+            lp = float(loss_of(forward(E0 + eps * dE, fib0 + eps * dF, sig0 + eps * dS, v00 + eps * dV)))
+            lm = float(loss_of(forward(E0 - eps * dE, fib0 - eps * dF, sig0 - eps * dS, v00 - eps * dV)))
             fd = (lp - lm) / (2 * eps)
             an = float((gE * dE).sum() + (gF * dF).sum() + (gS * dS).sum() + (gV * dV).sum())
             errs.append(abs(an - fd) / max(abs(fd), 1e-30))
@@ -412,7 +429,13 @@ def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
     return {"plain_forward_ms": plain_ms, "forward_ms": fwd_ms, "forward_backward_ms": tot_ms,
             "ratio": tot_ms / plain_ms, "ratio_vs_rollout_forward": tot_ms / fwd_ms,
             "value": sc.n * n_steps / (tot_ms * 1e-3), "unit": UNIT + " (forward+backward)",
-            "substeps": n_steps, "checkpoint_every": every, "particles": sc.n, "loss": L0,
+            "substeps": n_steps, "checkpoint_every": k_auto,
+            "segment_gb": dfx.segment_bytes(sim, k_auto) / 1e9,
+            "checkpointed": {"checkpoint_every": every, "forward_ms": fwd_k, "forward_backward_ms": tot_k,
+                             "ratio": tot_k / plain_ms, "segment_gb": dfx.segment_bytes(sim, every) / 1e9,
+                             "grad_rel_diff_vs_one_segment": gdiff,
+                             "grad_rel_diff_run_to_run": gspread},
+            "particles": sc.n, "loss": L0,
             "grad_norms": {"E": float(gE.norm()), "fibers": float(gF.norm()), "sigma_c": float(gS.norm()),
                            "v0": float(gV.norm())},
             "fd_check": fd}

@@ -176,15 +176,47 @@ class _Rollout(torch.autograd.Function):
         return g_mu, g_lam, g_sc, g_A0, g_v0, None, None, None, None
 
 
+def segment_bytes(sim: AnisoMPM, k: int) -> int:
+    """Device bytes of a k-substep recording segment: the tape (grid and
+    particle records of every substep) and the k + 1 particle states."""
+    return _lib.tape_size(sim.n, sim.n_grid, k) + (k + 1) * _MUTABLE * sim._S.stride(0) * 4
+
+
+def auto_segment(sim: AnisoMPM, n_steps: int, memory_fraction: float = 0.5) -> int:
+    """The longest segment (at most ``n_steps``) whose recording fits in
+    ``memory_fraction`` of the device's free memory.  A segment as long as
+    the rollout records every substep during the forward, so the backward
+    recomputes nothing (1M particles on 128^3: ~0.23 GB per substep)."""
+    free, _ = torch.cuda.mem_get_info(sim.device)
+    budget = int(free * memory_fraction)
+    lo, hi = 1, max(1, int(n_steps))
+    if segment_bytes(sim, hi) <= budget:
+        return hi
+    while lo < hi:   # largest k with segment_bytes(k) <= budget (1 if none)
+        mid = (lo + hi + 1) // 2
+        if segment_bytes(sim, mid) <= budget:
+            lo = mid
+        else:
+            hi = mid - 1
+    return lo
+
+
 def rollout(sim: AnisoMPM, n_steps: int, mu=None, lam=None, sigma_c=None, A0=None, v0=None,
-            time0: float = 0.0, checkpoint_every: int = 10):
+            time0: float = 0.0, checkpoint_every=10):
     """Final positions after ``n_steps`` substeps, differentiable with respect
     to the given per-particle mu, lam, sigma_c, A0 and initial velocity v0
-    (any left as None is taken from ``sim`` as a constant)."""
+    (any left as None is taken from ``sim`` as a constant).
+
+    ``checkpoint_every`` = k: the forward keeps the state every k substeps and
+    records the last segment; the backward re-runs every other segment from
+    its checkpoint.  ``"auto"`` takes the longest segment that fits in half
+    the free device memory (``auto_segment``)."""
     if n_steps < 1:
         raise ValueError("n_steps must be >= 1")
-    if checkpoint_every < 1:
-        raise ValueError("checkpoint_every must be >= 1")
+    if checkpoint_every == "auto":
+        checkpoint_every = auto_segment(sim, n_steps)
+    if not isinstance(checkpoint_every, int) or checkpoint_every < 1:
+        raise ValueError("checkpoint_every must be an int >= 1 or 'auto'")
     mu = sim.mu.detach().clone() if mu is None else mu
     lam = sim.lam.detach().clone() if lam is None else lam
     sigma_c = sim.sigma_c.detach().clone() if sigma_c is None else sigma_c

@@ -92,16 +92,22 @@ def test_adjoint_through_fracture_tracks_reference_autograd():
 
 
 def test_checkpoint_interval_does_not_change_gradients():
-    """Checkpoints every 1, 7 and 20 substeps (one segment) give the same
+    """Checkpoints every 1, 7 and 20 substeps (one segment) and the
+    memory-sized segment ("auto": the whole rollout here) give the same
     gradients up to float32 atomic-order noise (the bar of 20 substeps)."""
     g, meta = golden("plain_small")
     xbar = 2.0 * (g["xT"] - g["target"]) / meta["n"]
     _, a = gpu_grads("plain_small", xbar, every=1)
     _, b = gpu_grads("plain_small", xbar, every=7)
     _, c = gpu_grads("plain_small", xbar, every=20)
+    _, d = gpu_grads("plain_small", xbar, every="auto")
     for k in a:
         assert np.linalg.norm(a[k]) > 0, k
-        assert rel_l2(a[k], b[k]) < 1e-4 and rel_l2(a[k], c[k]) < 1e-4, k
+        assert rel_l2(a[k], b[k]) < 1e-4 and rel_l2(a[k], c[k]) < 1e-4 and rel_l2(a[k], d[k]) < 1e-4, k
+    sim = make_gpu_sim(CASES["plain_small"]())
+    assert dfx.auto_segment(sim, 20) == 20
+    assert dfx.auto_segment(sim, 20, memory_fraction=1e-12) == 1
+    assert dfx.segment_bytes(sim, 20) > dfx.segment_bytes(sim, 7) > 0
 
 
 def rot_z(deg):
