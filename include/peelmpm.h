@@ -320,7 +320,11 @@ typedef struct pm_render_params {
     float max_raw_radius;            /* splats whose unclamped radius reaches this are dropped */
 } pm_render_params;
 
-int pm_render_workspace_size(int64_t n, int32_t width, int32_t height, size_t *bytes);
+/* Workspace of pm_render_gaussians for n gaussians, a width x height image and
+ * footprint radii up to r_max (1..1024): per gaussian the projected splat and
+ * the depth key, per 8x8 screen tile the list of splats whose footprint square
+ * touches it (capacity n x (2 r_max / 8 + 2)^2 ids, at most the tile count). */
+int pm_render_workspace_size(int64_t n, int32_t width, int32_t height, int32_t r_max, size_t *bytes);
 /* xyz (n,3), cov3d (n,3,3) row-major, color (n,3): device float arrays.  The
  * reference's per-splat opacity does not enter its compositing, so it is not
  * an argument. */

@@ -335,11 +335,12 @@ int pm_observe(const pm_particles *P, const int8_t *group, int32_t n_groups, flo
 }
 
 // ------------------------------------------------------------------ renderer
-int pm_render_workspace_size(int64_t n, int32_t width, int32_t height, size_t *bytes) {
+int pm_render_workspace_size(int64_t n, int32_t width, int32_t height, int32_t r_max, size_t *bytes) {
     if (!bytes) return fail(PM_ERR_ARG, "bytes is NULL");
     if (n < 0 || n >= (1LL << 31) || width < 1 || height < 1 || (int64_t)width * height > (1LL << 30))
         return fail(PM_ERR_ARG, "bad n, width or height");
-    *bytes = pm::render_workspace_bytes(n, (long long)width * height);
+    if (r_max < 1 || r_max > 1024) return fail(PM_ERR_ARG, "r_max must be in [1, 1024]");
+    *bytes = pm::render_workspace_bytes(n, width, height, r_max);
     return PM_OK;
 }
 
@@ -349,9 +350,8 @@ int pm_render_gaussians(const pm_camera *cam, const pm_render_params *rp, const 
     if ((rc = check_device())) return rc;
     if (!cam || !rp || !image) return fail(PM_ERR_ARG, "camera, parameters or image is NULL");
     if (n > 0 && (!xyz || !cov3d || !color)) return fail(PM_ERR_ARG, "NULL gaussian array");
-    if (rp->r_max < 1) return fail(PM_ERR_ARG, "r_max must be >= 1");
     size_t need = 0;
-    if ((rc = pm_render_workspace_size(n, cam->width, cam->height, &need))) return rc;
+    if ((rc = pm_render_workspace_size(n, cam->width, cam->height, rp->r_max, &need))) return rc;
     if (!ws || ((uintptr_t)ws & 255) != 0 || ws_bytes < need)
         return fail(PM_ERR_WORKSPACE, "render workspace missing, misaligned or too small");
     pm::launch_render(*cam, *rp, xyz, cov3d, color, n, image, ws, (cudaStream_t)stream);

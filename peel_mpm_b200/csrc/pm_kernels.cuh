@@ -46,7 +46,7 @@ int launch_observe(const Parts &P, const int8_t *group, int n_groups, float thr,
                    float *snap_x, long long snap_stride, cudaStream_t s);
 
 // Gaussian-splat renderer (pm_render.cu).
-size_t render_workspace_bytes(long long n, long long npix);
+size_t render_workspace_bytes(long long n, int width, int height, int r_max);
 void launch_render(const pm_camera &cam, const pm_render_params &rp, const float *xyz, const float *cov,
                    const float *color, long long n, float *img, void *ws, cudaStream_t s);
 void launch_carry(const Parts &P, const int *bind, const float *off0, const float *cov0, const float *color0,

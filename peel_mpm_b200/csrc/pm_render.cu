@@ -4,46 +4,69 @@
 // splats weighted by exp(-(z - z_min) / tau) -- and coverage compositing over
 // a background.  The image is a headless device buffer (H, W, 3).
 //
-// Kernels: k_splat_project (one thread per gaussian: camera transform,
-// Jacobian, 2D covariance + 0.3 dilation, conic, radius, culling; depth key
-// for the median), the radix sort of the depth keys when tau is derived from
-// the median depth, k_splat_zmin and k_splat_blend (one warp per gaussian,
-// lanes over its footprint pixels, float atomics into the pixel buffers) and
-// k_splat_compose (one thread per pixel).
+// Screen tiles of 8x8 pixels.  k_splat_project (one thread per gaussian:
+// camera transform, Jacobian, 2D covariance + 0.3 dilation, conic, radius,
+// culling) packs each drawn splat into 48 bytes and counts it into every tile
+// its (2r+1)^2 footprint square touches; a scan of the tile counts and
+// k_splat_emit build per-tile splat lists; k_splat_tiles runs one warp per
+// tile, two pixels per lane: the soft z-buffer walks the tile's list once from
+// shared memory with the pixels' state in registers and each pixel is
+// composed at the end -- no per-pixel atomics, no clear of pixel buffers.
+// tau from the median depth uses the library's radix sort of the depth keys.
 #include "pm_kernels.cuh"
 
 namespace pm {
 namespace {
 
-struct Splat {
-    float u, v, z, c00, c01, c11;
-    int u0, v0, rad;
-};
+constexpr int kTile = 8;                  // screen tile edge, pixels
 
 struct RenderWS {
-    float *u, *v, *z, *c00, *c01, *c11;
-    int *u0, *v0, *rad;
-    int *list;        // compacted drawn splats
-    unsigned *count;  // [0] drawn splats
-    float *tau;       // [0] tau, [1] 1 / tau
-    float *zmin, *logrev;
-    float4 *csum;     // per pixel: colour sums (x, y, z) and weight sum (w)
-    WS sort;          // key / value buffers of the median sort
+    float4 *sp;        // [3n] per splat: {u, v, c00, c01}, {c11, z, u0, v0 (int bits)}, {r, g, b, rad (int bits)}
+    unsigned *count;   // [0] drawn splats, [1] list overflow (never set when the capacity bound holds)
+    float *tau;        // [0] tau, [1] 1 / max(tau, 1e-6)
+    unsigned *tcnt;    // [ntiles] splats per tile
+    unsigned *tfill;   // [ntiles] emit cursors
+    unsigned *tstart;  // [ntiles + 1] exclusive prefix of tcnt
+    int *tlist;        // [cap] splat ids grouped by tile
+    long long cap;
+    int ntx, nty;
+    WS sort;           // key / value buffers of the median sort
 };
 
-__global__ void __launch_bounds__(256) k_splat_clear(RenderWS r, long long npix, unsigned *count) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *count = 0;
-    if (i < npix) {
-        r.zmin[i] = __int_as_float(0x7f800000);   // +inf
-        r.csum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        r.logrev[i] = 0.0f;
+__device__ __forceinline__ void splat_tiles(int u0, int v0, int rad, int W, int H, int &tx0, int &ty0, int &nx,
+                                            int &ny) {
+    const int x0 = max(u0 - rad, 0), x1 = min(u0 + rad, W - 1);
+    const int y0 = max(v0 - rad, 0), y1 = min(v0 + rad, H - 1);
+    tx0 = x0 / kTile;
+    ty0 = y0 / kTile;
+    nx = x1 / kTile - tx0 + 1;
+    ny = y1 / kTile - ty0 + 1;
+}
+
+__global__ void __launch_bounds__(256) k_splat_clear(RenderWS r, int ntiles) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 4) r.count[i] = 0;
+    if (i < ntiles) {
+        r.tcnt[i] = 0;
+        r.tfill[i] = 0;
     }
+}
+
+// Each lane walks the tiles of its own splat; lanes of a warp that hit the
+// same tile in the same step (neighbouring gaussians) add to it with one atomic.
+__device__ __forceinline__ unsigned tile_reserve(unsigned act, unsigned *ctr, int t, bool on) {
+    const unsigned peers = __match_any_sync(act, on ? t : -1);
+    const int leader = __ffs(peers) - 1;
+    const unsigned lane = threadIdx.x & 31;
+    unsigned base = 0;
+    if (on && (int)lane == leader) base = atomicAdd(&ctr[t], (unsigned)__popc(peers));
+    base = __shfl_sync(act, base, leader);
+    return base + (unsigned)__popc(peers & lanemask_lt());
 }
 
 __global__ void __launch_bounds__(256) k_splat_project(const pm_camera cam, const pm_render_params rp,
                                                        const float *__restrict__ xyz, const float *__restrict__ cov,
-                                                       long long n, RenderWS r) {
+                                                       const float *__restrict__ color, long long n, RenderWS r) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float X[3] = {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
@@ -102,13 +125,29 @@ __global__ void __launch_bounds__(256) k_splat_project(const pm_camera cam, cons
             c11 = a * inv_det;
         }
     }
-    r.u[i] = u; r.v[i] = v; r.z[i] = z;
-    r.c00[i] = c00; r.c01[i] = c01; r.c11[i] = c11;
-    r.u0[i] = u0; r.v0[i] = v0; r.rad[i] = ok ? rad : 0;
+    const int rd = ok ? rad : 0;
+    r.sp[3 * i] = make_float4(u, v, c00, c01);
+    r.sp[3 * i + 1] = make_float4(c11, z, __int_as_float(u0), __int_as_float(v0));
+    if (ok)
+        r.sp[3 * i + 2] = make_float4(color[3 * i], color[3 * i + 1], color[3 * i + 2], __int_as_float(rd));
+    else
+        r.sp[3 * i + 2] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
     // depth key for the median of the drawn splats (z > near > 0: the float bits order like the values)
     r.sort.keys_a[i] = ok ? __float_as_uint(z) : 0xffffffffu;
     r.sort.vals_a[i] = (int)i;
-    if (ok) r.list[atomicAdd(r.count, 1u)] = (int)i;
+    const unsigned act = __activemask(), drawn = __ballot_sync(act, ok);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(act) - 1) && drawn) atomicAdd(r.count, (unsigned)__popc(drawn));
+    // tile counts of the footprint square
+    int tx0 = 0, ty0 = 0, nx = 0, ny = 0;
+    if (ok) splat_tiles(u0, v0, rd, cam.width, cam.height, tx0, ty0, nx, ny);
+    const int nt = nx * ny;
+    const int steps = __reduce_max_sync(act, nt);
+    for (int k = 0; k < steps; ++k) {
+        const bool on = k < nt;
+        const int ky = on ? k / nx : 0;
+        const int t = on ? (ty0 + ky) * r.ntx + tx0 + (k - ky * nx) : 0;
+        tile_reserve(act, r.tcnt, t, on);
+    }
 }
 
 // tau = 0.02 * median depth (torch.median: the lower middle element), or the given tau
@@ -116,127 +155,195 @@ __global__ void k_splat_tau(RenderWS r, float tau_given, const unsigned *sorted)
     if (threadIdx.x != 0) return;
     float tau = tau_given;
     if (!(tau_given > 0.0f)) {
-        const unsigned c = *r.count;
+        const unsigned c = r.count[0];
         tau = c > 0 ? 0.02f * __uint_as_float(sorted[(c - 1) / 2]) : 1.0f;
     }
     r.tau[0] = tau;
     r.tau[1] = 1.0f / (tau > 1e-6f ? tau : 1e-6f);
 }
 
-// One drawn splat, held in registers for its footprint loop.
-struct SplatR {
-    float u, v, z, c00, c01, c11;
-    int u0, v0, rad, side;
-    FastDiv fside;
+// Exclusive scan of the tile counts (one CTA of 1024 threads).
+__global__ void __launch_bounds__(1024) k_tile_scan(RenderWS r, int ntiles) {
+    __shared__ unsigned wsum[32];
+    __shared__ unsigned carry;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < ntiles; base += 1024) {
+        const int i = base + tid;
+        const unsigned v = i < ntiles ? r.tcnt[i] : 0u;
+        unsigned incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            unsigned w = wsum[lane], wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += y;
+            }
+            wsum[lane] = wi - w;   // exclusive over warps
+        }
+        __syncthreads();
+        const unsigned c = carry;
+        if (i < ntiles) r.tstart[i] = c + wsum[wid] + incl - v;
+        __syncthreads();
+        if (tid == 1023) carry = c + wsum[wid] + incl;
+        __syncthreads();
+    }
+    if (tid == 0) r.tstart[ntiles] = carry;
+}
+
+// Per-tile lists: every drawn splat id into each tile of its footprint square.
+__global__ void __launch_bounds__(256) k_splat_emit(const pm_camera cam, long long n, RenderWS r) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p1 = r.sp[3 * i + 1], p2 = r.sp[3 * i + 2];
+    const int rd = __float_as_int(p2.w);
+    int tx0 = 0, ty0 = 0, nx = 0, ny = 0;
+    if (rd > 0) splat_tiles(__float_as_int(p1.z), __float_as_int(p1.w), rd, cam.width, cam.height, tx0, ty0, nx, ny);
+    const int nt = nx * ny;
+    const unsigned act = __activemask();
+    const int steps = __reduce_max_sync(act, nt);
+    for (int k = 0; k < steps; ++k) {
+        const bool on = k < nt;
+        const int ky = on ? k / nx : 0;
+        const int t = on ? (ty0 + ky) * r.ntx + tx0 + (k - ky * nx) : 0;
+        const unsigned slot = tile_reserve(act, r.tfill, t, on);
+        if (on) {
+            const long long at = (long long)r.tstart[t] + slot;
+            if (slot < r.tcnt[t] && at < r.cap)
+                r.tlist[at] = (int)i;
+            else
+                r.count[1] = 1;
+        }
+    }
+}
+
+// One warp per 8x8 tile (4 tiles per CTA), two pixels per lane (rows y and
+// y + 4).  The warp walks its tile's list in batches of 32 splats staged in
+// shared memory.  A splat counts at a pixel when the pixel lies in its
+// footprint square and alpha = exp(min(power, 0)) exceeds 1/255 (a power below
+// -6 gives exp(power) < 0.0025 < 1/255: dropped before the exponential with
+// the same outcome).  The reference's two passes -- nearest depth z_min, then
+// sums of c w and w with w = alpha exp(-(z - z_min) / tau) -- are done in one:
+// the sums are kept relative to the nearest depth seen so far and rescaled by
+// exp(-(z_old - z_new) / tau) when a nearer splat arrives, which is the same
+// sum up to rounding.  Sum log(max(1 - alpha, 1e-6)) gives the coverage.
+constexpr int kTileWarps = 4;
+
+struct PixAcc {
+    float zmin, c0, c1, c2, w, lr;
 };
 
-__device__ __forceinline__ SplatR load_splat(const RenderWS &r, int g) {
-    SplatR q;
-    q.u = r.u[g]; q.v = r.v[g]; q.z = r.z[g];
-    q.c00 = r.c00[g]; q.c01 = r.c01[g]; q.c11 = r.c11[g];
-    q.u0 = r.u0[g]; q.v0 = r.v0[g]; q.rad = r.rad[g];
-    q.side = 2 * q.rad + 1;
-    q.fside = make_fastdiv(q.side);
-    return q;
-}
-
-// Footprint pixel k of the splat: its screen coordinates and alpha
-// exp(min(power, 0)), or false when the pixel is off screen or its alpha is
-// not above 1/255.  A power below -6 gives exp(power) < 0.0025 < 1/255, so
-// those pixels are dropped before the exponential with the same outcome.
-__device__ __forceinline__ bool splat_pixel(const SplatR &q, int k, int W, int H, int &px, int &py, float &ga) {
-    const int ky = fdiv(k, q.fside), kx = k - ky * q.side;
-    px = q.u0 + kx - q.rad;
-    py = q.v0 + ky - q.rad;
-    if (px < 0 || px >= W || py < 0 || py >= H) return false;
-    const float dx = (float)px + 0.5f - q.u, dy = (float)py + 0.5f - q.v;
-    const float power = -0.5f * (q.c00 * dx * dx + q.c11 * dy * dy) - q.c01 * dx * dy;
-    if (power < -6.0f) return false;
-    ga = expf(power < 0.0f ? power : 0.0f);
-    return ga > (1.0f / 255.0f);
-}
-
-// pass 1: nearest depth per pixel (z > 0: int ordering of the bits)
-__global__ void __launch_bounds__(256) k_splat_zmin(const pm_camera cam, RenderWS r) {
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (warp >= (int)*r.count) return;
-    const SplatR q = load_splat(r, r.list[warp]);
-    const int zb = __float_as_int(q.z), W = cam.width, H = cam.height, nk = q.side * q.side;
-    int *zmin = reinterpret_cast<int *>(r.zmin);
-    for (int k = lane; k < nk; k += 32) {
-        int px, py;
-        float ga;
-        if (!splat_pixel(q, k, W, H, px, py, ga)) continue;
-        int *zp = zmin + (long long)py * W + px;
-        if (zb < __ldcg(zp)) atomicMin(zp, zb);   // the stored depth only decreases: skip the atomic when nearer
+__device__ __forceinline__ void pix_add(PixAcc &p, const float4 &A, const float4 &B, const float4 &Cc, int px, int py,
+                                        float inv_tau) {
+    const int rd = __float_as_int(Cc.w);
+    if (abs(px - __float_as_int(B.z)) > rd || abs(py - __float_as_int(B.w)) > rd) return;
+    const float dx = ((float)px + 0.5f) - A.x, dy = ((float)py + 0.5f) - A.y;
+    const float power = -0.5f * (A.z * dx * dx + B.x * dy * dy) - A.w * dx * dy;
+    if (power < -6.0f) return;
+    const float ga = expf(power < 0.0f ? power : 0.0f);
+    if (!(ga > (1.0f / 255.0f))) return;
+    float w;
+    if (B.y < p.zmin) {
+        const float sc = p.w > 0.0f ? expf(-(p.zmin - B.y) * inv_tau) : 0.0f;
+        p.c0 *= sc; p.c1 *= sc; p.c2 *= sc; p.w *= sc;
+        p.zmin = B.y;
+        w = ga;   // exp(0)
+    } else {
+        w = ga * expf(-(B.y - p.zmin) * inv_tau);
     }
+    p.c0 += Cc.x * w;
+    p.c1 += Cc.y * w;
+    p.c2 += Cc.z * w;
+    p.w += w;
+    const float om = 1.0f - ga;
+    p.lr += logf(om > 1e-6f ? om : 1e-6f);
 }
 
-// pass 2: soft-z-buffer blend
-__global__ void __launch_bounds__(256) k_splat_blend(const pm_camera cam, RenderWS r, const float *__restrict__ color) {
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (warp >= (int)*r.count) return;
-    const int g = r.list[warp];
-    const SplatR q = load_splat(r, g);
-    const float inv_tau = r.tau[1];
-    const float c0 = color[3 * g], c1 = color[3 * g + 1], c2 = color[3 * g + 2];
-    const int W = cam.width, H = cam.height, nk = q.side * q.side;
-    for (int k = lane; k < nk; k += 32) {
-        int px, py;
-        float ga;
-        if (!splat_pixel(q, k, W, H, px, py, ga)) continue;
-        const long long pix = (long long)py * W + px;
-        const float w = ga * expf(-(q.z - __ldcg(&r.zmin[pix])) * inv_tau);
-        atomicAdd(&r.csum[pix], make_float4(c0 * w, c1 * w, c2 * w, w));
-        const float om = 1.0f - ga;
-        atomicAdd(&r.logrev[pix], logf(om > 1e-6f ? om : 1e-6f));
-    }
-}
-
-__global__ void __launch_bounds__(256) k_splat_compose(const pm_render_params rp, RenderWS r, long long npix,
-                                                       float *__restrict__ img) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npix) return;
-    const float cover = 1.0f - expf(r.logrev[i]);
-    const float4 cs = r.csum[i];
-    const float ws = cs.w, csum[3] = {cs.x, cs.y, cs.z};
+__device__ __forceinline__ void pix_store(const PixAcc &p, const pm_camera &cam, const pm_render_params &rp, int px,
+                                          int py, float *img) {
+    if (px >= cam.width || py >= cam.height) return;
+    const float cover = 1.0f - expf(p.lr);
+    const float csum[3] = {p.c0, p.c1, p.c2};
+    float *o = img + 3 * ((long long)py * cam.width + px);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float rgb = ws > 1e-8f ? csum[c] / (ws > 1e-8f ? ws : 1e-8f) : rp.bg[c];
-        float o = rgb * cover + rp.bg[c] * (1.0f - cover);
-        o = o < 0.0f ? 0.0f : (o > 1.0f ? 1.0f : o);
-        img[3 * i + c] = o;
+        const float rgb = p.w > 1e-8f ? csum[c] / (p.w > 1e-8f ? p.w : 1e-8f) : rp.bg[c];
+        const float v = rgb * cover + rp.bg[c] * (1.0f - cover);
+        o[c] = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
     }
+}
+
+__global__ void __launch_bounds__(32 * kTileWarps) k_splat_tiles(const pm_camera cam, const pm_render_params rp,
+                                                                 RenderWS r, float *__restrict__ img, int ntiles) {
+    __shared__ float4 sA[kTileWarps][32], sB[kTileWarps][32], sC[kTileWarps][32];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x * kTileWarps + wid;
+    if (tile >= ntiles) return;   // whole warps only; no block-wide barrier below
+    const int px = (tile % r.ntx) * kTile + (lane & (kTile - 1));
+    const int py0 = (tile / r.ntx) * kTile + (lane >> 3), py1 = py0 + 4;
+    const unsigned beg = r.tstart[tile], end = beg + r.tcnt[tile];
+    const float inv_tau = r.tau[1];
+    const float inf = __int_as_float(0x7f800000);
+    PixAcc a = {inf, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, b = a;
+    for (unsigned base = beg; base < end; base += 32) {
+        const int cnt = (int)min(32u, end - base);
+        __syncwarp();
+        if (lane < cnt) {
+            const long long g = r.tlist[base + lane];
+            sA[wid][lane] = r.sp[3 * g];
+            sB[wid][lane] = r.sp[3 * g + 1];
+            sC[wid][lane] = r.sp[3 * g + 2];
+        }
+        __syncwarp();
+        for (int j = 0; j < cnt; ++j) {
+            const float4 A = sA[wid][j], B = sB[wid][j], Cc = sC[wid][j];
+            pix_add(a, A, B, Cc, px, py0, inv_tau);
+            pix_add(b, A, B, Cc, px, py1, inv_tau);
+        }
+    }
+    pix_store(a, cam, rp, px, py0, img);
+    pix_store(b, cam, rp, px, py1, img);
 }
 
 struct RenderLayout {
     Layout sort;
-    size_t u, v, z, c00, c01, c11, u0, v0, rad, list, count, tau, zmin, csum, logrev, total;
+    size_t sp, count, tau, tcnt, tfill, tstart, tlist, total;
+    long long cap;
+    int ntx, nty;
 };
 
-RenderLayout make_render_layout(long long n, long long npix) {
+// Tiles a footprint square of side 2 r_max + 1 can touch, per axis:
+// floor(2 r_max / kTile) + 2, and never more than the screen has.
+RenderLayout make_render_layout(long long n, int width, int height, int r_max) {
     RenderLayout R;
+    R.ntx = (width + kTile - 1) / kTile;
+    R.nty = (height + kTile - 1) / kTile;
+    const long long ntiles = (long long)R.ntx * R.nty;
+    const long long per_axis = 2LL * (r_max > 1 ? r_max : 1) / kTile + 2;
+    const long long per = std::min(per_axis, (long long)R.ntx) * std::min(per_axis, (long long)R.nty);
+    R.cap = std::max<long long>(1, n * per);
     R.sort = make_layout_sized(n, 0, 0, 32, 1, 0);
-    const size_t A = 256, nn = (size_t)(n > 0 ? n : 1), np = (size_t)npix;
+    const size_t A = 256, nn = (size_t)(n > 0 ? n : 1), nt = (size_t)ntiles;
     size_t o = R.sort.total;
-    R.u = o;      o = align_up(o + 4 * nn, A);
-    R.v = o;      o = align_up(o + 4 * nn, A);
-    R.z = o;      o = align_up(o + 4 * nn, A);
-    R.c00 = o;    o = align_up(o + 4 * nn, A);
-    R.c01 = o;    o = align_up(o + 4 * nn, A);
-    R.c11 = o;    o = align_up(o + 4 * nn, A);
-    R.u0 = o;     o = align_up(o + 4 * nn, A);
-    R.v0 = o;     o = align_up(o + 4 * nn, A);
-    R.rad = o;    o = align_up(o + 4 * nn, A);
-    R.list = o;   o = align_up(o + 4 * nn, A);
+    R.sp = o;     o = align_up(o + 48 * nn, A);
     R.count = o;  o = align_up(o + 16, A);
     R.tau = o;    o = align_up(o + 16, A);
-    R.zmin = o;   o = align_up(o + 4 * np, A);
-    R.csum = o;   o = align_up(o + 16 * np, A);
-    R.logrev = o; o = align_up(o + 4 * np, A);
+    R.tcnt = o;   o = align_up(o + 4 * nt, A);
+    R.tfill = o;  o = align_up(o + 4 * nt, A);
+    R.tstart = o; o = align_up(o + 4 * (nt + 1), A);
+    R.tlist = o;  o = align_up(o + 4 * (size_t)R.cap, A);
     R.total = o;
     return R;
 }
+
 
 // Gaussian carrying (run_orange.py:116-133): gaussian i bound to particle
 // b = bind[i] moves with the particle's affine motion: position
@@ -285,35 +392,36 @@ void launch_carry(const Parts &P, const int *bind, const float *off0, const floa
                                                           color);
 }
 
-size_t render_workspace_bytes(long long n, long long npix) { return make_render_layout(n, npix).total; }
+size_t render_workspace_bytes(long long n, int width, int height, int r_max) {
+    return make_render_layout(n, width, height, r_max).total;
+}
 
 void launch_render(const pm_camera &cam, const pm_render_params &rp, const float *xyz, const float *cov,
                    const float *color, long long n, float *img, void *ws, cudaStream_t s) {
-    const long long npix = (long long)cam.width * cam.height;
-    const RenderLayout L = make_render_layout(n, npix);
+    const RenderLayout L = make_render_layout(n, cam.width, cam.height, rp.r_max);
     char *b = (char *)ws;
     RenderWS r;
-    r.u = (float *)(b + L.u); r.v = (float *)(b + L.v); r.z = (float *)(b + L.z);
-    r.c00 = (float *)(b + L.c00); r.c01 = (float *)(b + L.c01); r.c11 = (float *)(b + L.c11);
-    r.u0 = (int *)(b + L.u0); r.v0 = (int *)(b + L.v0); r.rad = (int *)(b + L.rad);
-    r.list = (int *)(b + L.list);
+    r.sp = (float4 *)(b + L.sp);
     r.count = (unsigned *)(b + L.count);
     r.tau = (float *)(b + L.tau);
-    r.zmin = (float *)(b + L.zmin); r.csum = (float4 *)(b + L.csum);
-    r.logrev = (float *)(b + L.logrev);
+    r.tcnt = (unsigned *)(b + L.tcnt);
+    r.tfill = (unsigned *)(b + L.tfill);
+    r.tstart = (unsigned *)(b + L.tstart);
+    r.tlist = (int *)(b + L.tlist);
+    r.cap = L.cap;
+    r.ntx = L.ntx;
+    r.nty = L.nty;
     r.sort = make_ws(ws, L.sort);
-    const unsigned pb = (unsigned)((npix + 255) / 256);
-    k_splat_clear<<<pb > 0 ? pb : 1, 256, 0, s>>>(r, npix, r.count);
-    if (n > 0) k_splat_project<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(cam, rp, xyz, cov, n, r);
+    const int ntiles = L.ntx * L.nty;
+    k_splat_clear<<<(unsigned)((std::max(ntiles, 4) + 255) / 256), 256, 0, s>>>(r, ntiles);
+    if (n > 0) k_splat_project<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(cam, rp, xyz, cov, color, n, r);
     const bool median = !(rp.tau > 0.0f);
     if (median && n > 0) launch_sort(r.sort, n, s);
     k_splat_tau<<<1, 32, 0, s>>>(r, rp.tau, r.sort.sorted_keys);
-    if (n > 0) {
-        const unsigned wb = (unsigned)((n * 32 + 255) / 256);   // one warp per gaussian (the drawn ones act)
-        k_splat_zmin<<<wb, 256, 0, s>>>(cam, r);
-        k_splat_blend<<<wb, 256, 0, s>>>(cam, r, color);
-    }
-    k_splat_compose<<<pb > 0 ? pb : 1, 256, 0, s>>>(rp, r, npix, img);
+    k_tile_scan<<<1, 1024, 0, s>>>(r, ntiles);
+    if (n > 0) k_splat_emit<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(cam, n, r);
+    k_splat_tiles<<<(unsigned)((ntiles + kTileWarps - 1) / kTileWarps), 32 * kTileWarps, 0, s>>>(cam, rp, r, img,
+                                                                                                   ntiles);
 }
 
 }  // namespace pm

@@ -53,7 +53,8 @@ def render_gaussians(cam: Camera, xyz, cov3d, color, opacity, bg=(1.0, 1.0, 1.0)
     """(H, W, 3) image in [0, 1] of the gaussians (xyz (N,3), cov3d (N,3,3),
     color (N,3)).  ``opacity`` is accepted and, as in the reference, does not
     enter the compositing; ``chunk`` (the reference's memory bound) has no
-    effect here: footprints are never materialised."""
+    effect here: (splat, pixel) pairs are never materialised, only per-tile
+    splat lists."""
     dev = cam.device
     if downsample is not None and downsample < xyz.shape[0]:
         g = torch.Generator(device="cpu").manual_seed(seed)
@@ -72,7 +73,8 @@ def render_gaussians(cam: Camera, xyz, cov3d, color, opacity, bg=(1.0, 1.0, 1.0)
     rp.near = float(near)
     rp.max_raw_radius = float(max_raw_radius)
     need = C.c_size_t(0)
-    _lib.check(lib.pm_render_workspace_size(n, int(cam.W), int(cam.H), C.byref(need)), "pm_render_workspace_size")
+    _lib.check(lib.pm_render_workspace_size(n, int(cam.W), int(cam.H), int(r_max), C.byref(need)),
+               "pm_render_workspace_size")
     ws = torch.empty(need.value, dtype=torch.uint8, device=dev)
     img = torch.empty((cam.H, cam.W, 3), dtype=torch.float32, device=dev)
     camst = cam._struct()
