@@ -234,11 +234,15 @@ __global__ void __launch_bounds__(256) k_splat_emit(const pm_camera cam, long lo
 // sums of c w and w with w = alpha exp(-(z - z_min) / tau) -- are done in one:
 // the sums are kept relative to the nearest depth seen so far and rescaled by
 // exp(-(z_old - z_new) / tau) when a nearer splat arrives, which is the same
-// sum up to rounding.  Sum log(max(1 - alpha, 1e-6)) gives the coverage.
+// sum up to rounding.  The coverage 1 - exp(sum log(max(1 - alpha, 1e-6))) is
+// taken as 1 - prod max(1 - alpha, 1e-6): the same quantity, and a product
+// that underflows gives coverage 1.0f exactly as the sum of logs does.  The
+// exponentials use the __expf intrinsic (a few ulp; the image tolerance is
+// 1e-4 absolute).
 constexpr int kTileWarps = 4;
 
 struct PixAcc {
-    float zmin, c0, c1, c2, w, lr;
+    float zmin, c0, c1, c2, w, rev;   // rev: prod max(1 - alpha, 1e-6)
 };
 
 __device__ __forceinline__ void pix_add(PixAcc &p, const float4 &A, const float4 &B, const float4 &Cc, int px, int py,
@@ -248,29 +252,29 @@ __device__ __forceinline__ void pix_add(PixAcc &p, const float4 &A, const float4
     const float dx = ((float)px + 0.5f) - A.x, dy = ((float)py + 0.5f) - A.y;
     const float power = -0.5f * (A.z * dx * dx + B.x * dy * dy) - A.w * dx * dy;
     if (power < -6.0f) return;
-    const float ga = expf(power < 0.0f ? power : 0.0f);
+    const float ga = __expf(power < 0.0f ? power : 0.0f);
     if (!(ga > (1.0f / 255.0f))) return;
     float w;
     if (B.y < p.zmin) {
-        const float sc = p.w > 0.0f ? expf(-(p.zmin - B.y) * inv_tau) : 0.0f;
+        const float sc = p.w > 0.0f ? __expf(-(p.zmin - B.y) * inv_tau) : 0.0f;
         p.c0 *= sc; p.c1 *= sc; p.c2 *= sc; p.w *= sc;
         p.zmin = B.y;
         w = ga;   // exp(0)
     } else {
-        w = ga * expf(-(B.y - p.zmin) * inv_tau);
+        w = ga * __expf(-(B.y - p.zmin) * inv_tau);
     }
     p.c0 += Cc.x * w;
     p.c1 += Cc.y * w;
     p.c2 += Cc.z * w;
     p.w += w;
     const float om = 1.0f - ga;
-    p.lr += logf(om > 1e-6f ? om : 1e-6f);
+    p.rev *= om > 1e-6f ? om : 1e-6f;
 }
 
 __device__ __forceinline__ void pix_store(const PixAcc &p, const pm_camera &cam, const pm_render_params &rp, int px,
                                           int py, float *img) {
     if (px >= cam.width || py >= cam.height) return;
-    const float cover = 1.0f - expf(p.lr);
+    const float cover = 1.0f - p.rev;
     const float csum[3] = {p.c0, p.c1, p.c2};
     float *o = img + 3 * ((long long)py * cam.width + px);
 #pragma unroll
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_splat_tiles(const pm_camera
     const unsigned beg = r.tstart[tile], end = beg + r.tcnt[tile];
     const float inv_tau = r.tau[1];
     const float inf = __int_as_float(0x7f800000);
-    PixAcc a = {inf, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, b = a;
+    PixAcc a = {inf, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f}, b = a;
     for (unsigned base = beg; base < end; base += 32) {
         const int cnt = (int)min(32u, end - base);
         __syncwarp();
