@@ -254,7 +254,7 @@ int pm_batch_substep(int32_t n_scenes, const int64_t *n, const int32_t *n_grid, 
     pm::launch_set_clock_batch(sc, w, dev_clocks, s);
     if (bp.n_total > 0) {
         pm::launch_keys(sc, w, parts, s);
-        pm::launch_sort(w, bp.n_total, s, w.inv_perm);
+        pm::launch_sort(w, bp.n_total, s, w.inv_perm, true);
         pm::launch_p2g(sc, parts, w, s, recorded_range(ws));
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s);

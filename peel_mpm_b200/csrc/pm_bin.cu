@@ -30,33 +30,76 @@ __global__ void __launch_bounds__(256) k_keys(const float *__restrict__ x, long 
 }
 
 // Substep keys: block-major sort key of the base cell, offset by the scene's
-// first sort block; identity ids; allow.any() per scene (a warp whose lanes
-// share a scene votes once).
+// first sort block; identity ids; allow.any() per scene; and the first radix
+// pass's digit histogram.  One CTA per radix tile (kSortTile particles), so the
+// tile's histogram column is complete when the CTA ends; each thread takes
+// particles t, t + 256, ... of the tile, four at a time with their loads
+// issued together.
 template <class SC>
-__global__ void __launch_bounds__(256) k_keys_t(const SC sc, const float *__restrict__ x, long long n, long long ps,
-                                                unsigned *__restrict__ keys, int *__restrict__ vals,
-                                                const unsigned char *__restrict__ allow, Ctrl *ctrl) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
-        const int sid = sc.of_particle(p);
-        const pm_params &prm = sc.params(sid);
-        const int ng = prm.n_grid;
-        const float inv_dx = (float)prm.inv_dx;
-        int qb[3];
+__global__ void __launch_bounds__(kSortThreads) k_keys_t(const SC sc, const float *__restrict__ x, long long n,
+                                                         long long ps, unsigned *__restrict__ keys,
+                                                         int *__restrict__ vals, const unsigned char *__restrict__ allow,
+                                                         Ctrl *ctrl, unsigned *__restrict__ hist, int n_tiles) {
+    __shared__ unsigned cnt[kRadix];
+    for (int i = threadIdx.x; i < kRadix; i += kSortThreads) cnt[i] = 0;
+    __syncthreads();
+    const long long t0 = (long long)blockIdx.x * kSortTile;
+    const int lane = threadIdx.x & 31;
+    bool any_plain = false;
+    int sid = 0;
+    if (SC::batched) sid = sc.of_particle(min(t0 + threadIdx.x, n - 1));
+    constexpr int G = 4;
+#pragma unroll 1
+    for (int k0 = 0; k0 < kSortItems; k0 += G) {
+        float xp[G][3];
+        unsigned char al[G];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) qb[a] = sat_base(floorf(__fsub_rn(__fmul_rn(x[a * ps + p], inv_dx), 0.5f)), ng);
-        keys[p] = (sc.sblock_base(sid) << kSortBlockBits) + blocked_key(qb, ng);
-        vals[p] = (int)p;
-        const bool a = allow[p] != 0;
-        const unsigned act = __activemask();
-        const int lane = threadIdx.x & 31, first = __ffs(act) - 1;
-        const int s0 = __shfl_sync(act, sid, first);
-        if (__all_sync(act, sid == s0)) {
-            if (__any_sync(act, a) && lane == first) ctrl[s0].any_allow = 1;
-        } else if (a) {
-            ctrl[sid].any_allow = 1;
+        for (int g = 0; g < G; ++g) {
+            const long long p = t0 + (long long)(k0 + g) * kSortThreads + threadIdx.x;
+            const bool ok = p < n;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) xp[g][a] = ok ? x[a * ps + p] : 0.0f;
+            al[g] = ok ? allow[p] : (unsigned char)0;
+        }
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const long long p = t0 + (long long)(k0 + g) * kSortThreads + threadIdx.x;
+            const bool ok = p < n;
+            if (SC::batched && ok) {
+                while (p >= sc.p_end(sid, n)) ++sid;   // particles of a thread come in increasing order
+            }
+            const pm_params &prm = sc.params(sid);
+            const int ng = prm.n_grid;
+            const float inv_dx = (float)prm.inv_dx;
+            int qb[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) qb[a] = sat_base(floorf(__fsub_rn(__fmul_rn(xp[g][a], inv_dx), 0.5f)), ng);
+            const unsigned key = (sc.sblock_base(sid) << kSortBlockBits) + blocked_key(qb, ng);
+            if (ok) {
+                keys[p] = key;
+                vals[p] = (int)p;
+                atomicAdd(&cnt[key & (kRadix - 1)], 1u);
+            }
+            const bool a = ok && al[g] != 0;
+            if (SC::batched) {
+                // a warp whose lanes share a scene votes once
+                const int s0 = __shfl_sync(0xffffffffu, sid, 0);
+                if (__all_sync(0xffffffffu, sid == s0)) {
+                    if (__any_sync(0xffffffffu, a) && lane == 0) ctrl[s0].any_allow = 1;
+                } else if (a) {
+                    ctrl[sid].any_allow = 1;
+                }
+            } else {
+                any_plain |= a;
+            }
         }
     }
+    if (!SC::batched) {
+        if (__syncthreads_or(any_plain) && threadIdx.x == 0) ctrl->any_allow = 1;
+    } else {
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < kRadix; i += kSortThreads) hist[(long long)i * n_tiles + blockIdx.x] = cnt[i];
 }
 
 // Compacts the marked blocks into block_list and clears the marks.
@@ -245,13 +288,14 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *
     }
 }
 
-void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv) {
-    const int tiles = w.n_tiles;
+void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv, bool hist0_ready) {
+    if (n <= 0) return;
+    const int tiles = (int)((n + kSortTile - 1) / kSortTile);
     unsigned *kin = w.keys_a, *kout = w.keys_b;
     int *vin = w.vals_a, *vout = w.vals_b;
     for (int pass = 0; pass < w.passes; ++pass) {
         const int shift = pass * kRadixBits;
-        k_radix_hist<<<tiles, kSortThreads, 0, s>>>(kin, n, shift, w.hist, tiles);
+        if (pass > 0 || !hist0_ready) k_radix_hist<<<tiles, kSortThreads, 0, s>>>(kin, n, shift, w.hist, tiles);
         k_radix_rowscan<<<kRadix, 256, 0, s>>>(w.hist, tiles, w.dtot);
         k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, w.hist, tiles, w.dtot,
                                                        pass == w.passes - 1 ? inv : nullptr);
@@ -262,8 +306,10 @@ void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv) {
 
 template <class SC>
 void launch_keys(const SC &sc, const WS &w, const Parts &P, cudaStream_t s) {
-    const int blocks = (int)std::min<long long>((P.n + 255) / 256, 148LL * 16);
-    k_keys_t<SC><<<blocks > 0 ? blocks : 1, 256, 0, s>>>(sc, P.x, P.n, P.ps, w.keys_a, w.vals_a, P.allow, w.ctrl);
+    if (P.n <= 0) return;
+    const int tiles = (int)((P.n + kSortTile - 1) / kSortTile);
+    k_keys_t<SC><<<tiles, kSortThreads, 0, s>>>(sc, P.x, P.n, P.ps, w.keys_a, w.vals_a, P.allow, w.ctrl, w.hist,
+                                                tiles);
 }
 template void launch_keys<PlainScenes>(const PlainScenes &, const WS &, const Parts &, cudaStream_t);
 template void launch_keys<BatchScenes>(const BatchScenes &, const WS &, const Parts &, cudaStream_t);

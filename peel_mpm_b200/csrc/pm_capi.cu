@@ -163,7 +163,7 @@ int pm_bin(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     const pm::Parts parts = pm::make_parts(P);
     cudaStream_t s = (cudaStream_t)stream;
     pm::launch_keys(pm::PlainScenes{*prm}, w, parts, s);
-    pm::launch_sort(w, P->n, s, w.inv_perm);
+    pm::launch_sort(w, P->n, s, w.inv_perm, true);
     return cuda_check("pm_bin");
 }
 
@@ -210,7 +210,7 @@ static int substep_common(const pm_params *prm, const pm_particles *P, void *ws,
     if (P->n > 0) {
         const pm::PlainScenes sc{*prm};
         pm::launch_keys(sc, w, parts, s);
-        pm::launch_sort(w, P->n, s, w.inv_perm);
+        pm::launch_sort(w, P->n, s, w.inv_perm, true);
         pm::launch_p2g(sc, parts, w, s, prm->p2g_range);
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s);
@@ -282,7 +282,7 @@ int pm_substep_record(const pm_params *prm, const pm_particles *P, void *ws, siz
     if (P->n > 0) {
         const pm::PlainScenes sc{*prm};
         pm::launch_keys(sc, w, parts, s);
-        pm::launch_sort(w, P->n, s, w.inv_perm);
+        pm::launch_sort(w, P->n, s, w.inv_perm, true);
         pm::launch_p2g(sc, parts, w, s, prm->p2g_range);
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s);

@@ -8,7 +8,9 @@
 namespace pm {
 
 template <class SC> void launch_keys(const SC &sc, const WS &w, const Parts &P, cudaStream_t s);
-void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv = nullptr);
+// hist0_ready: the first pass's tile histogram was written by launch_keys
+// (the substep path), so the sort starts at that pass's column scan.
+void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv = nullptr, bool hist0_ready = false);
 void launch_compact(const WS &w, cudaStream_t s);
 void prepare_p2g();
 void launch_keys_only(const float *x, long long n, long long ps, int ng, float inv_dx, bool blocked, const WS &w,
