@@ -332,7 +332,7 @@ int pm_render_gaussians(const pm_camera *cam, const pm_render_params *rp, const 
                         const float *color, int64_t n, float *image, void *ws, size_t ws_bytes, void *stream);
 
 /* Gaussian carrying (run_orange.py:116-133): gaussian i, bound to particle
- * bind[i] (device int32, out-of-range ids are skipped), gets position
+ * bind[i] (device int32; an out-of-range id gives NaN outputs), gets position
  * affine (x) + F off0_i, covariance F cov0_i F^T and colour
  * color0_i (1 - crack_tint d) from its particle's current state; affine is a
  * device 3x4 row-major [A | t] (the demo's sim-to-world map); off0 (n,3),

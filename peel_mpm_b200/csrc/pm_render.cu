@@ -361,7 +361,14 @@ __global__ void __launch_bounds__(256) k_carry(const Parts P, const int *__restr
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g_n) return;
     const long long b = bind[i];
-    if (b < 0 || b >= P.n) return;
+    if (b < 0 || b >= P.n) {   // an unbound gaussian: NaN outputs (the host wrapper rejects such bindings)
+        const float q = __int_as_float(0x7fc00000);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pos[3 * i + k] = color[3 * i + k] = q;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) cov[9 * i + k] = q;
+        return;
+    }
     const long long ps = P.ps;
     float F[9], xp[3];
 #pragma unroll

@@ -96,11 +96,16 @@ def carry_gaussians(sim, bind, off0, cov0, color0, sim_to_world=None, crack_tint
     ``sim_to_world`` is ``(A (3,3), t (3,))`` (identity by default)."""
     dev = sim.device
     f32 = lambda a: torch.as_tensor(a, device=dev).to(torch.float32).contiguous()
-    bind = torch.as_tensor(bind, device=dev).to(torch.int32).contiguous()
+    bind = torch.as_tensor(bind, device=dev)
+    g = bind.shape[0]
+    if g and (int(bind.min()) < 0 or int(bind.max()) >= sim.n):   # torch indexing would raise here too
+        raise IndexError(f"gaussian bindings must lie in [0, {sim.n})")
+    bind = bind.to(torch.int32).contiguous()
     off0, cov0, color0 = f32(off0), f32(cov0).reshape(-1, 9), f32(color0)
+    if off0.shape != (g, 3) or cov0.shape != (g, 9) or color0.shape != (g, 3):
+        raise ValueError("off0 (n,3), cov0 (n,3,3) and color0 (n,3) must match bind (n,)")
     A, t = (np.eye(3), np.zeros(3)) if sim_to_world is None else sim_to_world
     aff = f32(np.concatenate([np.asarray(A, np.float32).reshape(3, 3), np.asarray(t, np.float32).reshape(3, 1)], 1))
-    g = bind.shape[0]
     pos = torch.empty((g, 3), dtype=torch.float32, device=dev)
     cov = torch.empty((g, 3, 3), dtype=torch.float32, device=dev)
     col = torch.empty((g, 3), dtype=torch.float32, device=dev)

@@ -8,7 +8,9 @@ The reference ``render_gaussians`` (render.py:71-162: EWA projection, soft
 z-buffer in two passes, coverage compositing) renders seeded synthetic
 gaussians on the CPU in float32: an anisotropic cloud in front of the camera
 with some splats behind it, partly outside the frame and one oversized
-splat (dropped by max_raw_radius).  Inputs, camera and images are saved;
+splat (dropped by max_raw_radius); the cases vary tau, r_max, the scale
+modifier, the background, the random downsampling and the overdraw.  Inputs,
+camera and images are saved;
 the GPU box has no reference checkout, the tests read only this file.
 """
 from __future__ import annotations
@@ -44,6 +46,11 @@ CASES = {
     "cloud_default": (0, 3000, 128, 96, 150.0, 140.0, {}),
     "cloud_tau_rmax": (1, 5000, 160, 120, 220.0, 220.0, {"tau": 0.05, "r_max": 16, "scale_modifier": 1.3,
                                                          "bg": (0.1, 0.2, 0.3)}),
+    # the reference's random subset (torch.randperm on a seeded CPU generator)
+    "cloud_downsample": (2, 6000, 96, 96, 120.0, 120.0, {"downsample": 2500, "seed": 7}),
+    # heavy overdraw (hundreds of splats per pixel at r_max 24) on a frame that
+    # is not a multiple of the 8-pixel screen tile
+    "cloud_dense": (3, 10000, 101, 75, 160.0, 160.0, {"r_max": 24, "scale_modifier": 2.6}),
 }
 
 

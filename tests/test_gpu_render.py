@@ -77,3 +77,17 @@ def test_carried_gaussians_match_torch_restatement():
     assert torch.allclose(pos, pos_ref, rtol=1e-6, atol=1e-7)
     assert torch.allclose(cov, cov_ref, rtol=1e-5, atol=1e-12)
     assert torch.allclose(col, col_ref, rtol=1e-6, atol=1e-7)
+
+
+def test_carry_rejects_unbound_gaussians():
+    from helpers import make_gpu_sim
+    from peel_mpm_b200 import scenes
+    from peel_mpm_b200.render import carry_gaussians
+    sim = make_gpu_sim(scenes.tiny_bar())
+    z3 = torch.zeros((2, 3), device="cuda:0")
+    cov = torch.zeros((2, 3, 3), device="cuda:0")
+    for bad in ([0, sim.n], [-1, 0]):
+        with pytest.raises(IndexError):
+            carry_gaussians(sim, torch.tensor(bad, device="cuda:0"), z3, cov, z3)
+    pos, c, col = carry_gaussians(sim, torch.empty(0, dtype=torch.long, device="cuda:0"), z3[:0], cov[:0], z3[:0])
+    assert pos.shape == (0, 3) and c.shape == (0, 3, 3) and col.shape == (0, 3)
