@@ -287,8 +287,9 @@ struct DamageGeom {
     float sig[9], ev[3], Q[9], sp[9], A[9], M[9], A0[9];
     float phi;
 };
-__device__ __forceinline__ void damage_geom(const float R[9], const float tdev[9], float tv, float J, float sc,
-                                            const Parts &P, long long p, DamageGeom &g) {
+__device__ __forceinline__ void damage_geom(const float R[9], const float V[9], const float S[3], const float tdev[9],
+                                            float tv, float J, float sc, const Parts &P, long long p,
+                                            DamageGeom &g) {
     const long long ps = P.ps;
     float sg[9];
 #pragma unroll
@@ -297,7 +298,14 @@ __device__ __forceinline__ void damage_geom(const float R[9], const float tdev[9
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) g.sig[3 * i + j] = 0.5f * (sg[3 * i + j] + sg[3 * j + i]);
-    sym_eig3<5>(g.sig, g.ev, g.Q);
+    {   // eigensystem as the forward took it: U = R V from the taped polar decomposition
+        float U[9];
+        mm3(R, V, U);
+        if (polar_u_ok(S))
+            stress_eig_polar(U, g.sig, g.ev, g.Q);
+        else
+            sym_eig3<5>(g.sig, g.ev, g.Q);
+    }
     {
         float ED[9];
 #pragma unroll
@@ -489,7 +497,7 @@ __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, cons
         const float phib = (c.phi > 1.0f) ? c.zeta * driveb : 0.0f;
         if (phib != 0.0f) {
             DamageGeom dg;
-            damage_geom(c.R, c.tdev, c.tv, c.J, c.sc, P, p, dg);
+            damage_geom(c.R, c.V, c.S, c.tdev, c.tv, c.J, c.sc, P, p, dg);
             const float isc2 = 1.0f / (c.sc * c.sc);
             o.scb += -2.0f * c.phi / c.sc * phib;
             float Mb[9];

@@ -441,6 +441,36 @@ __device__ __forceinline__ void sym_eig3(const float *Ain, float ev[3], float V[
 #undef PM_SWAPCOL
 }
 
+// Eigensystem of the Cauchy stress of the fixed-corotated model, sig =
+// sym(2 mu (F - R) F^T + tv I) / J, from the polar decomposition instead of a
+// second Jacobi solve: with F = U S V^T and R = U V^T, (F - R) F^T =
+// U (S^2 - S) U^T, so sig is diagonal in the left singular vectors U (an
+// f_clamp rescaling of S keeps U).  Columns of Ucols must be the unit vectors
+// F v_j / |F v_j|; the eigenvalues are the Rayleigh quotients q_j^T sig q_j.
+// polar_u_ok() says whether U is usable: not when the smallest |F v_j| is
+// below 1e-3 of the largest (a nearly singular F, whose U is ill-defined);
+// the caller then solves sig by Jacobi sweeps as the reference does.
+// Elsewhere the result agrees with the 5-sweep Jacobi solve to float32
+// rounding; the order of the eigenpairs differs, which sigma+ = Q relu(e) Q^T
+// and phi do not see.
+__device__ __forceinline__ bool polar_u_ok(const float nrm[3]) {
+    const float mx = fmaxf(nrm[0], fmaxf(nrm[1], nrm[2]));
+    const float mn = fminf(nrm[0], fminf(nrm[1], nrm[2]));
+    return mn >= 1e-3f * mx;
+}
+__device__ __forceinline__ void stress_eig_polar(const float Ucols[9], const float sig[9], float ev[3], float Q[9]) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Q[k] = Ucols[k];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float q0 = Q[j], q1 = Q[3 + j], q2 = Q[6 + j];
+        const float s0 = sig[0] * q0 + sig[1] * q1 + sig[2] * q2;
+        const float s1 = sig[3] * q0 + sig[4] * q1 + sig[5] * q2;
+        const float s2 = sig[6] * q0 + sig[7] * q1 + sig[8] * q2;
+        ev[j] = q0 * s0 + q1 * s1 + q2 * s2;
+    }
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -66,12 +66,18 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
 #pragma unroll
     for (int i = 0; i < 3; ++i) S[i] = sqrtf(clamp_min(lamC[i], 1e-12f));   // (617)
     float W[9], R[9];
+    bool u_ok;
     mm3(F, V, W);                                                    // (619)
+    {
+        float wn[3];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        const float nr = sqrtf(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]) + 1e-12f;
+        for (int j = 0; j < 3; ++j) {
+            wn[j] = sqrtf(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]);
+            const float nr = wn[j] + 1e-12f;
 #pragma unroll
-        for (int i = 0; i < 3; ++i) W[3 * i + j] = W[3 * i + j] / nr;   // (620)
+            for (int i = 0; i < 3; ++i) W[3 * i + j] = W[3 * i + j] / nr;   // (620)
+        }
+        u_ok = polar_u_ok(wn);
     }
     mmt3(W, V, R);                                                   // R = What V^T (621)
     if (rec) {
@@ -121,7 +127,10 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
 #pragma unroll
             for (int j = 0; j < 3; ++j) sgs[3 * i + j] = 0.5f * (sg[3 * i + j] + sg[3 * j + i]);
         float ev[3], EV[9];
-        sym_eig3<5>(sgs, ev, EV);
+        if (u_ok)   // (652: sym_eig of sig)
+            stress_eig_polar(W, sgs, ev, EV);
+        else
+            sym_eig3<5>(sgs, ev, EV);
         float sp[9];
         {
             float ED[9];
