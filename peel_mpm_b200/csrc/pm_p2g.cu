@@ -1,21 +1,25 @@
-// Fused constitutive update + P2G, cell-aggregated.
+// Constitutive update + P2G, cell-aggregated, in two kernels.
 //
-// One CTA takes 2048 consecutive particles of the block-sorted order and splits
-// them into segments that share one 8^3-cell sort block.  Each segment owns two
-// shared-memory tiles: the quadratic momentum tile (nodes [8b, 8b+10)^3,
-// {mv, m}) and the cubic damage tile (nodes [8b-1, 8b+11)^3, {sum w d, sum w}).
-// Sub-chunks of 256 particles then go through
-//   phase 1, one particle per thread: particle BC, polar decomposition (Jacobi
-//     eigensolve of F^T F), fixed-corotated Kirchhoff stress, anisotropic
-//     phase-field damage (Jacobi eigensolve of the Cauchy stress), degradation
-//     and the APIC affine term; the P2G payload goes to shared memory;
-//   phase 2, one work item per (cell, x-slab): all particles of a cell share
-//     their quadratic base, so an item sums the cell's contributions to 9
-//     quadratic nodes (3 slabs) or 25 cubic nodes (5 slabs; a cell's cubic
-//     stencils span 5^3 nodes) in registers and adds each node once.  Lanes hold
-//     distinct cells, so the float shared atomics rarely meet on one address.
-// The tiles are flushed with one vector atomic per touched node.  Particles
-// whose stencil needs the reference's edge clamping (base cell outside
+// k_stress, one thread per particle in particle order (coalesced state
+// reads): particle BC, polar decomposition (Jacobi eigensolve of F^T F),
+// fixed-corotated Kirchhoff stress, anisotropic phase-field damage (the
+// Cauchy stress's eigensystem taken from the polar decomposition, a Jacobi
+// solve only for nearly singular F), degradation and the APIC affine term;
+// the P2G payload (5 float4) goes to the particle's slot in the sorted order.
+//
+// k_scatter, one CTA per range of consecutive sorted particles (the range is
+// a tunable, 64..4096), split into segments that share one 8^3-cell sort
+// block.  Each segment owns two shared-memory tiles: the quadratic momentum
+// tile (nodes [8b, 8b+10)^3, {mv, m}) and the cubic damage tile (nodes
+// [8b-1, 8b+11)^3, {sum w d, sum w}).  Sub-chunks stage their payload in shared
+// memory, then one work item per (cell, x-slab): all particles of a cell share
+// their quadratic base, so an item sums the cell's contributions to 9
+// quadratic nodes (3 slabs) or 25 cubic nodes (5 slabs; a cell's cubic
+// stencils span 5^3 nodes) in registers and adds each node once.  Lanes hold
+// distinct cells, so the float shared atomics rarely meet on one address.
+// The tiles are flushed over the segment's footprint with one vector atomic
+// per touched node, marking the touched 4^3 grid blocks.  Particles whose
+// stencil needs the reference's edge clamping (base cell outside
 // [1, n_grid-4]) scatter directly to global memory instead.
 //
 // Reference: anisompm.py:601-724 (constitutive, damage, P2G) and 768-776
