@@ -543,6 +543,10 @@ def run_ours(args):
         nplanes = 27
         host = torch.empty((nplanes, sim._S.shape[1]), dtype=torch.float32, pin_memory=True)
         host.copy_(sim._S[:nplanes])
+        for i in range(max(3, args.warmup)):   # untimed: the first eager calls set up the torch op and workspace
+            sim._S[:nplanes].copy_(host, non_blocking=True)
+            sim.substep(sim._step * sim.dt)
+            host.copy_(sim._S[:nplanes], non_blocking=True)
         torch.cuda.synchronize()
         barrier()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
