@@ -23,10 +23,11 @@ Beside it, in the same JSON line:
                  "auto": no recompute in the backward), and with checkpoints
                  every 10 (segments re-run in the backward): forward time,
                  forward+backward time and their ratio to the plain forward;
-                 gradients with respect to E, fibers, sigma_c and v0 of a
-                 fixed random linear functional of the final positions, with
-                 an optional central-difference check along random
-                 directions.
+                 gradients with respect to E, fibers, sigma_c and v0 of the
+                 mean squared distance to the final positions of a run with
+                 E*1.2, fibers rotated 15 degrees about z and sigma_c*0.8,
+                 their run-to-run spread, and an optional central-difference
+                 check along random directions.
   render      -- the 1M slab's particles carrying one gaussian each
                  (positions x + F off0, covariances F cov0 F^T, damage tint)
                  and EWA-splatted to a 1280x720 image: median carry and
@@ -337,6 +338,7 @@ def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
     with checkpoints every ``every`` substeps (the backward re-runs the
     segments) and with one segment sized to device memory (every substep
     recorded during the forward: nothing re-run)."""
+    import math
     from peel_mpm_b200 import differentiable as dfx
     sim, sc = build_sim(torch, device, seed=0)
     dev = sim.device
@@ -354,13 +356,16 @@ def bench_adjoint(torch, device, n_steps=100, every=10, fd_dirs=32):
         mu, lam, A0 = dfx.material(E, sc.nu, fib, sc.alpha)
         return dfx.rollout(sim, n_steps, mu=mu, lam=lam, sigma_c=sig, A0=A0, v0=v0, checkpoint_every=k)
 
-    # loss: a fixed random linear functional of the final positions, so the
-    # gradient's seed does not depend on float32 noise of the forward
-    wgen = torch.Generator(device=dev).manual_seed(1)
-    Wt = torch.randn((sc.n, 3), device=dev, generator=wgen)
+    # loss: mean squared distance of the final positions to those of a run with
+    # E x 1.2, fibers rotated 15 degrees about z and sigma_c x 0.8
+    t = math.radians(15.0)
+    rz = torch.tensor([[math.cos(t), -math.sin(t), 0.0], [math.sin(t), math.cos(t), 0.0], [0.0, 0.0, 1.0]],
+                      device=dev)
+    with torch.no_grad():
+        target = forward(E0 * 1.2, fib0 @ rz.t(), sig0 * 0.8, v00).clone()
 
     def loss_of(xT):
-        return (xT * Wt).sum() / sc.n
+        return ((xT - target) ** 2).sum(1).mean()
 
     s = torch.cuda.current_stream()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
