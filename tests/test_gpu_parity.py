@@ -292,6 +292,31 @@ def test_plain_small_vs_reference():
         assert errs[200][f] < 10 * max(env[f], 1e-4), (f, errs[200])
 
 
+@pytest.mark.parametrize("name,stride", [("tiny_bar", 1), ("plain_small", 8)])
+def test_error_against_the_float64_reference(name, stride):
+    """The GPU's float32 state after 200 substeps against the reference run in
+    float64: x, v, F, C no further from it than twice the reference's own
+    float32 run (or 2e-4), the chaotic damage fields within ten times the
+    larger of that and the reference's reordering noise."""
+    _, meta = goldens()
+    sc = scenes.SCENES[name]()
+    sim = make_gpu_sim(sc)
+    for s in range(200):
+        sim.substep(s * sc.dt)
+    st = gpu_state(sim, stride)
+    g64 = golden_state(name, "f64", 200)
+    g32 = golden_state(name, "f32", 200)
+    env = meta["noise_envelope"][f"{name}_200"]
+    ours = {f: rel_l2(g64[f], st[f]) for f in FIELDS}
+    ref = {f: rel_l2(g64[f], g32[f]) for f in FIELDS}
+    print(name, "vs float64 reference, ours:", {f: f"{v:.1e}" for f, v in ours.items()},
+          "reference float32:", {f: f"{v:.1e}" for f, v in ref.items()})
+    for f in KIN:
+        assert ours[f] < max(2 * ref[f], 2e-4), (f, ours[f], ref[f])
+    for f in ("d", "lap", "D_hist"):
+        assert ours[f] < 10 * max(ref[f], env.get(f, 0.0), 1e-4), (f, ours[f], ref[f])
+
+
 @pytest.mark.parametrize("name", ["knobs_drop", "interface_peel"])
 def test_knob_scenes_vs_reference(name):
     errs, _ = _compare_to_goldens(name, [10, 60], 1)
