@@ -370,7 +370,7 @@ int pm_bin_sort(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid,
  * No counterpart in the reference, which has no binning and never allocates
  * outside PyTorch. */
 #define PM_BIN_STATIC_MAX_N 262144
-#define PM_BIN_STATIC_SCRATCH_BYTES (16u * PM_BIN_STATIC_MAX_N + 4u * (256u * (PM_BIN_STATIC_MAX_N / 4096u) + 256u))
+#define PM_BIN_STATIC_SCRATCH_BYTES (16u * PM_BIN_STATIC_MAX_N + 4u * (512u * (PM_BIN_STATIC_MAX_N / 4096u) + 512u))
 int pm_bin_sort_static(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid, double inv_dx,
                        uint32_t *keys_out, int32_t *perm_out, void *stream);
 

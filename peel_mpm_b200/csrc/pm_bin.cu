@@ -123,13 +123,15 @@ __global__ void __launch_bounds__(256) k_compact_blocks(unsigned char *__restric
 }
 
 // ------------------------------------------------------------ radix sort
-// Per tile (kSortTile keys) digit histogram -> hist[digit * n_tiles + tile].
-// Full tiles load keys as uint4 (order does not matter for a histogram); int32
-// shared atomics aggregate equal addresses in hardware.
+// Per tile (kSortTile keys) digit histogram -> hist[digit * n_tiles + tile]
+// for RB-bit digits.  Full tiles load keys as uint4 (order does not matter for
+// a histogram); int32 shared atomics aggregate equal addresses in hardware.
+template <int RB>
 __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const unsigned *__restrict__ keys, long long n,
                                                              int shift, unsigned *__restrict__ hist, int n_tiles) {
-    __shared__ unsigned cnt[kRadix];
-    for (int i = threadIdx.x; i < kRadix; i += blockDim.x) cnt[i] = 0;
+    constexpr unsigned R = 1u << RB;
+    __shared__ unsigned cnt[R];
+    for (int i = threadIdx.x; i < (int)R; i += blockDim.x) cnt[i] = 0;
     __syncthreads();
     const long long t0 = (long long)blockIdx.x * kSortTile;
     if (t0 + kSortTile <= n) {
@@ -139,19 +141,19 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const unsigned *__r
         for (int it = 0; it < kSortItems / 4; ++it) v[it] = k4[it * kSortThreads + threadIdx.x];
 #pragma unroll
         for (int it = 0; it < kSortItems / 4; ++it) {
-            atomicAdd(&cnt[(v[it].x >> shift) & (kRadix - 1)], 1u);
-            atomicAdd(&cnt[(v[it].y >> shift) & (kRadix - 1)], 1u);
-            atomicAdd(&cnt[(v[it].z >> shift) & (kRadix - 1)], 1u);
-            atomicAdd(&cnt[(v[it].w >> shift) & (kRadix - 1)], 1u);
+            atomicAdd(&cnt[(v[it].x >> shift) & (R - 1)], 1u);
+            atomicAdd(&cnt[(v[it].y >> shift) & (R - 1)], 1u);
+            atomicAdd(&cnt[(v[it].z >> shift) & (R - 1)], 1u);
+            atomicAdd(&cnt[(v[it].w >> shift) & (R - 1)], 1u);
         }
     } else {
         for (int it = 0; it < kSortItems; ++it) {
             const long long i = t0 + (long long)it * kSortThreads + threadIdx.x;
-            if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & (kRadix - 1)], 1u);
+            if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & (R - 1)], 1u);
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kRadix; i += blockDim.x) hist[(long long)i * n_tiles + blockIdx.x] = cnt[i];
+    for (int i = threadIdx.x; i < (int)R; i += blockDim.x) hist[(long long)i * n_tiles + blockIdx.x] = cnt[i];
 }
 
 // Exclusive scan of each digit's row hist[d][0..n_tiles) in place; row totals
@@ -187,12 +189,20 @@ __global__ void __launch_bounds__(256) k_radix_rowscan(unsigned *__restrict__ hi
     if (tid == 0) dtot[blockIdx.x] = carry;
 }
 
-// Stable scatter of one digit pass.  Warp w of a tile owns keys
-// [w*512, w*512+512) of the tile and ranks them in 16 rounds of 32 in index
-// order; per-warp digit counters are then offset by the earlier warps.  The
-// tile is first written to shared memory in (digit, rank) order, then copied
-// out so that consecutive threads write consecutive addresses of one digit's
-// run.
+// Stable scatter of one digit pass with RB-bit digits.  Warp w of a tile owns
+// keys [w*512, w*512+512) of the tile and ranks them in 16 rounds of 32 in
+// index order; per-warp digit counters are then offset by the earlier warps.
+// The tile is first written to shared memory in (digit, rank) order, then
+// copied out so that consecutive threads write consecutive addresses of one
+// digit's run.  Shared memory (dynamic): per-warp digit counters, the tile's
+// global and local digit starts and the staged tile (43 KB for 8-bit digits,
+// 53 KB for 9-bit ones).
+template <int RB>
+constexpr size_t radix_scatter_smem() {
+    return 4u * ((size_t)(kSortThreads / 32 + 2) * (1u << RB) + 2u * kSortTile);
+}
+
+template <int RB>
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *__restrict__ kin,
                                                                 const int *__restrict__ vin,
                                                                 unsigned *__restrict__ kout, int *__restrict__ vout,
@@ -201,14 +211,18 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *
                                                                 const unsigned *__restrict__ dtot,
                                                                 int *__restrict__ inv) {
     constexpr int W = kSortThreads / 32;
-    __shared__ unsigned wcnt[W][kRadix];
-    __shared__ unsigned gbase[kRadix];     // global start of the tile's run of each digit
-    __shared__ unsigned lbase[kRadix];     // tile-local start of each digit
-    __shared__ unsigned wtot[W];
-    __shared__ unsigned skey[kSortTile];
-    __shared__ int sval[kSortTile];
+    constexpr unsigned R = 1u << RB;
+    constexpr int DPT = (int)R / kSortThreads;   // digits per thread in the prefix step
+    static_assert(DPT >= 1 && (int)R == DPT * kSortThreads, "digits must fill the block");
+    extern __shared__ unsigned sm_radix[];
+    unsigned *wcnt = sm_radix;                   // [W][R]
+    unsigned *gbase = wcnt + W * R;              // [R] global start of the tile's run of each digit
+    unsigned *lbase = gbase + R;                 // [R] tile-local start of each digit
+    unsigned *skey = lbase + R;                  // [kSortTile]
+    int *sval = (int *)(skey + kSortTile);       // [kSortTile]
+    __shared__ unsigned wv[W], wc[W];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < W * kRadix; i += blockDim.x) (&wcnt[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < W * (int)R; i += blockDim.x) wcnt[i] = 0;
     __syncthreads();
     const long long tile0 = (long long)blockIdx.x * kSortTile;
     const int tile_len = (int)min((long long)kSortTile, n - tile0);
@@ -223,37 +237,46 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *
         const bool ok = i < n;
         key[r] = ok ? kin[i] : 0u;
         val[r] = ok ? vin[i] : 0;
-        const unsigned dg = ok ? (key[r] >> shift) & (kRadix - 1) : 0xffffffffu;
+        const unsigned dg = ok ? (key[r] >> shift) & (R - 1) : 0xffffffffu;
         const unsigned peers = __match_any_sync(0xffffffffu, dg);
         const int leader = __ffs(peers) - 1;
         unsigned before = 0;
         if (ok && lane == leader) {
-            before = wcnt[wid][dg];
-            wcnt[wid][dg] = before + (unsigned)__popc(peers);
+            before = wcnt[wid * R + dg];
+            wcnt[wid * R + dg] = before + (unsigned)__popc(peers);
         }
         before = __shfl_sync(0xffffffffu, before, leader);
         rank[r] = before + (unsigned)__popc(peers & lt);
         __syncwarp();
     }
     __syncthreads();
-    {   // per digit (one per thread): exclusive prefix over warps, tile count
-        const int dg = threadIdx.x;   // kRadix == kSortThreads
-        unsigned run = 0;
+    {   // per digit (DPT consecutive digits per thread): exclusive prefix over
+        // warps and the tile count; then exclusive scans over all digits of the
+        // global digit totals (dtot) and of the tile's own counts
+        unsigned tc[DPT], gt[DPT];
+        unsigned st = 0, sg = 0;
 #pragma unroll
-        for (int w = 0; w < W; ++w) {
-            const unsigned c = wcnt[w][dg];
-            wcnt[w][dg] = run;
-            run += c;
+        for (int q = 0; q < DPT; ++q) {
+            const int dg = threadIdx.x * DPT + q;
+            unsigned run = 0;
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                const unsigned c = wcnt[w * R + dg];
+                wcnt[w * R + dg] = run;
+                run += c;
+            }
+            tc[q] = run;
+            gt[q] = dtot[dg];
+            st += run;
+            sg += gt[q];
         }
-        // exclusive scans over digits: global digit bases (dtot) and the tile's own counts
-        unsigned v = dtot[dg], vi = v, c = run, ci = run;
+        unsigned vi = sg, ci = st;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const unsigned y = __shfl_up_sync(0xffffffffu, vi, o);
             const unsigned z = __shfl_up_sync(0xffffffffu, ci, o);
             if (lane >= o) { vi += y; ci += z; }
         }
-        __shared__ unsigned wv[W], wc[W];
         if (lane == 31) { wv[wid] = vi; wc[wid] = ci; }
         __syncthreads();
         unsigned pv = 0, pc = 0;
@@ -262,17 +285,23 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *
             pv += (w < wid) ? wv[w] : 0u;
             pc += (w < wid) ? wc[w] : 0u;
         }
-        gbase[dg] = pv + vi - v + offs[(long long)dg * n_tiles + blockIdx.x];
-        lbase[dg] = pc + ci - c;
+        unsigned ag = pv + vi - sg, at = pc + ci - st;   // exclusive starts of this thread's first digit
+#pragma unroll
+        for (int q = 0; q < DPT; ++q) {
+            const int dg = threadIdx.x * DPT + q;
+            gbase[dg] = ag + offs[(long long)dg * n_tiles + blockIdx.x];
+            lbase[dg] = at;
+            ag += gt[q];
+            at += tc[q];
+        }
     }
-    (void)wtot;
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const long long i = t0 + r * 32 + lane;
         if (i < n) {
-            const unsigned dg = (key[r] >> shift) & (kRadix - 1);
-            const unsigned lp = lbase[dg] + wcnt[wid][dg] + rank[r];
+            const unsigned dg = (key[r] >> shift) & (R - 1);
+            const unsigned lp = lbase[dg] + wcnt[wid * R + dg] + rank[r];
             skey[lp] = key[r];
             sval[lp] = val[r];
         }
@@ -280,7 +309,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *
     __syncthreads();
     for (int i = threadIdx.x; i < tile_len; i += kSortThreads) {
         const unsigned k = skey[i];
-        const unsigned dg = (k >> shift) & (kRadix - 1);
+        const unsigned dg = (k >> shift) & (R - 1);
         const unsigned gp = gbase[dg] + (unsigned)i - lbase[dg];
         kout[gp] = k;
         vout[gp] = sval[i];
@@ -288,17 +317,46 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned *
     }
 }
 
+// One-time kernel attribute set-up for the current device (the 9-bit scatter
+// needs more than 48 KB of dynamic shared memory); not a stream operation, so
+// pm_prepare runs it before any capture.
+void prepare_sort() {
+    static int done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || done[dev]) return;
+    cudaFuncSetAttribute(k_radix_scatter<kRadixBitsTop>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)radix_scatter_smem<kRadixBitsTop>());
+    done[dev] = 1;
+}
+
+template <int RB>
+static void radix_pass(const WS &w, long long n, int tiles, int shift, bool need_hist, const unsigned *kin,
+                       const int *vin, unsigned *kout, int *vout, int *inv, cudaStream_t s) {
+    if (need_hist) k_radix_hist<RB><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, w.hist, tiles);
+    k_radix_rowscan<<<1u << RB, 256, 0, s>>>(w.hist, tiles, w.dtot);
+    k_radix_scatter<RB><<<tiles, kSortThreads, radix_scatter_smem<RB>(), s>>>(kin, vin, kout, vout, n, shift, w.hist,
+                                                                             tiles, w.dtot, inv);
+}
+
 void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv, bool hist0_ready) {
     if (n <= 0) return;
+    prepare_sort();
     const int tiles = (int)((n + kSortTile - 1) / kSortTile);
     unsigned *kin = w.keys_a, *kout = w.keys_b;
     int *vin = w.vals_a, *vout = w.vals_b;
+    int shift = 0, rem = w.key_bits;
     for (int pass = 0; pass < w.passes; ++pass) {
-        const int shift = pass * kRadixBits;
-        if (pass > 0 || !hist0_ready) k_radix_hist<<<tiles, kSortThreads, 0, s>>>(kin, n, shift, w.hist, tiles);
-        k_radix_rowscan<<<kRadix, 256, 0, s>>>(w.hist, tiles, w.dtot);
-        k_radix_scatter<<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, w.hist, tiles, w.dtot,
-                                                       pass == w.passes - 1 ? inv : nullptr);
+        const int rb = radix_digit_bits(rem);
+        // launch_keys leaves the first pass's 8-bit histogram
+        const bool need_hist = pass > 0 || !hist0_ready || rb != kRadixBits;
+        int *iv = pass == w.passes - 1 ? inv : nullptr;
+        if (rb == kRadixBitsTop)
+            radix_pass<kRadixBitsTop>(w, n, tiles, shift, need_hist, kin, vin, kout, vout, iv, s);
+        else
+            radix_pass<kRadixBits>(w, n, tiles, shift, need_hist, kin, vin, kout, vout, iv, s);
+        shift += rb;
+        rem -= rb;
         unsigned *tk = kin; kin = kout; kout = tk;
         int *tv = vin; vin = vout; vout = tv;
     }

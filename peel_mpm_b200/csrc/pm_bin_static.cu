@@ -19,7 +19,7 @@ namespace {
 constexpr long long kMaxN = PM_BIN_STATIC_MAX_N;
 constexpr int kMaxTiles = (int)((kMaxN + pm::kSortTile - 1) / pm::kSortTile);
 constexpr size_t kKeyBytes = 4u * (size_t)kMaxN;
-constexpr size_t kBytes = 4 * kKeyBytes + 4u * ((size_t)pm::kRadix * kMaxTiles + pm::kRadix);
+constexpr size_t kBytes = 4 * kKeyBytes + 4u * ((size_t)pm::kRadixTop * kMaxTiles + pm::kRadixTop);
 static_assert(kBytes == PM_BIN_STATIC_SCRATCH_BYTES, "header size must match the array");
 static_assert(kKeyBytes % 256 == 0, "sub-buffers stay 256-byte aligned");
 
@@ -71,8 +71,10 @@ extern "C" int pm_bin_sort_static(const float *x, int64_t n, int64_t plane_strid
     w.vals_b = (int *)(b + 3 * kKeyBytes);
     w.hist = (unsigned *)(b + 4 * kKeyBytes);
     w.n_tiles = (int)((n + pm::kSortTile - 1) / pm::kSortTile);
-    w.dtot = w.hist + (size_t)pm::kRadix * w.n_tiles;
-    w.passes = pm::make_layout(n, n_grid).passes;
+    w.dtot = w.hist + (size_t)pm::kRadixTop * w.n_tiles;
+    const pm::Layout L = pm::make_layout(n, n_grid);
+    w.passes = L.passes;
+    w.key_bits = L.key_bits;
     const unsigned *sorted = (w.passes & 1) ? w.keys_b : w.keys_a;
     const int *perm = (w.passes & 1) ? w.vals_b : w.vals_a;
     cudaStream_t s = (cudaStream_t)stream;

@@ -112,6 +112,7 @@ int pm_prepare(void) {
     int rc = check_device();
     if (rc) return rc;
     pm::prepare_p2g();
+    pm::prepare_sort();
     return cuda_check("pm_prepare");
 }
 

@@ -16,8 +16,20 @@ constexpr int kSortBlockBits = 9;      // log2(8^3)
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;   // keys per radix tile
+// Radix digits: 8 bits per pass; the last pass takes 9 when exactly 9 bits
+// remain, which saves a pass (25-bit keys: 8 + 8 + 9).
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
+constexpr int kRadixBitsTop = 9;
+constexpr int kRadixTop = 1 << kRadixBitsTop;
+__host__ __device__ constexpr int radix_digit_bits(int remaining) {
+    return remaining == kRadixBitsTop ? kRadixBitsTop : kRadixBits;
+}
+__host__ __device__ inline int radix_passes(int key_bits) {
+    int p = 0;
+    for (int rem = key_bits < 1 ? 1 : key_bits; rem > 0; rem -= radix_digit_bits(rem)) ++p;
+    return p;
+}
 constexpr int kG2PThreads = 256;     // G2P particles per CTA
 
 // Device control block: per-substep inputs and status counters.
@@ -53,7 +65,7 @@ __host__ __device__ inline int blocked_key_bits(int ng) {
 struct Layout {
     size_t ctrl, keys_a, keys_b, vals_a, vals_b, hist, block_mask, block_list;
     size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, tables, total;
-    int passes, n_tiles, nbs;
+    int passes, key_bits, n_tiles, nbs;
     long long n_blocks, n_nodes;
 };
 
@@ -65,8 +77,8 @@ __host__ __device__ inline Layout make_layout_sized(long long n, long long n_nod
     const size_t A = 256;
     L.n_tiles = (int)((n + kSortTile - 1) / kSortTile);
     if (L.n_tiles < 1) L.n_tiles = 1;
-    L.passes = (key_bits + kRadixBits - 1) / kRadixBits;
-    if (L.passes < 1) L.passes = 1;
+    L.key_bits = key_bits < 1 ? 1 : key_bits;
+    L.passes = radix_passes(L.key_bits);
     L.nbs = 0;
     L.n_blocks = n_blocks;
     L.n_nodes = n_nodes;
@@ -77,7 +89,7 @@ __host__ __device__ inline Layout make_layout_sized(long long n, long long n_nod
     L.keys_b = o;     o = align_up(o + 4 * nn, A);
     L.vals_a = o;     o = align_up(o + 4 * nn, A);
     L.vals_b = o;     o = align_up(o + 4 * nn, A);
-    L.hist = o;       o = align_up(o + 4 * ((size_t)kRadix * L.n_tiles + kRadix), A);
+    L.hist = o;       o = align_up(o + 4 * ((size_t)kRadixTop * L.n_tiles + kRadixTop), A);
     L.block_mask = o; o = align_up(o + (size_t)L.n_blocks, A);
     L.block_list = o; o = align_up(o + 4 * (size_t)L.n_blocks, A);
     L.g_mom = o;      o = align_up(o + 16 * (size_t)L.n_nodes, A);
@@ -106,8 +118,8 @@ struct WS {
     Ctrl *ctrl;
     unsigned *keys_a, *keys_b;
     int *vals_a, *vals_b;
-    unsigned *hist;          // [kRadix][n_tiles] tile counts
-    unsigned *dtot;          // [kRadix] digit totals of the current pass
+    unsigned *hist;          // [digits][n_tiles] tile counts (up to kRadixTop digits)
+    unsigned *dtot;          // [digits] digit totals of the current pass
     unsigned char *block_mask;
     int *block_list;
     float4 *g_mom;      // {mv.x, mv.y, mv.z, m}, zero between substeps
@@ -122,7 +134,7 @@ struct WS {
     const unsigned *sorted_keys;
     const int *perm;
     int *inv_perm;      // particle -> sorted position, written by the last radix pass
-    int passes, n_tiles, nbs;
+    int passes, key_bits, n_tiles, nbs;
     long long n_blocks;
 };
 
@@ -135,7 +147,7 @@ inline WS make_ws(void *base, const Layout &L) {
     w.vals_a = (int *)(b + L.vals_a);
     w.vals_b = (int *)(b + L.vals_b);
     w.hist = (unsigned *)(b + L.hist);
-    w.dtot = w.hist + (size_t)kRadix * L.n_tiles;
+    w.dtot = w.hist + (size_t)kRadixTop * L.n_tiles;
     w.block_mask = (unsigned char *)(b + L.block_mask);
     w.block_list = (int *)(b + L.block_list);
     w.g_mom = (float4 *)(b + L.g_mom);
@@ -148,6 +160,7 @@ inline WS make_ws(void *base, const Layout &L) {
     w.tape_aff_stride = 0;
     w.payload = (float4 *)(b + L.payload);
     w.passes = L.passes;
+    w.key_bits = L.key_bits;
     w.n_tiles = L.n_tiles;
     w.nbs = L.nbs;
     w.n_blocks = L.n_blocks;

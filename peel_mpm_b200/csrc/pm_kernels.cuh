@@ -13,6 +13,7 @@ template <class SC> void launch_keys(const SC &sc, const WS &w, const Parts &P, 
 void launch_sort(const WS &w, long long n, cudaStream_t s, int *inv = nullptr, bool hist0_ready = false);
 void launch_compact(const WS &w, cudaStream_t s);
 void prepare_p2g();
+void prepare_sort();
 void launch_keys_only(const float *x, long long n, long long ps, int ng, float inv_dx, bool blocked, const WS &w,
                       cudaStream_t s);
 template <class SC> void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int range = 0);

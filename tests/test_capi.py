@@ -45,7 +45,8 @@ def test_workspace_layout_is_aligned_and_disjoint(n, ng):
     nn = max(n, 1)
     G = ng ** 3
     assert L.keys_b - L.keys_a >= 4 * nn and L.g_dmg - L.g_mom >= 16 * G and L.payload - L.g_gd >= 4 * G and L.inv_perm - L.payload >= 80 * nn and L.total - L.inv_perm >= 4 * nn
-    assert L.sort_passes == 3 if ng >= 64 else L.sort_passes >= 1
+    key_bits = max(max(_bits(ng ** 3), 1), _bits(((ng + 7) // 8) ** 3) + 9)
+    assert L.sort_passes == _radix_passes(key_bits)
     assert _lib.workspace_size(n, ng) == L.total
 
 
@@ -68,6 +69,16 @@ def _bits(v):
     return b
 
 
+def _radix_passes(key_bits):
+    """LSD passes of the sort: 8-bit digits, the last one 9 bits wide when
+    exactly 9 bits remain."""
+    p, rem = 0, max(key_bits, 1)
+    while rem > 0:
+        rem -= 9 if rem == 9 else 8
+        p += 1
+    return p
+
+
 @pytest.mark.parametrize("ns,gs", [([1000, 0, 5000, 70000], [32, 64, 48, 128]), ([1], [4]),
                                    ([4096] * 64, [32 + 16 * (k % 7) for k in range(64)])])
 def test_batch_layout_packs_scenes(ns, gs):
@@ -77,7 +88,7 @@ def test_batch_layout_packs_scenes(ns, gs):
     assert L.n_grid_blocks == sum(((g + 3) // 4) ** 3 for g in gs)
     assert L.n_sort_blocks == sum(((g + 7) // 8) ** 3 for g in gs)
     assert L.n_g2p_ctas == sum((n + 255) // 256 for n in ns)
-    assert L.ws.sort_passes == (_bits(L.n_sort_blocks) + 9 + 7) // 8
+    assert L.ws.sort_passes == _radix_passes(_bits(L.n_sort_blocks) + 9)
     w = L.ws
     offs = [w.ctrl, w.keys_a, w.keys_b, w.vals_a, w.vals_b, w.hist, w.block_mask, w.block_list, w.g_mom, w.g_dmg,
             w.g_vel, w.g_gd, w.payload, w.inv_perm, L.params, L.tables, w.total]
