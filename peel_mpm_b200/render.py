@@ -89,23 +89,41 @@ def to_uint8(img):
     return (img.clamp(0, 1) * 255).to(torch.uint8).cpu().numpy()
 
 
-def carry_gaussians(sim, bind, off0, cov0, color0, sim_to_world=None, crack_tint=0.0):
+def world_map(A=None, t=None, device="cuda:0"):
+    """The affine sim-to-world map x -> A x + t as the (3, 4) float32 device
+    tensor [A | t] that ``carry_gaussians`` takes (identity by default)."""
+    A = np.eye(3) if A is None else np.asarray(A, np.float64).reshape(3, 3)
+    t = np.zeros(3) if t is None else np.asarray(t, np.float64).reshape(3)
+    return torch.tensor(np.concatenate([A, t[:, None]], 1), dtype=torch.float32, device=device)
+
+
+def carry_gaussians(sim, bind, off0, cov0, color0, sim_to_world=None, crack_tint=0.0, check_bind=True):
     """Gaussians carried by the solver's particles (run_orange.py:116-133):
     positions ``A x + t + F off0``, covariances ``F cov0 F^T`` and colours
     darkened by damage, for gaussian i bound to particle ``bind[i]``.
-    ``sim_to_world`` is ``(A (3,3), t (3,))`` (identity by default)."""
+    ``sim_to_world`` is ``(A (3,3), t (3,))``, a (3, 4) device tensor from
+    ``world_map`` (no host-to-device copy per call), or None (identity).
+    ``check_bind`` range-checks the bindings, which synchronises the host once;
+    a caller that checked them already passes False (an out-of-range id then
+    gives NaN outputs)."""
     dev = sim.device
     f32 = lambda a: torch.as_tensor(a, device=dev).to(torch.float32).contiguous()
     bind = torch.as_tensor(bind, device=dev)
     g = bind.shape[0]
-    if g and (int(bind.min()) < 0 or int(bind.max()) >= sim.n):   # torch indexing would raise here too
+    if check_bind and g and (int(bind.min()) < 0 or int(bind.max()) >= sim.n):   # torch indexing would raise too
         raise IndexError(f"gaussian bindings must lie in [0, {sim.n})")
     bind = bind.to(torch.int32).contiguous()
     off0, cov0, color0 = f32(off0), f32(cov0).reshape(-1, 9), f32(color0)
     if off0.shape != (g, 3) or cov0.shape != (g, 9) or color0.shape != (g, 3):
         raise ValueError("off0 (n,3), cov0 (n,3,3) and color0 (n,3) must match bind (n,)")
-    A, t = (np.eye(3), np.zeros(3)) if sim_to_world is None else sim_to_world
-    aff = f32(np.concatenate([np.asarray(A, np.float32).reshape(3, 3), np.asarray(t, np.float32).reshape(3, 1)], 1))
+    if isinstance(sim_to_world, torch.Tensor):
+        aff = sim_to_world
+        if aff.shape != (3, 4) or aff.dtype != torch.float32 or aff.device != torch.device(dev) or \
+                not aff.is_contiguous():
+            raise ValueError("sim_to_world tensor must be a contiguous (3, 4) float32 tensor on the solver's device")
+    else:
+        A, t = (None, None) if sim_to_world is None else sim_to_world
+        aff = world_map(A, t, dev)
     pos = torch.empty((g, 3), dtype=torch.float32, device=dev)
     cov = torch.empty((g, 3, 3), dtype=torch.float32, device=dev)
     col = torch.empty((g, 3), dtype=torch.float32, device=dev)
