@@ -37,10 +37,18 @@ class Camera:
         return X @ self.R + self.T
 
     def _struct(self):
+        # R and T live on the device; their host copy is read back only when a
+        # tensor is replaced or modified in place (identity and version
+        # counter), so rendering a sequence of frames does not synchronise
+        key = (id(self.R), self.R._version, id(self.T), self.T._version)
+        if getattr(self, "_rt_key", None) != key:
+            self._rt_host = (self.R.detach().cpu().numpy().reshape(-1).tolist(),
+                             self.T.detach().cpu().numpy().reshape(-1).tolist())
+            self._rt_key = key
         c = _lib.pm_camera()
-        for k, v in enumerate(self.R.detach().cpu().numpy().reshape(-1).tolist()):
+        for k, v in enumerate(self._rt_host[0]):
             c.R[k] = v
-        for k, v in enumerate(self.T.detach().cpu().numpy().reshape(-1).tolist()):
+        for k, v in enumerate(self._rt_host[1]):
             c.T[k] = v
         c.fx, c.fy = float(self.fx), float(self.fy)
         c.width, c.height = int(self.W), int(self.H)
