@@ -87,6 +87,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-late", action="store_true", help="skip the late-run (substeps 400-420) sample")
     return ap.parse_args()
 
 
@@ -203,8 +204,11 @@ def time_kernels(torch, sim, steps, t0):
     return {k: v / steps for k, v in acc.items()}
 
 
-def cpu_baseline(sample_steps=3):
-    """The oracle port on the host cores: full 1M scene, a few substeps."""
+def cpu_baseline(torch, device, sample_steps=3):
+    """The oracle port on the host cores: full 1M scene, a few substeps.
+    The same substeps run on the GPU from the same initial state give the
+    line's ``parity`` key (relative L2 per field after 1 + sample_steps
+    substeps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     from peel_mpm_b200 import scenes
@@ -216,9 +220,21 @@ def cpu_baseline(sample_steps=3):
     for i in range(sample_steps):
         sim.substep((i + 1) * sc.dt)
     dt = time.perf_counter() - t
-    return {"value": sc.n * sample_steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+    base = {"value": sc.n * sample_steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{sample_steps} substeps of the 1,048,576-particle scene after 1 warm-up, "
                       f"C oracle with OpenMP on {cores} threads"}
+    gpu, _ = build_sim(torch, device, seed=0)
+    for i in range(sample_steps + 1):
+        gpu.substep(i * sc.dt)
+    torch.cuda.synchronize()
+    errs = {}
+    for f in ("x", "v", "F", "C", "d", "lap", "D_hist"):
+        a = getattr(sim, f).astype(np.float64).ravel()
+        b = getattr(gpu, f).detach().cpu().numpy().astype(np.float64).ravel()
+        errs[f] = float(np.linalg.norm(a - b) / max(np.linalg.norm(a), 1e-30))
+    parity = {"substeps": sample_steps + 1, "particles": sc.n, "rel_l2_vs_oracle": errs, "bound": 1e-5,
+              "full_runs": "tests/test_gpu_parity_configs.py: 1M x 500, peel 1/8 x 200, 64-scene batch x 20"}
+    return base, parity
 
 
 # ------------------------------------------------------------------ arms
@@ -321,7 +337,8 @@ def bench_batched(torch, device, rank=0, world=1, max_over_ranks=lambda v: v, ba
             "ms_per_substep": tb / n_sub, "sequential_ms_per_substep": ts / n_sub,
             "scenes": len(all_scs), "particles": total, "grids": sorted({sc.n_grid for sc in all_scs}),
             "scenes_per_rank": len(scs), "substeps_per_frame": n_sub, "frames": reps,
-            "p2g_range": tuned, "gpu_launches_per_substep": 6 + 3 * passes,
+            "tuned": {"knobs": tuned, "candidates_ms": autotune._CACHE[autotune.bucket(batch)]["ms"]},
+            "gpu_launches_per_substep": 7 + 3 * passes,
             "nonfinite": sum(x["nonfinite"] for x in st),
             "what": "64 scenes, log-uniform 4k-256k particles, one BatchedAnisoMPM.run_frame per frame (one CUDA "
                     "graph) vs AnisoMPM.run_frame per scene (one CUDA graph each; and eager, one C call per "
@@ -518,7 +535,7 @@ def run_ours(args):
     sim, sc = build_sim(torch, device, seed=rank)
     n = sim.n
     from peel_mpm_b200 import autotune
-    tuned = autotune.tune(sim)       # P2G tile for this size bucket (state restored afterwards)
+    tuned = autotune.tune(sim)       # launch knobs for this size bucket (state restored afterwards)
     t0 = 0.0
     chunk = min(100, args.steps)
     for i in range(args.warmup):
@@ -541,6 +558,27 @@ def run_ours(args):
     value = world * n * args.steps / (ms_max * 1e-3)
     st = sim.status()
     n_active = st["n_active_blocks"] * 64
+
+    # late-run sample: the scene's state around substep 400 of its 500 (fractured,
+    # more active blocks), 20 substeps timed the same way
+    late = None
+    if not args.no_late:
+        done = sim._step
+        if done < 400:
+            run_frames(sim, 400 - done, done * sim.dt, chunk)
+        torch.cuda.synchronize()
+        barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k = 20
+        a.record(s)
+        run_frames(sim, k, sim._step * sim.dt, k)
+        b.record(s)
+        torch.cuda.synchronize()
+        late_ms = max_over_ranks(a.elapsed_time(b))
+        st_late = sim.status()
+        late = {"substeps": f"{sim._step - k}-{sim._step}", "ms_per_step": late_ms / k,
+                "value": world * n * k / (late_ms * 1e-3), "unit": UNIT,
+                "n_active_blocks": st_late["n_active_blocks"], "nonfinite": st_late["nonfinite"]}
 
     # e2e: mutable state from pinned host memory in, back out, every substep
     e2e = None
@@ -596,13 +634,13 @@ def run_ours(args):
     if rank == 0 and args.form in ("all", "adjoint"):
         forms["fwd_adjoint"] = bench_adjoint(torch, device, fd_dirs=args.fd_dirs)
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline()
+        cpu, parity = cpu_baseline(torch, device)
 
-    # clock, keys (+ first digit histogram), 3 per radix pass but the first's histogram, stress, scatter,
-    # compact, grid, g2p
-    launches_per_step = 6 + 3 * sim_passes(sim)
+    # clock, keys (+ first digit histogram), 3 per radix pass but the first's histogram, sub-block list,
+    # stress, tiles, compact, grid, g2p
+    launches_per_step = 7 + 3 * sim_passes(sim)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -610,10 +648,12 @@ def run_ours(args):
                 "config": {"workload": "plain AnisoMPM substep, 1,048,576 particles, 128^3 grid (seeded slab)",
                            "particles": n, "n_grid": sim.n_grid, "dt": sim.dt, "parallelism": f"replicas{world}",
                            "l2": "inputs larger than L2 (particle state ~290 MB)",
-                           "graph_substeps": chunk, "p2g_range": tuned,
-                           "p2g_range_ms": autotune._CACHE[autotune.bucket(sim)]["ms"]},
+                           "graph_substeps": chunk},
+                "tuned": {"knobs": tuned, "candidates_ms": autotune._CACHE[autotune.bucket(sim)]["ms"],
+                          "substeps_per_candidate": autotune._CACHE[autotune.bucket(sim)]["substeps"]},
                 "clocks": clocks.summary(), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches_per_step * args.steps, "status": st}
+                "gpu_launches": launches_per_step * args.steps, "status": st, "late_run": late,
+                "parity": parity}
         line.update(forms)
         print(json.dumps(line), flush=True)
     if world > 1:

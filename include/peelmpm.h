@@ -77,9 +77,10 @@ typedef struct pm_params {
     double f_clamp_hi;
     int32_t n_grips;
     int32_t n_colliders;
-    int32_t p2g_range;          /* sorted particles per P2G block (64..4096); 0 = 512 (tuning knob, no
-                                   effect on results beyond float summation order) */
-    int32_t reserved;
+    int32_t p2g_ctas_per_sm;    /* resident P2G CTAs per SM (0: as many as fit, else 1..8); a tuning
+                                   knob with no effect on results (the grid sums are exact) */
+    int32_t grid_ctas_per_sm;   /* grid-update CTAs per SM (0: the library default, else 1..64); a
+                                   tuning knob with no effect on results */
     pm_grip grips[PM_MAX_GRIPS];
     pm_collider colliders[PM_MAX_COLLIDERS];
 } pm_params;
@@ -142,14 +143,22 @@ int pm_prepare(void);
 int pm_workspace_size(int64_t n, int32_t n_grid, size_t *bytes);
 int pm_workspace_init(void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, void *stream);
 
-/* Byte offsets of the workspace's views (for inspection and tests). */
+/* Byte offsets of the workspace's views (for inspection and tests).  g_mom
+ * and g_dmg hold int64 fixed-point sums (4 and 2 per node) whose units are
+ * fixed per substep from the particles' bounds; pm_grid_sums converts them. */
 typedef struct pm_ws_layout {
     size_t ctrl, keys_a, keys_b, vals_a, vals_b, hist, block_mask, block_list;
-    size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, total;
+    size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, work, total;
     int32_t sort_passes;             /* sorted keys/perm end in *_a if even, *_b if odd */
     int32_t n_tiles;
 } pm_ws_layout;
 int pm_workspace_layout(int64_t n, int32_t n_grid, pm_ws_layout *out);
+
+/* The P2G accumulators of a plain workspace as floats, between pm_p2g and
+ * pm_grid_update: mom (n_grid^3, 4) {m v, m} and dmg (n_grid^3, 2)
+ * {sum w d, sum w} (anisompm.py:716-724, 771-776).  For inspection; the
+ * substep itself never needs it. */
+int pm_grid_sums(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, float *mom, float *dmg, void *stream);
 
 /* ------------------------------------------------------------ the substep */
 
@@ -343,16 +352,21 @@ int pm_carry_gaussians(const pm_particles *P, const int32_t *bind, const float *
 
 /* ---------------------------------------------------------------- helpers */
 
-/* Batched 3x3 symmetric eigendecomposition by 5-sweep cyclic Jacobi, A
- * (n,3,3) row-major contiguous -> ascending evals (n,3), eigenvector columns
- * evecs (n,3,3).  Replaces sym_eig (anisompm.py:48-95). */
+/* Batched 3x3 symmetric eigendecomposition by cyclic Jacobi with `sweeps`
+ * sweeps (the reference's default is 5; any count >= 0, 0 sorting the
+ * symmetrised diagonal), A (n,3,3) row-major contiguous -> ascending evals
+ * (n,3), eigenvector columns evecs (n,3,3).  Replaces sym_eig
+ * (anisompm.py:48-95). */
 int pm_sym_eig(const float *A, int64_t n, int32_t sweeps, float *evals, float *evecs, void *stream);
 
 /* Binning only, in the reference's own numbering: keys_out = the sorted
  * _node_index of every particle's quadratic base cell (anisompm.py:544-548,
  * 586-590) and perm_out = the stable argsort of those keys, for positions x
- * (3 planes of stride `plane_stride`).  Uses the workspace's sort buffers;
- * keys_out / perm_out must not alias the workspace. */
+ * (3 planes of stride `plane_stride`).  Uses the sort buffers at the start of
+ * a substep workspace, so ws_bytes need only be pm_bin_workspace_size(n,
+ * n_grid) (a full pm_workspace_size workspace also serves); keys_out /
+ * perm_out must not alias the workspace. */
+int pm_bin_workspace_size(int64_t n, int32_t n_grid, size_t *bytes);
 int pm_bin_sort(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid, double inv_dx,
                 uint32_t *keys_out, int32_t *perm_out, void *ws, size_t ws_bytes, void *stream);
 

@@ -18,8 +18,9 @@ PM_OK, PM_ERR_ARG, PM_ERR_CUDA, PM_ERR_WORKSPACE, PM_ERR_UNSUPPORTED = 0, 1, 2, 
 
 EXPORTS = (
     "pm_abi_version", "pm_last_error", "pm_struct_size", "pm_prepare", "pm_workspace_size", "pm_workspace_init",
-    "pm_workspace_layout", "pm_substep", "pm_substep_dev_clock", "pm_set_clock", "pm_bin", "pm_p2g",
-    "pm_grid_update", "pm_g2p", "pm_read_status", "pm_sym_eig", "pm_bin_sort", "pm_bin_sort_static",
+    "pm_workspace_layout", "pm_grid_sums", "pm_substep", "pm_substep_dev_clock", "pm_set_clock", "pm_bin", "pm_p2g",
+    "pm_grid_update", "pm_g2p", "pm_read_status", "pm_sym_eig", "pm_bin_workspace_size", "pm_bin_sort",
+    "pm_bin_sort_static",
     "pm_batch_workspace_size", "pm_batch_workspace_layout", "pm_batch_workspace_init", "pm_batch_set_params",
     "pm_batch_workspace_release", "pm_batch_substep", "pm_batch_read_status",
     "pm_tape_size", "pm_tape_init", "pm_substep_record", "pm_substep_adjoint", "pm_observe",
@@ -46,7 +47,8 @@ class pm_params(C.Structure):
         ("gravity", C.c_double * 3), ("grid_damp", C.c_double),
         ("use_f_clamp", C.c_int32), ("record_stress", C.c_int32),
         ("f_clamp_lo", C.c_double), ("f_clamp_hi", C.c_double),
-        ("n_grips", C.c_int32), ("n_colliders", C.c_int32), ("p2g_range", C.c_int32), ("reserved", C.c_int32),
+        ("n_grips", C.c_int32), ("n_colliders", C.c_int32), ("p2g_ctas_per_sm", C.c_int32),
+        ("grid_ctas_per_sm", C.c_int32),
         ("grips", pm_grip * PM_MAX_GRIPS), ("colliders", pm_collider * PM_MAX_COLLIDERS),
     ]
 
@@ -73,7 +75,8 @@ class pm_status_info(C.Structure):
 
 class pm_ws_layout(C.Structure):
     _fields_ = [(f, C.c_size_t) for f in ("ctrl", "keys_a", "keys_b", "vals_a", "vals_b", "hist", "block_mask",
-                                          "block_list", "g_mom", "g_dmg", "g_vel", "g_gd", "payload", "inv_perm", "total")] + \
+                                          "block_list", "g_mom", "g_dmg", "g_vel", "g_gd", "payload", "inv_perm",
+                                          "work", "total")] + \
                [("sort_passes", C.c_int32), ("n_tiles", C.c_int32)]
 
 
@@ -128,6 +131,7 @@ def load():
         "pm_workspace_size": (C.c_int, [i64, i32, C.POINTER(sz)]),
         "pm_workspace_init": (C.c_int, [vp, sz, i64, i32, vp]),
         "pm_workspace_layout": (C.c_int, [i64, i32, C.POINTER(pm_ws_layout)]),
+        "pm_grid_sums": (C.c_int, [vp, sz, i64, i32, vp, vp, vp]),
         "pm_substep": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), vp, sz, C.POINTER(pm_clock), vp]),
         "pm_substep_dev_clock": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), vp, sz, vp, i32, vp]),
         "pm_set_clock": (C.c_int, [C.POINTER(pm_params), vp, sz, i64, C.POINTER(pm_clock), vp]),
@@ -137,6 +141,7 @@ def load():
         "pm_g2p": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), vp, sz, vp]),
         "pm_read_status": (C.c_int, [vp, sz, i64, i32, C.POINTER(pm_status_info), vp]),
         "pm_sym_eig": (C.c_int, [vp, i64, i32, vp, vp, vp]),
+        "pm_bin_workspace_size": (C.c_int, [i64, i32, C.POINTER(sz)]),
         "pm_bin_sort": (C.c_int, [vp, i64, i64, i32, C.c_double, vp, vp, vp, sz, vp]),
         "pm_bin_sort_static": (C.c_int, [vp, i64, i64, i32, C.c_double, vp, vp, vp]),
         "pm_batch_workspace_size": (C.c_int, [i32, vp, vp, C.POINTER(sz)]),
@@ -188,6 +193,13 @@ def workspace_size(n: int, n_grid: int) -> int:
     lib = load()
     out = C.c_size_t(0)
     check(lib.pm_workspace_size(int(n), int(n_grid), C.byref(out)), "pm_workspace_size")
+    return int(out.value)
+
+
+def bin_workspace_size(n: int, n_grid: int) -> int:
+    lib = load()
+    out = C.c_size_t(0)
+    check(lib.pm_bin_workspace_size(int(n), int(n_grid), C.byref(out)), "pm_bin_workspace_size")
     return int(out.value)
 
 

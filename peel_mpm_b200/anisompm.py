@@ -182,7 +182,8 @@ class AnisoMPM:
         self.n = 0
         self.record_stress = False
         self.use_graphs = True
-        self.p2g_range = 0        # sorted particles per P2G block; 0 = library default (autotune.tune sets it)
+        self.p2g_ctas_per_sm = 0  # launch knobs (0 = library defaults; autotune.tune sets them); results
+        self.grid_ctas_per_sm = 0  # do not depend on them
         self._S = None            # float32 planes (N_PLANES, stride)
         self._allow = None        # bool (N)
         self._imask = None        # bool (N)
@@ -428,7 +429,8 @@ class AnisoMPM:
     def _build_params(self, grips):
         key = (self.n_grid, self.grid_lim, self.dt, self._gravity_host, self.grid_damp,
                None if self.f_clamp is None else tuple(float(v) for v in self.f_clamp), self.damage_every,
-               bool(self.record_stress), int(self.p2g_range), tuple((g.velocity, g.ramp) for g in grips),
+               bool(self.record_stress), int(self.p2g_ctas_per_sm), int(self.grid_ctas_per_sm),
+               tuple((g.velocity, g.ramp) for g in grips),
                tuple((c.kind, c.mode, c.friction, c.radius, tuple(c.normal)) for c in self.colliders))
         if key == self._params_key:
             return self._params
@@ -443,7 +445,8 @@ class AnisoMPM:
         if self.f_clamp is not None:
             p.f_clamp_lo, p.f_clamp_hi = float(self.f_clamp[0]), float(self.f_clamp[1])
         p.record_stress = int(bool(self.record_stress))
-        p.p2g_range = int(self.p2g_range)
+        p.p2g_ctas_per_sm = int(self.p2g_ctas_per_sm)
+        p.grid_ctas_per_sm = int(self.grid_ctas_per_sm)
         p.n_grips = len(grips)
         for i, g in enumerate(grips):
             for a in range(3):

@@ -1,28 +1,31 @@
-"""Autotuner for the P2G tile: sorted particles per P2G block.
+"""Autotuner for the substep's launch knobs, per size bucket.
 
-The P2G scatter kernel gives each block a fixed range of particles in sorted
-(cell) order.  Small ranges let the hardware scheduler balance blocks whose
-cell structure differs; large ranges amortise the shared-tile set-up and flush
-over more particles.  The best range depends on how many particles share a
-sort block (particles per cell, scene size) and on the grid, so it is
-measured: ``tune(obj)`` times a few substeps of ``obj`` (an ``AnisoMPM`` or a
-``BatchedAnisoMPM``) with each candidate range, restores the state, sets
-``obj.p2g_range`` to the fastest and caches the choice per size bucket
-(log2 of particles per scene, grid size, number of scenes), so scenes of the
-same bucket reuse it.  ``save``/``load`` persist the cache as JSON.
+Two knobs shape the launches and never the results (the P2G grid sums are
+exact integers, the grid update is one thread per node row either way):
 
-The range changes only the float summation order inside P2G, never which
-contributions are summed.
+* ``p2g_ctas_per_sm``: resident CTAs per SM of the persistent P2G kernel,
+  which takes 4^3-cell sub-blocks from a work list.  More CTAs hide more
+  latency; fewer leave each CTA more L1/shared-memory bandwidth.
+* ``grid_ctas_per_sm``: CTAs per SM of the grid update over the active 4^3
+  node blocks (a grid-stride cap; 0 gives every 4-node row its own thread).
+
+``tune(obj)`` times a few substeps of ``obj`` (an ``AnisoMPM`` or a
+``BatchedAnisoMPM``) per candidate, one knob at a time (P2G first, then the
+grid update at the chosen P2G value), restores the state, sets the knobs to
+the fastest and caches the choice per size bucket (log2 of particles per
+scene, grid size, number of scenes), so scenes of the same bucket reuse it.
+``save``/``load`` persist the cache as JSON.
 """
 from __future__ import annotations
 
 import json
 import math
-from typing import Iterable, Optional
+from typing import Optional
 
 import torch
 
-CANDIDATES = (128, 256, 512, 1024, 2048)
+P2G_CANDIDATES = (0, 1, 2, 3)          # 0: as many as fit (3 at the kernel's register and shared-memory use)
+GRID_CANDIDATES = (0, 4, 8, 16, 32)    # 0: one thread per node row
 _CACHE: dict = {}
 
 
@@ -69,26 +72,33 @@ def _time_frame(obj, substeps: int, reps: int) -> float:
     return best
 
 
-def tune(obj, candidates: Iterable[int] = CANDIDATES, substeps: int = 4, reps: int = 2,
-         force: bool = False) -> int:
-    """Pick ``obj.p2g_range`` by timing; returns the chosen range."""
+def _apply(obj, knobs: dict):
+    obj.p2g_ctas_per_sm = int(knobs["p2g_ctas_per_sm"])
+    obj.grid_ctas_per_sm = int(knobs["grid_ctas_per_sm"])
+
+
+def tune(obj, substeps: int = 4, reps: int = 2, force: bool = False, p2g_candidates=P2G_CANDIDATES,
+         grid_candidates=GRID_CANDIDATES) -> dict:
+    """Pick the launch knobs of ``obj`` by timing; returns them as a dict."""
     key = bucket(obj)
     if not force and key in _CACHE:
-        obj.p2g_range = _CACHE[key]["range"]
-        return obj.p2g_range
+        _apply(obj, _CACHE[key]["knobs"])
+        return dict(_CACHE[key]["knobs"])
     saved = _mutable_state(obj)
-    times = {}
+    times = {"p2g_ctas_per_sm": {}, "grid_ctas_per_sm": {}}
+    knobs = {"p2g_ctas_per_sm": 0, "grid_ctas_per_sm": 0}
     try:
-        for r in candidates:
-            obj.p2g_range = int(r)
-            times[int(r)] = _time_frame(obj, substeps, reps)
-            _restore(obj, saved)
+        for name, cands in (("p2g_ctas_per_sm", p2g_candidates), ("grid_ctas_per_sm", grid_candidates)):
+            for c in cands:
+                _apply(obj, dict(knobs, **{name: int(c)}))
+                times[name][int(c)] = _time_frame(obj, substeps, reps)
+                _restore(obj, saved)
+            knobs[name] = min(times[name], key=times[name].get)
     finally:
         _restore(obj, saved)
-    best = min(times, key=times.get)
-    obj.p2g_range = best
-    _CACHE[key] = {"range": best, "ms": times}
-    return best
+    _apply(obj, knobs)
+    _CACHE[key] = {"knobs": dict(knobs), "ms": times, "substeps": substeps}
+    return dict(knobs)
 
 
 def cache() -> dict:
@@ -105,4 +115,5 @@ def load(path: str):
         data = json.load(f)
     for k, v in data.items():
         parts = k.split("|")
+        v["ms"] = {name: {int(c): t for c, t in d.items()} for name, d in v["ms"].items()}
         _CACHE[(parts[0], int(parts[1]), int(parts[2]), int(parts[3]))] = v

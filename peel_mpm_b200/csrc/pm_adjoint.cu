@@ -7,10 +7,16 @@
 // The forward substep t is first recorded (pm_substep_record) into a tape
 // slot: grid velocity and mass {v, m}, the normalised damage field gd, the
 // cubic weight sums, the active 4^3 block list and the step's clock.  The
-// adjoint then runs three kernels:
-//   k_adj_scatter   G2P adjoint as a scatter (particle order): the adjoint of
-//                   the grid velocity and damage field, accumulated with one
-//                   vector atomic per cubic-stencil node;
+// adjoint then runs four kernels:
+//   k_adj_pre       per particle (particle order): the G2P tail adjoint and
+//                   the G2P adjoint's scatter payload, written to the
+//                   particle's slot of the forward substep's recorded sort,
+//                   and the bounds that fix the fixed-point units;
+//   k_adj_tiles     G2P adjoint as a scatter over the recorded sub-block work
+//                   list (the forward P2G's cell-aggregated tiles): the adjoint
+//                   of the grid velocity and damage field in int64 fixed
+//                   point, so the sums do not depend on the atomics' order and
+//                   a backward pass is reproducible bit for bit;
 //   k_adj_grid      grid-update adjoint over the recorded active blocks
 //                   (normalisation by mass and by the cubic weight sum);
 //   k_adj_particle  P2G adjoint as a gather plus the constitutive adjoint
@@ -35,7 +41,14 @@ struct TapeHead {
     int any_allow;
     long long step;
     double time;
-    double pad;
+    unsigned n_work;    // non-empty sub-blocks of the substep's sort
+    unsigned pad;
+};
+
+// Control block of one adjoint substep: the bounds of the scatter's
+// contributions (float bits) and the dynamic work cursor.
+struct AdjCtrl {
+    unsigned mom_bound, lap_bound, work_next, pad;
 };
 
 // Quadratic weights with their derivatives wrt the local coordinate fx.
@@ -138,17 +151,17 @@ __device__ __forceinline__ void g2p_tail_adj(const pm_params &prm, const float x
     for (int k = 0; k < 9; ++k) Ct[k] = a.Cb[k] + dt * FbFt[k];
 }
 
-// ---------------------------------------------------------------- k_adj_scatter
-// Adjoint of v' = sum w v_i, C' = K sum w v_i dpos^T and lap' = sum L gd_i:
-// acc[i].xyz += w (vbar + K Cbar dpos), acc[i].w += L lapbar.  The quadratic
-// stencil is contained in the cubic one (per axis the quadratic node o_q is
-// the cubic node o_c = o_q + s with s = 1 when frac(X) >= 0.5, else 0), so
-// one float4 atomic per cubic node carries both.  Per axis the quadratic
-// weight, dpos and the K Cbar dpos column are tabulated over the 4 cubic
-// nodes (zero weight where the quadratic stencil does not reach), so a node
-// costs a few multiply-adds.
-__global__ void __launch_bounds__(256) k_adj_scatter(const pm_params prm, const Parts pre, const Parts post,
-                                                     const pm_state_adj ain, float4 *__restrict__ acc) {
+// ---------------------------------------------------------------- k_adj_pre
+// Adjoint of v' = sum w v_i, C' = K sum w v_i dpos^T and lap' = sum L gd_i has
+// the form of a P2G scatter: node i receives w (vt + K Ct dpos) and
+// lb (w''x wy wz + wx w''y wz + wx wy w''z) with lb = L lapbar.  This kernel
+// forms each particle's {fx | x, lb}, vt and K Ct (the momentum scatter's
+// {fx, mv, aff} slots) at its position in the forward substep's sort.
+constexpr int kAdjCW = 30;   // expanded cubic w and w'' per particle (5 per axis each)
+
+__global__ void __launch_bounds__(256) k_adj_pre(const pm_params prm, const Parts pre, const Parts post,
+                                                 const pm_state_adj ain, const int *__restrict__ iperm,
+                                                 float4 *__restrict__ pay, AdjCtrl *actl) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= pre.n) return;
     const long long ps = pre.ps;
@@ -169,16 +182,57 @@ __global__ void __launch_bounds__(256) k_adj_scatter(const pm_params prm, const 
     float vt[3], Ct[9];
     bool inside[3];
     g2p_tail_adj(prm, xp, vpost, F, a, vt, Ct, inside);
+    float kc[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) kc[k] = K * Ct[k];
+    const float lb = a.lapb * L2;
+    float fx[3];
+    bool reg = true;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const float X = __fmul_rn(xp[ax], inv_dx);
+        const float fb = floorf(__fsub_rn(X, 0.5f));
+        reg = reg && (fb >= 1.0f) && (fb <= (float)(ng - 4));
+        fx[ax] = __fsub_rn(X, fb);
+    }
+    float4 *dst = pay + 5 * (long long)iperm[p];
+    dst[0] = reg ? make_float4(fx[0], fx[1], fx[2], 0.0f) : make_float4(xp[0], xp[1], xp[2], 0.0f);
+    dst[1] = make_float4(vt[0], vt[1], vt[2], lb);
+    dst[2] = make_float4(kc[0], kc[1], kc[2], kc[3]);
+    dst[3] = make_float4(kc[4], kc[5], kc[6], kc[7]);
+    dst[4] = make_float4(kc[8], reg ? 1.0f : 0.0f, 0.0f, 0.0f);
+    // bounds of one node contribution: |w (vt + K Ct dpos)| with w <= 1,
+    // |dpos| <= 1.5 dx per axis (the cubic stencil's quadratic part), and
+    // |lb W''| with |w''x wy wz + wx w''y wz + wx wy w''z| <= 3 (|w''| <= 2, w <= 2/3)
+    const float hx = 1.5f * dx;
+    float bm = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        bm = fmaxf(bm, fabsf(vt[c]) + hx * (fabsf(kc[3 * c]) + fabsf(kc[3 * c + 1]) + fabsf(kc[3 * c + 2])));
+    unsigned bmom = bound_bits(bm), blap = bound_bits(3.0f * lb);
+    const unsigned am = __activemask();
+    bmom = __reduce_max_sync(am, bmom);
+    blap = __reduce_max_sync(am, blap);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1)) {
+        atomicMax(&actl->mom_bound, bmom);
+        atomicMax(&actl->lap_bound, blap);
+    }
+}
+
+// One particle whose stencil needs the reference's edge clamping, straight
+// into the global adjoint grid (4 int64 per node: momentum adjoint, damage
+// adjoint).
+__device__ __noinline__ void adj_scatter_global(const float xp[3], const float vt[3], const float kc[9], float lb,
+                                                float inv_dx, float dx, int ng, float smom, float slap,
+                                                long long *acc) {
     Quad q;
     quad_weights(xp, inv_dx, ng, q);
     Cubic c;
     cubic_weights(xp, inv_dx, ng, c);
-    // per axis, over the 4 cubic nodes: quadratic weight (0 outside the
-    // quadratic stencil) and K Cbar[:, axis] dpos_axis
     float wq[3][4], U[3][4][3];
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        const bool s1 = q.b[ax] != c.b[ax];   // quadratic base one node higher
+        const bool s1 = q.b[ax] != c.b[ax];   // quadratic base one node above the cubic one
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
             float w = 0.0f, oq = 0.0f;
@@ -190,12 +244,11 @@ __global__ void __launch_bounds__(256) k_adj_scatter(const pm_params prm, const 
             wq[ax][o] = w;
             const float dp = (oq - q.fx[ax]) * dx;
 #pragma unroll
-            for (int i = 0; i < 3; ++i) U[ax][o][i] = K * Ct[3 * i + ax] * dp;
+            for (int i = 0; i < 3; ++i) U[ax][o][i] = kc[3 * i + ax] * dp;
         }
     }
-    const float lb = a.lapb * L2;
 #pragma unroll
-    for (int ox = 0; ox < 4; ++ox) {
+    for (int ox = 0; ox < 4; ++ox)
 #pragma unroll
         for (int oy = 0; oy < 4; ++oy) {
             const float ab = lb * (c.w2[ox][0] * c.w[oy][1] + c.w[ox][0] * c.w2[oy][1]);
@@ -204,19 +257,254 @@ __global__ void __launch_bounds__(256) k_adj_scatter(const pm_params prm, const 
             const float b0 = vt[0] + U[0][ox][0] + U[1][oy][0];
             const float b1 = vt[1] + U[0][ox][1] + U[1][oy][1];
             const float b2 = vt[2] + U[0][ox][2] + U[1][oy][2];
-            const int row = (clampi(c.b[0] + ox, 0, ng - 1) * ng + clampi(c.b[1] + oy, 0, ng - 1)) * ng;
+            const long long row = ((long long)clampi(c.b[0] + ox, 0, ng - 1) * ng + clampi(c.b[1] + oy, 0, ng - 1)) * ng;
 #pragma unroll
             for (int oz = 0; oz < 4; ++oz) {
                 const float wk = wxy * wq[2][oz];
-                float4 val;
-                val.x = wk * (b0 + U[2][oz][0]);
-                val.y = wk * (b1 + U[2][oz][1]);
-                val.z = wk * (b2 + U[2][oz][2]);
-                val.w = ab * c.w[oz][2] + e * c.w2[oz][2];
-                // atomics are the cost here: skip the nodes this particle adds nothing to
-                // (outside its quadratic stencil when its lap adjoint is zero)
-                if (val.x != 0.0f || val.y != 0.0f || val.z != 0.0f || val.w != 0.0f)
-                    atomicAdd(&acc[row + clampi(c.b[2] + oz, 0, ng - 1)], val);
+                long long *g = acc + 4 * (row + clampi(c.b[2] + oz, 0, ng - 1));
+                tile_add(g, wk * (b0 + U[2][oz][0]), smom);
+                tile_add(g + 1, wk * (b1 + U[2][oz][1]), smom);
+                tile_add(g + 2, wk * (b2 + U[2][oz][2]), smom);
+                tile_add(g + 3, ab * c.w[oz][2] + e * c.w2[oz][2], slap);
+            }
+        }
+}
+
+// ---------------------------------------------------------------- k_adj_tiles
+// The G2P adjoint scatter over the forward substep's non-empty 4^3-cell
+// sub-blocks, with the forward P2G's cell-aggregated (cell, x-slab) items:
+// quadratic slabs sum w (vt + K Ct dpos) into the momentum-adjoint tile
+// (nodes [4s, 4s+6)^3), cubic slabs sum lb W'' into the damage-adjoint tile
+// (nodes [4s-1, 4s+7)^3), both int64 fixed point, flushed with one atomic per
+// touched node and component.  The adjoint touches exactly the nodes the
+// forward P2G touched, so no block marks are needed.
+constexpr int kATh = 256;
+constexpr int kAPayStride = kATh + kATh / 32;
+constexpr int kASub = 4, kAQE = 6, kACE = 8, kAQN = 216, kACN = 512;
+constexpr size_t kAdjTileSmem = sizeof(long long) * (3 * kAQN + kACN) + sizeof(float) * (17 + kAdjCW) * kAPayStride +
+                                sizeof(int) * (kATh + 2) + 2 * kATh;
+
+__global__ void __launch_bounds__(kATh, 2) k_adj_tiles(const pm_params prm, const unsigned *__restrict__ keys,
+                                                       const int *__restrict__ work, const TapeHead *head,
+                                                       const float4 *__restrict__ pay, AdjCtrl *actl,
+                                                       long long *__restrict__ acc, long long n) {
+    extern __shared__ long long s_adj[];
+    long long *qt = s_adj;                                                 // [3][kAQN]
+    long long *ct = qt + 3 * kAQN;                                         // [kACN]
+    float (*sp)[kAPayStride] = (float (*)[kAPayStride])(ct + kACN);      // [17][kAPayStride]
+    float (*cw)[kAPayStride] = (float (*)[kAPayStride])(sp[17]);        // [kAdjCW][kAPayStride]
+    int *runs = (int *)(cw[kAdjCW]);                                      // [kATh + 2]
+    unsigned char *regular = (unsigned char *)(runs + kATh + 2);          // [kATh]
+    unsigned char *lcell = regular + kATh;                                // [kATh]
+    __shared__ int s_wcnt[kATh / 32];
+    __shared__ unsigned s_item;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const unsigned n_work = min(head->n_work, (unsigned)min(n, (long long)0x7fffffff));
+    const int ng = prm.n_grid;
+    const int nb = sort_blocks_per_axis(ng);
+    const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
+    const float smom = fix_scale(actl->mom_bound).scale, slap = fix_scale(actl->lap_bound).scale;
+    for (int i = tid; i < 3 * kAQN + kACN; i += kATh) qt[i] = 0;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(&actl->work_next, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= n_work) break;
+        const long long a = work[item];
+        const unsigned key0 = keys[a];
+        const unsigned sbk = key0 >> 6;
+        const unsigned blk = key0 >> kSortBlockBits;
+        const int bz = (int)(blk % nb), by = (int)((blk / nb) % nb), bx = (int)(blk / ((unsigned)nb * nb));
+        const unsigned oct = (key0 >> 6) & 7u;
+        const int org[3] = {bx * kSortBlock + (int)((oct >> 2) & 1u) * kASub,
+                            by * kSortBlock + (int)((oct >> 1) & 1u) * kASub,
+                            bz * kSortBlock + (int)(oct & 1u) * kASub};
+        for (long long sub = a;; sub += kATh) {
+            const long long i = sub + tid;
+            const unsigned key = i < n ? keys[i] : 0xffffffffu;
+            const bool valid = i < n && (key >> 6) == sbk;
+            if (valid) {
+                const float4 *src = pay + 5 * i;
+                const float4 q0 = src[0], q1 = src[1], q2 = src[2], q3 = src[3], q4 = src[4];
+                const int t = tid + (tid >> 5);
+                sp[0][t] = q0.x; sp[1][t] = q0.y; sp[2][t] = q0.z;
+                sp[3][t] = q1.x; sp[4][t] = q1.y; sp[5][t] = q1.z; sp[16][t] = q1.w;
+                sp[6][t] = q2.x; sp[7][t] = q2.y; sp[8][t] = q2.z; sp[9][t] = q2.w;
+                sp[10][t] = q3.x; sp[11][t] = q3.y; sp[12][t] = q3.z; sp[13][t] = q3.w;
+                sp[14][t] = q4.x;
+                regular[tid] = q4.y != 0.0f ? 1 : 0;
+                lcell[tid] = (unsigned char)(key & 63u);
+                if (q4.y != 0.0f) {
+                    float e[5];
+                    cw5(q0.x, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cw[k][t] = e[k];
+                    cw5(q0.y, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cw[5 + k][t] = e[k];
+                    cw5(q0.z, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cw[10 + k][t] = e[k];
+                    cw5_2(q0.x, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cw[15 + k][t] = e[k];
+                    cw5_2(q0.y, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cw[20 + k][t] = e[k];
+                    cw5_2(q0.z, e);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) cw[25 + k][t] = e[k];
+                }
+            }
+            int nruns, cnt;
+            {
+                const unsigned prev = (tid > 0 && i <= n) ? keys[i - 1] : 0xffffffffu;
+                const bool flag = valid && (tid == 0 || key != prev);
+                const unsigned fb = __ballot_sync(0xffffffffu, flag), vb = __ballot_sync(0xffffffffu, valid);
+                if (lane == 0) s_wcnt[wid] = (int)(__popc(fb) | (__popc(vb) << 16));
+                __syncthreads();
+                int pos = __popc(fb & lanemask_lt()), tot = 0, vt = 0;
+#pragma unroll
+                for (int w2 = 0; w2 < kATh / 32; ++w2) {
+                    const int c = s_wcnt[w2];
+                    pos += (w2 < wid) ? (c & 0xffff) : 0;
+                    tot += c & 0xffff;
+                    vt += c >> 16;
+                }
+                if (flag) runs[pos] = tid;
+                if (tid == 0) runs[tot] = vt;
+                nruns = tot;
+                cnt = vt;
+                __syncthreads();
+            }
+            if (valid && !regular[tid]) {
+                const int t = tid + (tid >> 5);
+                const float xp[3] = {sp[0][t], sp[1][t], sp[2][t]};
+                const float vt[3] = {sp[3][t], sp[4][t], sp[5][t]};
+                float kc[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) kc[k] = sp[6 + k][t];
+                adj_scatter_global(xp, vt, kc, sp[16][t], inv_dx, dx, ng, smom, slap, acc);
+            }
+            for (int it = tid; it < nruns * 8; it += kATh) {
+                const bool quad = it < 3 * nruns;
+                const int r = quad ? it / 3 : (it - 3 * nruns) / 5;
+                const int sl = quad ? it - 3 * r : 3 + (it - 3 * nruns - 5 * r);
+                const int ja = runs[r], jb = runs[r + 1];
+                int cq[3];
+                morton_decode(lcell[ja], cq);
+                if (sl < 3) {
+                    const int ox = sl;
+                    float acc3[3][3][3];
+#pragma unroll
+                    for (int i2 = 0; i2 < 3; ++i2)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) acc3[i2][j][c] = 0.0f;
+                    for (int j = ja; j < jb; ++j) {
+                        if (!regular[j]) continue;
+                        const int t = j + (j >> 5);
+                        const float fx0 = sp[0][t], fx1 = sp[1][t], fx2 = sp[2][t];
+                        float wx[3], wy[3], wz[3];
+                        qw(fx0, wx); qw(fx1, wy); qw(fx2, wz);
+                        const float dxo = ((float)ox - fx0) * dx;
+                        float base[3], ay[3], az[3];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            base[c] = sp[3 + c][t] + sp[6 + 3 * c][t] * dxo;
+                            ay[c] = sp[7 + 3 * c][t];
+                            az[c] = sp[8 + 3 * c][t];
+                        }
+                        const float wxs = ox == 0 ? wx[0] : (ox == 1 ? wx[1] : wx[2]);
+                        float bz3[3][3];
+#pragma unroll
+                        for (int oz = 0; oz < 3; ++oz) {
+                            const float dz = ((float)oz - fx2) * dx;
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) bz3[oz][c] = base[c] + az[c] * dz;
+                        }
+#pragma unroll
+                        for (int oy = 0; oy < 3; ++oy) {
+                            const float dy = ((float)oy - fx1) * dx;
+                            const float wxy = wxs * wy[oy];
+                            const float ady[3] = {ay[0] * dy, ay[1] * dy, ay[2] * dy};
+#pragma unroll
+                            for (int oz = 0; oz < 3; ++oz) {
+                                const float wk = wxy * wz[oz];
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) acc3[oy][oz][c] += wk * (bz3[oz][c] + ady[c]);
+                            }
+                        }
+                    }
+                    const int nx = cq[0] + ox;
+#pragma unroll
+                    for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                        for (int oz = 0; oz < 3; ++oz) {
+                            const int idx = (nx * kAQE + cq[1] + oy) * kAQE + cq[2] + oz;
+                            tile_add(&qt[idx], acc3[oy][oz][0], smom);
+                            tile_add(&qt[kAQN + idx], acc3[oy][oz][1], smom);
+                            tile_add(&qt[2 * kAQN + idx], acc3[oy][oz][2], smom);
+                        }
+                } else {
+                    const int nxs = sl - 3;
+                    float al[5][5];
+#pragma unroll
+                    for (int i2 = 0; i2 < 5; ++i2)
+#pragma unroll
+                        for (int j = 0; j < 5; ++j) al[i2][j] = 0.0f;
+                    for (int j = ja; j < jb; ++j) {
+                        if (!regular[j]) continue;
+                        const int t = j + (j >> 5);
+                        const float lb = sp[16][t];
+                        const float ax = lb * cw[15 + nxs][t], bx2 = lb * cw[nxs][t];   // lb w''x, lb wx
+                        float ez[5], e2z[5];
+#pragma unroll
+                        for (int k = 0; k < 5; ++k) {
+                            ez[k] = cw[10 + k][t];
+                            e2z[k] = cw[25 + k][t];
+                        }
+#pragma unroll
+                        for (int ny = 0; ny < 5; ++ny) {
+                            const float wy = cw[5 + ny][t], w2y = cw[20 + ny][t];
+                            const float t1 = ax * wy + bx2 * w2y;   // (w''x wy + wx w''y) lb
+                            const float t2 = bx2 * wy;              // wx wy lb
+#pragma unroll
+                            for (int nz = 0; nz < 5; ++nz) al[ny][nz] += t1 * ez[nz] + t2 * e2z[nz];
+                        }
+                    }
+                    const int nx = cq[0] + nxs;
+#pragma unroll
+                    for (int ny = 0; ny < 5; ++ny)
+#pragma unroll
+                        for (int nz = 0; nz < 5; ++nz)
+                            tile_add(&ct[(nx * kACE + cq[1] + ny) * kACE + cq[2] + nz], al[ny][nz], slap);
+                }
+            }
+            __syncthreads();
+            if (cnt < kATh) break;
+        }
+        for (int li = tid; li < kAQN; li += kATh) {
+            const long long q0 = qt[li], q1 = qt[kAQN + li], q2 = qt[2 * kAQN + li];
+            if ((q0 | q1 | q2) != 0) {
+                qt[li] = 0; qt[kAQN + li] = 0; qt[2 * kAQN + li] = 0;
+                const int tx = li / (kAQE * kAQE), ty = (li / kAQE) % kAQE, tz = li % kAQE;
+                long long *g = acc + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
+                if (q0) atomicAdd((unsigned long long *)g, (unsigned long long)q0);
+                if (q1) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q1);
+                if (q2) atomicAdd((unsigned long long *)(g + 2), (unsigned long long)q2);
+            }
+        }
+        for (int li = tid; li < kACN; li += kATh) {
+            const long long q3 = ct[li];
+            if (q3 != 0) {
+                ct[li] = 0;
+                const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
+                long long *g = acc + 4 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
+                                          (org[2] - 1 + tz));
+                atomicAdd((unsigned long long *)(g + 3), (unsigned long long)q3);
             }
         }
     }
@@ -230,8 +518,10 @@ __global__ void __launch_bounds__(256) k_adj_scatter(const pm_params prm, const 
 __global__ void __launch_bounds__(256) k_adj_grid(const pm_params prm, const int *__restrict__ blocks,
                                                   const TapeHead *head, const float4 *__restrict__ gvel,
                                                   const float *__restrict__ ggd, const float *__restrict__ gsw,
-                                                  float4 *__restrict__ acc, float4 *__restrict__ A,
-                                                  float4 *__restrict__ B, long long n_blocks) {
+                                                  long long *__restrict__ acc, const AdjCtrl *actl,
+                                                  float4 *__restrict__ A, float4 *__restrict__ B,
+                                                  long long n_blocks) {
+    const float umom = fix_scale(actl->mom_bound).unit, ulap = fix_scale(actl->lap_bound).unit;
     const long long nact = min((long long)head->n_active, n_blocks);
     const long long items = nact * 64;
     const int ng = prm.n_grid, nbs = (ng + kBlockEdge - 1) / kBlockEdge;
@@ -246,8 +536,12 @@ __global__ void __launch_bounds__(256) k_adj_grid(const pm_params prm, const int
         const int ix = bx * kBlockEdge + (l >> 4), iy = by * kBlockEdge + ((l >> 2) & 3), iz = bz * kBlockEdge + (l & 3);
         if (ix >= ng || iy >= ng || iz >= ng) continue;
         const long long node = ((long long)ix * ng + iy) * ng + iz;
-        const float4 ab = acc[node];
-        acc[node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        longlong2 *an = (longlong2 *)(acc + 4 * node);
+        const longlong2 a01 = an[0], a23 = an[1];
+        an[0] = make_longlong2(0, 0);
+        an[1] = make_longlong2(0, 0);
+        const float4 ab = make_float4(from_fix(a01.x, umom), from_fix(a01.y, umom), from_fix(a23.x, umom),
+                                      from_fix(a23.y, ulap));
         const float4 gv = gvel[node];
         float4 ao = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (gv.w > 1e-12f) {
@@ -292,8 +586,9 @@ __device__ __forceinline__ void damage_geom(const float R[9], const float V[9], 
                                             DamageGeom &g) {
     const long long ps = P.ps;
     float sg[9];
+    const float rJ = 1.0f / J;   // as the forward computes it
 #pragma unroll
-    for (int k = 0; k < 9; ++k) sg[k] = (tdev[k] + ((k % 4 == 0) ? tv : 0.0f)) / J;
+    for (int k = 0; k < 9; ++k) sg[k] = (tdev[k] + ((k % 4 == 0) ? tv : 0.0f)) * rJ;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -897,16 +1192,29 @@ __global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, co
     }
 }
 
-__global__ void k_tape_head(const Ctrl *ctrl, TapeHead *head) {
+__global__ void k_tape_head(const Ctrl *ctrl, TapeHead *head, long long n) {
     if (threadIdx.x == 0) {
         head->n_active = ctrl->n_active;
         head->any_allow = ctrl->any_allow;
         head->step = ctrl->step;
         head->time = ctrl->time;
+        head->n_work = (unsigned)min((long long)ctrl->n_work, n);
     }
 }
 
 }  // namespace
+
+// One-time kernel attribute set-up for the current device (not a stream
+// operation; pm_prepare runs it before any capture).
+void prepare_adjoint() {
+    static int done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaFuncSetAttribute(k_adj_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdjTileSmem);
+        done[dev] = 1;
+    }
+}
 
 // ------------------------------------------------------------------ tape layout
 TapeLayout make_tape_layout(long long n, int ng, int slots) {
@@ -918,15 +1226,20 @@ TapeLayout make_tape_layout(long long n, int ng, int slots) {
     const long long np = (n + 63) / 64 * 64 > 0 ? (n + 63) / 64 * 64 : 64;
     size_t o = 0;
     T.head = o;    o = align_up(o + sizeof(TapeHead) * (size_t)(slots > 0 ? slots : 1), A);
-    T.acc = o;     o = align_up(o + 16 * (size_t)G, A);
+    T.actl = o;    o = align_up(o + sizeof(AdjCtrl), A);
+    T.acc = o;     o = align_up(o + 32 * (size_t)G, A);     // 4 x int64 per node
     T.adj_q = o;   o = align_up(o + 16 * (size_t)G, A);
     T.adj_c = o;   o = align_up(o + 16 * (size_t)G, A);
+    T.apay = o;    o = align_up(o + 80 * (size_t)np, A);
     T.slot0 = o;
     size_t s = 0;
     T.vel = s;     s = align_up(s + 16 * (size_t)G, A);
     T.gd = s;      s = align_up(s + 4 * (size_t)G, A);
     T.sw = s;      s = align_up(s + 4 * (size_t)G, A);
     T.blocks = s;  s = align_up(s + 4 * (size_t)nb, A);
+    T.keys = s;    s = align_up(s + 4 * (size_t)np, A);
+    T.iperm = s;   s = align_up(s + 4 * (size_t)np, A);
+    T.work = s;    s = align_up(s + 4 * (size_t)np, A);
     T.aff = s;     s = align_up(s + 36 * (size_t)np, A);
     T.pol = s;     s = align_up(s + 88 * (size_t)np, A);
     T.aff_stride = np;
@@ -943,14 +1256,20 @@ void record_redirect(const TapeLayout &T, void *tape, int slot, WS &w) {
     w.g_gd = (float *)(b + T.gd);
     w.g_sw = (float *)(b + T.sw);
     w.block_list = (int *)(b + T.blocks);
+    w.inv_perm = (int *)(b + T.iperm);   // the substep's sort stays on the tape for the adjoint
+    w.work = (int *)(b + T.work);
     w.tape_aff = (float *)(b + T.aff);
     w.tape_pol = (float *)(b + T.pol);
     w.tape_aff_stride = T.aff_stride;
 }
 
-void launch_tape_head(const TapeLayout &T, void *tape, int slot, const WS &w, cudaStream_t s) {
+void launch_tape_head(const TapeLayout &T, void *tape, int slot, const WS &w, long long n, cudaStream_t s) {
     TapeHead *h = (TapeHead *)((char *)tape + T.head) + slot;
-    k_tape_head<<<1, 32, 0, s>>>(w.ctrl, h);
+    k_tape_head<<<1, 32, 0, s>>>(w.ctrl, h, n);
+    if (n > 0) {
+        char *b = (char *)tape + T.slot0 + T.slot_bytes * (size_t)slot;
+        cudaMemcpyAsync(b + T.keys, w.sorted_keys, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    }
 }
 
 void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, const pm_state_adj &ain,
@@ -959,7 +1278,9 @@ void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, c
     char *base = (char *)tape;
     char *b = base + T.slot0 + T.slot_bytes * (size_t)slot;
     const TapeHead *h = (const TapeHead *)(base + T.head) + slot;
-    float4 *acc = (float4 *)(base + T.acc);
+    AdjCtrl *actl = (AdjCtrl *)(base + T.actl);
+    long long *acc = (long long *)(base + T.acc);
+    float4 *apay = (float4 *)(base + T.apay);
     float4 *Aq = (float4 *)(base + T.adj_q);
     float4 *Bc = (float4 *)(base + T.adj_c);
     const float4 *gvel = (const float4 *)(b + T.vel);
@@ -968,10 +1289,25 @@ void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, c
     const int *blocks = (const int *)(b + T.blocks);
     const long long n = pre.n;
     if (n <= 0) return;
-    k_adj_scatter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prm, pre, post, ain, acc);
+    prepare_adjoint();
+    cudaMemsetAsync(actl, 0, sizeof(AdjCtrl), s);
+    k_adj_pre<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prm, pre, post, ain, (const int *)(b + T.iperm), apay, actl);
+    {
+        static int slots_dev[64] = {0};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int slots = (dev >= 0 && dev < 64) ? slots_dev[dev] : 0;
+        if (slots <= 0) {
+            slots = resident_slots((const void *)k_adj_tiles, kATh, kAdjTileSmem);
+            if (dev >= 0 && dev < 64) slots_dev[dev] = slots;
+        }
+        const long long blocks_t = std::max<long long>(1, std::min<long long>(slots, (n + 63) / 64));
+        k_adj_tiles<<<(unsigned)blocks_t, kATh, kAdjTileSmem, s>>>(prm, (const unsigned *)(b + T.keys),
+                                                                  (const int *)(b + T.work), h, apay, actl, acc, n);
+    }
     const long long max_items = T.n_blocks * 64;
     const int gb = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, 148LL * 8));
-    k_adj_grid<<<gb, 256, 0, s>>>(prm, blocks, h, gvel, ggd, gsw, acc, Aq, Bc, T.n_blocks);
+    k_adj_grid<<<gb, 256, 0, s>>>(prm, blocks, h, gvel, ggd, gsw, acc, actl, Aq, Bc, T.n_blocks);
     const float *taff = (const float *)(b + T.aff);
     const float *tpol = (const float *)(b + T.pol);
     k_adj_particle<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(prm, pre, post, ain, aout, grads, h, gvel, Aq, Bc,

@@ -111,15 +111,15 @@ pm::BatchScenes scenes_of(void *ws, const BatchPlan &bp) {
 std::mutex g_mu;
 struct WsRecord {
     uint64_t sig;
-    int p2g_range;   // from the stored parameters of scene 0
+    int p2g_ctas, grid_ctas;   // launch knobs, from the stored parameters of scene 0
 };
 std::unordered_map<uintptr_t, WsRecord> g_sig;
 
-// P2G range recorded for this workspace (0 when none).
-int recorded_range(const void *ws) {
+// Launch knobs recorded for this workspace (0 when none).
+WsRecord recorded_knobs(const void *ws) {
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_sig.find((uintptr_t)ws);
-    return it == g_sig.end() ? 0 : it->second.p2g_range;
+    return it == g_sig.end() ? WsRecord{0, 0, 0} : it->second;
 }
 
 
@@ -190,7 +190,7 @@ int pm_batch_workspace_layout(int32_t n_scenes, const int64_t *n, const int32_t 
     w.ctrl = L.ctrl; w.keys_a = L.keys_a; w.keys_b = L.keys_b; w.vals_a = L.vals_a; w.vals_b = L.vals_b;
     w.hist = L.hist; w.block_mask = L.block_mask; w.block_list = L.block_list; w.g_mom = L.g_mom;
     w.g_dmg = L.g_dmg; w.g_vel = L.g_vel; w.g_gd = L.g_gd; w.payload = L.payload; w.inv_perm = L.inv_perm;
-    w.total = L.total; w.sort_passes = L.passes; w.n_tiles = L.n_tiles;
+    w.work = L.work; w.total = L.total; w.sort_passes = L.passes; w.n_tiles = L.n_tiles;
     out->params = bp.off_prms;
     out->tables = bp.off_pb;
     out->n_total = bp.n_total;
@@ -213,7 +213,7 @@ int pm_batch_workspace_init(void *ws, size_t ws_bytes, int32_t n_scenes, const i
     if ((rc = upload_tables(ws, bp, prms, s))) return rc;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        g_sig[(uintptr_t)ws] = WsRecord{bp.sig, prms[0].p2g_range};
+        g_sig[(uintptr_t)ws] = WsRecord{bp.sig, prms[0].p2g_ctas_per_sm, prms[0].grid_ctas_per_sm};
     }
     return pm::api_cuda_check("pm_batch_workspace_init");
 }
@@ -233,7 +233,8 @@ int pm_batch_set_params(void *ws, size_t ws_bytes, int32_t n_scenes, const int64
         return pm::api_cuda_check("pm_batch_set_params");
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        g_sig[(uintptr_t)ws].p2g_range = prms[0].p2g_range;
+        g_sig[(uintptr_t)ws].p2g_ctas = prms[0].p2g_ctas_per_sm;
+        g_sig[(uintptr_t)ws].grid_ctas = prms[0].grid_ctas_per_sm;
     }
     return PM_OK;
 }
@@ -255,9 +256,10 @@ int pm_batch_substep(int32_t n_scenes, const int64_t *n, const int32_t *n_grid, 
     if (bp.n_total > 0) {
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, bp.n_total, s, w.inv_perm, true);
-        pm::launch_p2g(sc, parts, w, s, recorded_range(ws));
+        const WsRecord knobs = recorded_knobs(ws);
+        pm::launch_p2g(sc, parts, w, s, knobs.p2g_ctas);
         pm::launch_compact(w, s);
-        pm::launch_grid(sc, w, s);
+        pm::launch_grid(sc, w, s, knobs.grid_ctas);
         pm::launch_g2p(sc, parts, w, s, bp.n_ctas);
     }
     return pm::api_cuda_check("pm_batch_substep");

@@ -44,8 +44,9 @@ int check_params(const pm_params *prm) {
     if (prm->damage_every < 1) return fail(PM_ERR_ARG, "damage_every must be >= 1");
     if (prm->n_grips < 0 || prm->n_grips > PM_MAX_GRIPS) return fail(PM_ERR_ARG, "too many grips");
     if (prm->n_colliders < 0 || prm->n_colliders > PM_MAX_COLLIDERS) return fail(PM_ERR_ARG, "too many colliders");
-    if (prm->p2g_range != 0 && (prm->p2g_range < 64 || prm->p2g_range > 4096))
-        return fail(PM_ERR_ARG, "p2g_range must be 0 or in [64, 4096]");
+    if (prm->p2g_ctas_per_sm < 0 || prm->p2g_ctas_per_sm > 8) return fail(PM_ERR_ARG, "p2g_ctas_per_sm must be in [0, 8]");
+    if (prm->grid_ctas_per_sm < 0 || prm->grid_ctas_per_sm > 64)
+        return fail(PM_ERR_ARG, "grid_ctas_per_sm must be in [0, 64]");
     if (!(prm->dx > 0.0) || !(prm->inv_dx > 0.0)) return fail(PM_ERR_ARG, "dx must be positive");
     return PM_OK;
 }
@@ -113,6 +114,7 @@ int pm_prepare(void) {
     if (rc) return rc;
     pm::prepare_p2g();
     pm::prepare_sort();
+    pm::prepare_adjoint();
     return cuda_check("pm_prepare");
 }
 
@@ -130,10 +132,20 @@ int pm_workspace_layout(int64_t n, int32_t n_grid, pm_ws_layout *out) {
     out->ctrl = L.ctrl; out->keys_a = L.keys_a; out->keys_b = L.keys_b; out->vals_a = L.vals_a;
     out->vals_b = L.vals_b; out->hist = L.hist; out->block_mask = L.block_mask; out->block_list = L.block_list;
     out->g_mom = L.g_mom; out->g_dmg = L.g_dmg; out->g_vel = L.g_vel; out->g_gd = L.g_gd;
-    out->payload = L.payload; out->inv_perm = L.inv_perm; out->total = L.total;
+    out->payload = L.payload; out->inv_perm = L.inv_perm; out->work = L.work; out->total = L.total;
     out->sort_passes = L.passes;
     out->n_tiles = L.n_tiles;
     return PM_OK;
+}
+
+int pm_grid_sums(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, float *mom, float *dmg, void *stream) {
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (!mom || !dmg) return fail(PM_ERR_ARG, "mom or dmg is NULL");
+    pm::WS w;
+    if ((rc = get_ws(const_cast<void *>(ws), ws_bytes, n, n_grid, &w))) return rc;
+    pm::launch_grid_sums(w, (long long)n_grid * n_grid * n_grid, mom, dmg, (cudaStream_t)stream);
+    return cuda_check("pm_grid_sums");
 }
 
 int pm_workspace_init(void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, void *stream) {
@@ -173,7 +185,7 @@ int pm_p2g(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
-    pm::launch_p2g(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream, prm->p2g_range);
+    pm::launch_p2g(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream, prm->p2g_ctas_per_sm);
     pm::launch_compact(w, (cudaStream_t)stream);
     return cuda_check("pm_p2g");
 }
@@ -183,7 +195,7 @@ int pm_grid_update(const pm_params *prm, void *ws, size_t ws_bytes, int64_t n, v
     if ((rc = check_device()) || (rc = check_params(prm))) return rc;
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, n, prm->n_grid, &w))) return rc;
-    pm::launch_grid(pm::PlainScenes{*prm}, w, (cudaStream_t)stream);
+    pm::launch_grid(pm::PlainScenes{*prm}, w, (cudaStream_t)stream, prm->grid_ctas_per_sm);
     return cuda_check("pm_grid_update");
 }
 
@@ -212,9 +224,9 @@ static int substep_common(const pm_params *prm, const pm_particles *P, void *ws,
         const pm::PlainScenes sc{*prm};
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, P->n, s, w.inv_perm, true);
-        pm::launch_p2g(sc, parts, w, s, prm->p2g_range);
+        pm::launch_p2g(sc, parts, w, s, prm->p2g_ctas_per_sm);
         pm::launch_compact(w, s);
-        pm::launch_grid(sc, w, s);
+        pm::launch_grid(sc, w, s, prm->grid_ctas_per_sm);
         pm::launch_g2p(sc, parts, w, s);
     }
     return cuda_check("pm_substep");
@@ -284,12 +296,12 @@ int pm_substep_record(const pm_params *prm, const pm_particles *P, void *ws, siz
         const pm::PlainScenes sc{*prm};
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, P->n, s, w.inv_perm, true);
-        pm::launch_p2g(sc, parts, w, s, prm->p2g_range);
+        pm::launch_p2g(sc, parts, w, s, prm->p2g_ctas_per_sm);
         pm::launch_compact(w, s);
-        pm::launch_grid(sc, w, s);
+        pm::launch_grid(sc, w, s, prm->grid_ctas_per_sm);
         pm::launch_g2p(sc, parts, w, s);
     }
-    pm::launch_tape_head(T, tape, slot, w, s);
+    pm::launch_tape_head(T, tape, slot, w, P->n, s);
     return cuda_check("pm_substep_record");
 }
 
@@ -395,9 +407,16 @@ int pm_sym_eig(const float *A, int64_t n, int32_t sweeps, float *evals, float *e
     if ((rc = check_device())) return rc;
     if (n < 0) return fail(PM_ERR_ARG, "n < 0");
     if (n > 0 && (!A || !evals || !evecs)) return fail(PM_ERR_ARG, "NULL array");
-    if (sweeps < 1) return fail(PM_ERR_ARG, "sweeps must be >= 1");
+    if (sweeps < 0) return fail(PM_ERR_ARG, "sweeps must be >= 0");
     pm::launch_sym_eig(A, n, sweeps, evals, evecs, (cudaStream_t)stream);
     return cuda_check("pm_sym_eig");
+}
+
+int pm_bin_workspace_size(int64_t n, int32_t n_grid, size_t *bytes) {
+    if (!bytes) return fail(PM_ERR_ARG, "bytes is NULL");
+    if (n < 0 || n_grid < 4 || n_grid > 1024) return fail(PM_ERR_ARG, "bad n or n_grid");
+    *bytes = pm::make_layout(n, n_grid).block_mask;   // control block, keys, ids and histograms come first
+    return PM_OK;
 }
 
 int pm_bin_sort(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid, double inv_dx, uint32_t *keys_out,
@@ -407,8 +426,11 @@ int pm_bin_sort(const float *x, int64_t n, int64_t plane_stride, int32_t n_grid,
     if (n < 0 || plane_stride < n || n_grid < 4 || n_grid > 1024 || !(inv_dx > 0.0))
         return fail(PM_ERR_ARG, "bad size argument");
     if (n > 0 && (!x || !keys_out || !perm_out)) return fail(PM_ERR_ARG, "NULL array");
-    pm::WS w;
-    if ((rc = get_ws(ws, ws_bytes, n, n_grid, &w))) return rc;
+    if (!ws) return fail(PM_ERR_WORKSPACE, "workspace is NULL");
+    if (((uintptr_t)ws & 255) != 0) return fail(PM_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    const pm::Layout L = pm::make_layout(n, n_grid);
+    if (ws_bytes < L.block_mask) return fail(PM_ERR_WORKSPACE, "workspace smaller than pm_bin_workspace_size");
+    const pm::WS w = pm::make_ws(ws, L);   // only the sort buffers are touched
     if (n == 0) return PM_OK;
     cudaStream_t s = (cudaStream_t)stream;
     pm::launch_keys_only(x, n, plane_stride, n_grid, (float)inv_dx, false, w, s);

@@ -32,7 +32,14 @@ __host__ __device__ inline int radix_passes(int key_bits) {
 }
 constexpr int kG2PThreads = 256;     // G2P particles per CTA
 
-// Device control block: per-substep inputs and status counters.
+// Device control block: per-substep inputs and status counters.  The three
+// bounds are float bit patterns (non-negative floats order like their bits)
+// raised with atomicMax by the constitutive kernel: the largest magnitude of a
+// particle's momentum contribution to one node, of a particle mass and of a
+// particle damage; they fix the units of the grid's fixed-point accumulators
+// for the substep (see fix_scale).  n_work / work_next: the P2G work list of
+// non-empty 4^3-cell sub-blocks and its dynamic cursor (control block 0 of a
+// batch serves all scenes).
 struct Ctrl {
     double time;
     long long step;
@@ -40,6 +47,9 @@ struct Ctrl {
     unsigned n_active;
     unsigned nonfinite;
     unsigned tile_fallbacks;
+    unsigned mom_bound, mass_bound, dmg_bound;
+    unsigned n_work, work_next;
+    unsigned pad_;
     float col_origin[PM_MAX_COLLIDERS][3];
     float col_vel[PM_MAX_COLLIDERS][3];
 };
@@ -64,7 +74,7 @@ __host__ __device__ inline int blocked_key_bits(int ng) {
 
 struct Layout {
     size_t ctrl, keys_a, keys_b, vals_a, vals_b, hist, block_mask, block_list;
-    size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, tables, total;
+    size_t g_mom, g_dmg, g_vel, g_gd, payload, inv_perm, work, tables, total;
     int passes, key_bits, n_tiles, nbs;
     long long n_blocks, n_nodes;
 };
@@ -92,12 +102,13 @@ __host__ __device__ inline Layout make_layout_sized(long long n, long long n_nod
     L.hist = o;       o = align_up(o + 4 * ((size_t)kRadixTop * L.n_tiles + kRadixTop), A);
     L.block_mask = o; o = align_up(o + (size_t)L.n_blocks, A);
     L.block_list = o; o = align_up(o + 4 * (size_t)L.n_blocks, A);
-    L.g_mom = o;      o = align_up(o + 16 * (size_t)L.n_nodes, A);
-    L.g_dmg = o;      o = align_up(o + 8 * (size_t)L.n_nodes, A);
+    L.g_mom = o;      o = align_up(o + 32 * (size_t)L.n_nodes, A);   // 4 x int64 fixed point per node
+    L.g_dmg = o;      o = align_up(o + 16 * (size_t)L.n_nodes, A);   // 2 x int64 fixed point per node
     L.g_vel = o;      o = align_up(o + 16 * (size_t)L.n_nodes, A);
     L.g_gd = o;       o = align_up(o + 4 * (size_t)L.n_nodes, A);
     L.payload = o;    o = align_up(o + 80 * nn, A);
     L.inv_perm = o;   o = align_up(o + 4 * nn, A);
+    L.work = o;       o = align_up(o + 4 * nn, A);                    // starts of the non-empty sub-blocks
     L.tables = o;     o = align_up(o + table_bytes, A);
     L.total = o;
     return L;
@@ -122,8 +133,8 @@ struct WS {
     unsigned *dtot;          // [digits] digit totals of the current pass
     unsigned char *block_mask;
     int *block_list;
-    float4 *g_mom;      // {mv.x, mv.y, mv.z, m}, zero between substeps
-    float2 *g_dmg;      // {sum w d, sum w}, zero between substeps
+    long long *g_mom;   // {mv.x, mv.y, mv.z, m} per node, int64 fixed point, zero between substeps
+    long long *g_dmg;   // {sum w d, sum w} per node, int64 fixed point, zero between substeps
     float4 *g_vel;      // {v.x, v.y, v.z, unused}
     float *g_gd;        // normalised damage field
     float *g_sw;        // cubic weight sums (recorded for the adjoint; NULL otherwise)
@@ -134,6 +145,7 @@ struct WS {
     const unsigned *sorted_keys;
     const int *perm;
     int *inv_perm;      // particle -> sorted position, written by the last radix pass
+    int *work;          // sorted index of the first particle of every non-empty 4^3-cell sub-block
     int passes, key_bits, n_tiles, nbs;
     long long n_blocks;
 };
@@ -150,8 +162,8 @@ inline WS make_ws(void *base, const Layout &L) {
     w.dtot = w.hist + (size_t)kRadixTop * L.n_tiles;
     w.block_mask = (unsigned char *)(b + L.block_mask);
     w.block_list = (int *)(b + L.block_list);
-    w.g_mom = (float4 *)(b + L.g_mom);
-    w.g_dmg = (float2 *)(b + L.g_dmg);
+    w.g_mom = (long long *)(b + L.g_mom);
+    w.g_dmg = (long long *)(b + L.g_dmg);
     w.g_vel = (float4 *)(b + L.g_vel);
     w.g_gd = (float *)(b + L.g_gd);
     w.g_sw = nullptr;
@@ -168,6 +180,7 @@ inline WS make_ws(void *base, const Layout &L) {
     w.sorted_keys = (L.passes & 1) ? w.keys_b : w.keys_a;
     w.perm = (L.passes & 1) ? w.vals_b : w.vals_a;
     w.inv_perm = (int *)(b + L.inv_perm);
+    w.work = (int *)(b + L.work);
     return w;
 }
 
@@ -329,14 +342,64 @@ __device__ __forceinline__ unsigned cell_key(const int b[3], int ng) {
     return ((unsigned)x * (unsigned)ng + (unsigned)y) * (unsigned)ng + (unsigned)z;
 }
 
+// Morton (z-order) number of a cell inside its 8^3 sort block, bits
+// x2 y2 z2 x1 y1 z1 x0 y0 z0: every aligned run of 8^k numbers is a brick of
+// edge 2^k, and the top three bits name the cell's 4^3-cell sub-block (the
+// P2G work unit).
+__host__ __device__ __forceinline__ unsigned morton9(unsigned x, unsigned y, unsigned z) {
+    unsigned m = 0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+        m |= (((x >> b) & 1u) << (3 * b + 2)) | (((y >> b) & 1u) << (3 * b + 1)) | (((z >> b) & 1u) << (3 * b));
+    return m;
+}
+// Cell of Morton number m (low 6 bits: inside the 4^3 sub-block; 9 bits: inside the 8^3 block).
+__host__ __device__ __forceinline__ void morton_decode(unsigned m, int c[3]) {
+    c[0] = (int)(((m >> 2) & 1u) | ((m >> 4) & 2u) | ((m >> 6) & 4u));
+    c[1] = (int)(((m >> 1) & 1u) | ((m >> 3) & 2u) | ((m >> 5) & 4u));
+    c[2] = (int)((m & 1u) | ((m >> 2) & 2u) | ((m >> 4) & 4u));
+}
+
 // Sort key of the substep: the same base cell, numbered block-major (8^3-cell
-// blocks in x-major order, cells x-major inside a block) so that a run of the
-// sorted order is a compact brick.  A bijection of cell_key.
+// blocks in x-major order, cells in Morton order inside a block) so that a
+// run of the sorted order is a compact brick.  A bijection of cell_key.
 __device__ __forceinline__ unsigned blocked_key(const int b[3], int ng) {
     const int x = clampi(b[0], 0, ng - 1), y = clampi(b[1], 0, ng - 1), z = clampi(b[2], 0, ng - 1);
     const unsigned nb = (unsigned)sort_blocks_per_axis(ng);
     const unsigned blk = ((unsigned)(x >> 3) * nb + (unsigned)(y >> 3)) * nb + (unsigned)(z >> 3);
-    return (blk << kSortBlockBits) | ((unsigned)(x & 7) << 6) | ((unsigned)(y & 7) << 3) | (unsigned)(z & 7);
+    return (blk << kSortBlockBits) | morton9((unsigned)x & 7u, (unsigned)y & 7u, (unsigned)z & 7u);
+}
+
+// ------------------------------------------------------- fixed-point grid sums
+// P2G accumulates into int64 fixed point, so the sums are exact and do not
+// depend on the order of the atomic additions: a substep is bit-reproducible
+// run to run, which the adjoint's checkpoint re-runs rely on.  The unit of a
+// quantity is 2^(e - kFixBits) with 2^e above the substep's bound on one
+// contribution; a node total then holds 2^(63 - kFixBits) worst-case
+// contributions before it could overflow, and every contribution is resolved
+// to 2^-kFixBits of the bound (far finer than its own float32 rounding).
+constexpr int kFixBits = 36;
+// Scale (2^(kFixBits - e)) and unit (its inverse) from a bound's float bits;
+// bounds below 2^-90 (including zero) or not finite use 2^-90 / 2^127.
+struct FixScale {
+    float scale, unit;
+};
+__device__ __forceinline__ FixScale fix_scale(unsigned bound_bits) {
+    float b = __uint_as_float(bound_bits);
+    if (!(b >= 8.0779e-28f)) b = 8.0779e-28f;           // 2^-90; also NaN
+    if (!(b <= 1.0e38f)) b = 1.0e38f;
+    const int e = (int)((__float_as_uint(b) >> 23) & 0xffu) - 126;   // 2^(e-1) <= b < 2^e
+    FixScale f;
+    f.scale = __uint_as_float((unsigned)(127 + kFixBits - e) << 23);
+    f.unit = __uint_as_float((unsigned)(127 - kFixBits + e) << 23);
+    return f;
+}
+__device__ __forceinline__ long long to_fix(float v, float scale) { return __float2ll_rn(v * scale); }
+__device__ __forceinline__ float from_fix(long long q, float unit) { return __ll2float_rn(q) * unit; }
+// Magnitude bound of a value for the control block's atomicMax (NaN counts as 0).
+__device__ __forceinline__ unsigned bound_bits(float v) {
+    const float a = fabsf(v);
+    return a <= 3.4e38f ? __float_as_uint(a) : 0u;
 }
 
 // ------------------------------------------------------------ 3x3 algebra
@@ -410,9 +473,12 @@ __device__ __forceinline__ float nan_to_num(float a) {
 
 // sym_eig (anisompm.py:48-95): symmetrise + nan_to_num, 5 (or `sweeps`) cyclic
 // sweeps over pairs (0,1),(0,2),(1,2), eigenvalues ascending (stable order),
-// eigenvector columns in V (row-major).
+// eigenvector columns in V (row-major).  SWEEPS > 0 fixes the sweep count at
+// compile time (the substep's 5); SWEEPS == 0 takes it from `sweeps_rt`, any
+// count >= 1, as the reference's `sweeps` argument (anisompm.py:48, 68).
 template <int SWEEPS>
-__device__ __forceinline__ void sym_eig3(const float *Ain, float ev[3], float V[9]) {
+__device__ __forceinline__ void sym_eig3(const float *Ain, float ev[3], float V[9], int sweeps_rt = SWEEPS) {
+    const int n_sweeps = SWEEPS > 0 ? SWEEPS : sweeps_rt;
     float a00 = nan_to_num(0.5f * (Ain[0] + Ain[0]));
     float a11 = nan_to_num(0.5f * (Ain[4] + Ain[4]));
     float a22 = nan_to_num(0.5f * (Ain[8] + Ain[8]));
@@ -422,7 +488,7 @@ __device__ __forceinline__ void sym_eig3(const float *Ain, float ev[3], float V[
 #pragma unroll
     for (int k = 0; k < 9; ++k) V[k] = (k % 4 == 0) ? 1.0f : 0.0f;
 #pragma unroll
-    for (int sw = 0; sw < SWEEPS; ++sw) {
+    for (int sw = 0; sw < n_sweeps; ++sw) {
         // Once every lane's off-diagonal is below 1e-10 of its diagonal, the
         // remaining sweeps of the reference change nothing at float32
         // precision: a rotation with |t| ~ |apq|/gap <= 1e-10 leaves c = 1 and
@@ -482,6 +548,50 @@ __device__ __forceinline__ void stress_eig_polar(const float Ucols[9], const flo
         const float s2 = sig[6] * q0 + sig[7] * q1 + sig[8] * q2;
         ev[j] = q0 * s0 + q1 * s1 + q2 * s2;
     }
+}
+
+// ------------------------------------------------------- cell-aggregated scatter
+// Quadratic weights of one axis from fx (anisompm.py:549-556).
+__device__ __forceinline__ void qw(float f, float w[3]) {
+    const float t0 = 1.5f - f, t1 = f - 1.0f, t2 = f - 0.5f;
+    w[0] = 0.5f * (t0 * t0);
+    w[1] = 0.75f - t1 * t1;
+    w[2] = 0.5f * (t2 * t2);
+}
+// Cubic weights of one axis expanded onto the 5 nodes [qb-1, qb+3] of a
+// quadratic cell: with s = (fx >= 1) the particle's cubic base is qb - 1 + s
+// and its fraction f = fx - s (both exact), so node n takes weight w[n - s]
+// (anisompm.py:575-583).  cw5_2 expands the second-derivative factors w''
+// (anisompm.py:579-583) the same way.
+__device__ __forceinline__ void cw5(float fx, float e[5]) {
+    const bool s1 = fx >= 1.0f;
+    const float f = s1 ? fx - 1.0f : fx;
+    const float one = 1.0f - f;
+    const float w0 = (1.0f / 6.0f) * (one * one * one);
+    const float w1 = (2.0f / 3.0f - f * f) + 0.5f * (f * f * f);
+    const float w2 = (2.0f / 3.0f - one * one) + 0.5f * (one * one * one);
+    const float w3 = (1.0f / 6.0f) * (f * f * f);
+    e[0] = s1 ? 0.0f : w0;
+    e[1] = s1 ? w0 : w1;
+    e[2] = s1 ? w1 : w2;
+    e[3] = s1 ? w2 : w3;
+    e[4] = s1 ? w3 : 0.0f;
+}
+__device__ __forceinline__ void cw5_2(float fx, float e[5]) {
+    const bool s1 = fx >= 1.0f;
+    const float f = s1 ? fx - 1.0f : fx;
+    const float w0 = 1.0f - f, w1 = 3.0f * f - 2.0f, w2 = 1.0f - 3.0f * f, w3 = f;
+    e[0] = s1 ? 0.0f : w0;
+    e[1] = s1 ? w0 : w1;
+    e[2] = s1 ? w1 : w2;
+    e[3] = s1 ? w2 : w3;
+    e[4] = s1 ? w3 : 0.0f;
+}
+
+// Adds a float partial sum to an int64 fixed-point tile entry.
+__device__ __forceinline__ void tile_add(long long *t, float v, float scale) {
+    const long long q = to_fix(v, scale);
+    if (q != 0) atomicAdd((unsigned long long *)t, (unsigned long long)q);
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {

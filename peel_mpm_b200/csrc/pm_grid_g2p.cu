@@ -5,13 +5,25 @@
 namespace pm {
 
 // ------------------------------------------------------------------ clock
+// Per-substep reset of a control block's counters and bounds.
+__device__ __forceinline__ void reset_ctrl(Ctrl *c, bool shared_counters) {
+    c->any_allow = 0;
+    c->mom_bound = 0;
+    c->mass_bound = 0;
+    c->dmg_bound = 0;
+    if (shared_counters) {
+        c->n_active = 0;
+        c->n_work = 0;
+        c->work_next = 0;
+    }
+}
+
 __global__ void k_set_clock(Ctrl *c, const pm_clock clk, int ncol) {
     const int t = threadIdx.x;
     if (t == 0) {
         c->time = clk.time;
         c->step = clk.step;
-        c->any_allow = 0;
-        c->n_active = 0;
+        reset_ctrl(c, true);
     }
     if (t < ncol) {
 #pragma unroll
@@ -29,8 +41,7 @@ __global__ void k_set_clock_dev(Ctrl *c, const pm_clock *dev, int row, int ncol)
     if (t == 0) {
         c->time = clk->time;
         c->step = clk->step;
-        c->any_allow = 0;
-        c->n_active = 0;
+        reset_ctrl(c, true);
     }
     if (t < ncol) {
 #pragma unroll
@@ -51,8 +62,7 @@ __global__ void k_set_clock_b(Ctrl *c, const pm_params *prms, const pm_clock *de
     if (t == 0) {
         cs->time = clk->time;
         cs->step = clk->step;
-        cs->any_allow = 0;
-        if (sid == 0) cs->n_active = 0;
+        reset_ctrl(cs, sid == 0);
     }
     if (t < prms[sid].n_colliders) {
 #pragma unroll
@@ -120,13 +130,27 @@ __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
         if (ix >= ng || iy >= ng) continue;
         const int nz = min(kBlockEdge, ng - iz0);
         const long long row = sc.node_base(sid) + ((long long)ix * ng + iy) * ng + iz0;
+        // exact fixed-point sums -> float, each rounded once
+        const FixScale fm = fix_scale(ctrl->mom_bound), fmm = fix_scale(ctrl->mass_bound),
+                       fd = fix_scale(ctrl->dmg_bound), fw = fix_scale(__float_as_uint(1.0f));
+        longlong2 qm[kBlockEdge][2], qd[kBlockEdge];
+#pragma unroll
+        for (int k = 0; k < kBlockEdge; ++k) {
+            if (k < nz) {
+                const longlong2 *gm = (const longlong2 *)(w.g_mom + 4 * (row + k));
+                qm[k][0] = gm[0];
+                qm[k][1] = gm[1];
+                qd[k] = *(const longlong2 *)(w.g_dmg + 2 * (row + k));
+            }
+        }
         float4 mom[kBlockEdge];
         float2 dmg[kBlockEdge];
 #pragma unroll
         for (int k = 0; k < kBlockEdge; ++k) {
             if (k < nz) {
-                mom[k] = w.g_mom[row + k];
-                dmg[k] = w.g_dmg[row + k];
+                mom[k] = make_float4(from_fix(qm[k][0].x, fm.unit), from_fix(qm[k][0].y, fm.unit),
+                                     from_fix(qm[k][1].x, fm.unit), from_fix(qm[k][1].y, fmm.unit));
+                dmg[k] = make_float2(from_fix(qd[k].x, fd.unit), from_fix(qd[k].y, fw.unit));
             }
         }
         const float dt = (float)prm.dt;
@@ -139,8 +163,10 @@ __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
         for (int k = 0; k < kBlockEdge; ++k) {
             if (k >= nz) continue;
             const long long node = row + k;
-            w.g_mom[node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            w.g_dmg[node] = make_float2(0.0f, 0.0f);
+            longlong2 *gm = (longlong2 *)(w.g_mom + 4 * node);
+            gm[0] = make_longlong2(0, 0);
+            gm[1] = make_longlong2(0, 0);
+            *(longlong2 *)(w.g_dmg + 2 * node) = make_longlong2(0, 0);
             const bool active = mom[k].w > 1e-12f;
             const float inv_m = active ? 1.0f / mom[k].w : 0.0f;
             float v[3] = {mom[k].x * inv_m + gdt[0], mom[k].y * inv_m + gdt[1], mom[k].z * inv_m + gdt[2]};
@@ -177,17 +203,38 @@ __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
 }
 
 template <class SC>
-void launch_grid(const SC &sc, const WS &w, cudaStream_t s) {
+void launch_grid(const SC &sc, const WS &w, cudaStream_t s, int ctas_per_sm) {
     const long long max_items = w.n_blocks * 16;
     // a batch has many more active nodes than one scene and every row starts
-    // with a dependent chain of table loads (scene lookup, parameters): give
-    // each row its own thread rather than a grid-stride loop
-    const long long cap = SC::batched ? 148LL * 64 : 148LL * 8;
+    // with a dependent chain of table loads (scene lookup, parameters): by
+    // default give each row its own thread rather than a grid-stride loop;
+    // ctas_per_sm (the tunable) sets the grid-stride cap instead
+    const long long cap = ctas_per_sm > 0 ? 148LL * ctas_per_sm : (SC::batched ? 148LL * 64 : 148LL * 8);
     const int blocks = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, cap));
     k_grid<SC><<<blocks, 256, 0, s>>>(sc, w);
 }
-template void launch_grid<PlainScenes>(const PlainScenes &, const WS &, cudaStream_t);
-template void launch_grid<BatchScenes>(const BatchScenes &, const WS &, cudaStream_t);
+template void launch_grid<PlainScenes>(const PlainScenes &, const WS &, cudaStream_t, int);
+template void launch_grid<BatchScenes>(const BatchScenes &, const WS &, cudaStream_t, int);
+
+// Accumulators as floats {mv, m} and {sum w d, sum w} (inspection of a
+// substep between P2G and the grid update; no effect on the state).
+__global__ void k_grid_sums(const WS w, long long n_nodes, float4 *mom, float2 *dmg) {
+    const Ctrl *ctrl = w.ctrl;
+    const FixScale fm = fix_scale(ctrl->mom_bound), fmm = fix_scale(ctrl->mass_bound),
+                   fd = fix_scale(ctrl->dmg_bound), fw = fix_scale(__float_as_uint(1.0f));
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long *g = w.g_mom + 4 * i, *h = w.g_dmg + 2 * i;
+        mom[i] = make_float4(from_fix(g[0], fm.unit), from_fix(g[1], fm.unit), from_fix(g[2], fm.unit),
+                             from_fix(g[3], fmm.unit));
+        dmg[i] = make_float2(from_fix(h[0], fd.unit), from_fix(h[1], fw.unit));
+    }
+}
+
+void launch_grid_sums(const WS &w, long long n_nodes, float *mom, float *dmg, cudaStream_t s) {
+    const int blocks = (int)std::max<long long>(1, std::min<long long>((n_nodes + 255) / 256, 148LL * 16));
+    k_grid_sums<<<blocks, 256, 0, s>>>(w, n_nodes, (float4 *)mom, (float2 *)dmg);
+}
 
 // --------------------------------------------------------------------- G2P
 // One CTA per 256 particles in particle order (coalesced state reads and
@@ -208,11 +255,17 @@ constexpr int kGTC = 2400;   // staged cubic nodes (float)
 template <bool TILE>
 __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &P, const float4 *gvel,
                                              const float *ggd, unsigned *nonfinite, long long p, const float xp[3],
-                                             const float F[9], const int lo[3], const int qd[3], const int cd[3],
+                                             const int lo[3], const int qd[3], const int cd[3],
                                              const float4 *sq, const float *sc) {
     const long long ps = P.ps;
     const int ng = prm.n_grid;
     const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx, dt = (float)prm.dt;
+    // Quadratic gather (anisompm.py:749-760) as a contraction over z, then y,
+    // then x: with u = w g and dpos_j = (o_j - fx_j) dx,
+    //   v = sum_x wx T[x],  C_.x = sum_x wx DX T[x],  C_.y = sum_x wx Ty[x],
+    //   C_.z = sum_x wx Tz[x],  where T[x] = sum_{y,z} wy wz g,
+    //   Ty[x] = sum_{y,z} wy DY wz g and Tz[x] = sum_{y,z} wy wz DZ g,
+    // so every node costs 9 FMAs and one float4 load.
     float nv[3] = {0.0f, 0.0f, 0.0f}, nC[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) nC[k] = 0.0f;
@@ -237,30 +290,35 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
             DZ[o] = ((float)o - q.fx[2]) * dx;
         }
 #pragma unroll
-        for (int ox = 0; ox < 3; ++ox)
+        for (int ox = 0; ox < 3; ++ox) {
+            float T[3] = {0.0f, 0.0f, 0.0f}, Ty[3] = {0.0f, 0.0f, 0.0f}, Tz[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-            for (int oy = 0; oy < 3; ++oy) {
-                const float wxy = q.w[ox][0] * q.w[oy][1];
+            for (int oy = 0; oy < 3; ++oy)
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
-                    const float wk = wxy * q.w[oz][2];
                     const int node = NX[ox] + NY[oy] + NZ[oz];
                     const float4 g = TILE ? sq[node] : __ldg(&gvel[node]);
-                    const float u0 = wk * g.x, u1 = wk * g.y, u2 = wk * g.z;
-                    nv[0] += u0; nv[1] += u1; nv[2] += u2;
-                    const float dp[3] = {DX[ox], DY[oy], DZ[oz]};
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        nC[j] += u0 * dp[j];
-                        nC[3 + j] += u1 * dp[j];
-                        nC[6 + j] += u2 * dp[j];
-                    }
+                    const float wyz = q.w[oy][1] * q.w[oz][2], wyzy = wyz * DY[oy], wyzz = wyz * DZ[oz];
+                    T[0] += wyz * g.x; T[1] += wyz * g.y; T[2] += wyz * g.z;
+                    Ty[0] += wyzy * g.x; Ty[1] += wyzy * g.y; Ty[2] += wyzy * g.z;
+                    Tz[0] += wyzz * g.x; Tz[1] += wyzz * g.y; Tz[2] += wyzz * g.z;
                 }
+            const float wx = q.w[ox][0], wxd = wx * DX[ox];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                nv[i] += wx * T[i];
+                nC[3 * i] += wxd * T[i];
+                nC[3 * i + 1] += wx * Ty[i];
+                nC[3 * i + 2] += wx * Tz[i];
             }
+        }
         const float cfac = (float)(4.0 * prm.inv_dx * prm.inv_dx);
 #pragma unroll
         for (int k = 0; k < 9; ++k) nC[k] *= cfac;
     }
+    // Cubic Laplacian gather (anisompm.py:781-791): for each (x, y) column
+    // A = sum_z wz gd and B = sum_z w''z gd, then
+    // lap = sum_{x,y} (w''x wy + wx w''y) A + wx wy B.
     float lap = 0.0f;
     {
         Cubic c;
@@ -278,18 +336,21 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
                 NZ[o] = clampi(c.b[2] + o, 0, ng - 1);
             }
         }
-        // (w''x wy wz + wx w''y wz + wx wy w''z) = (w''x wy + wx w''y) wz + (wx wy) w''z
 #pragma unroll
         for (int ox = 0; ox < 4; ++ox)
 #pragma unroll
             for (int oy = 0; oy < 4; ++oy) {
-                const float ab = c.w2[ox][0] * c.w[oy][1] + c.w[ox][0] * c.w2[oy][1];
-                const float e = c.w[ox][0] * c.w[oy][1];
+                float A = 0.0f, B = 0.0f;
 #pragma unroll
                 for (int oz = 0; oz < 4; ++oz) {
                     const int node = NX[ox] + NY[oy] + NZ[oz];
-                    lap += (ab * c.w[oz][2] + e * c.w2[oz][2]) * (TILE ? sc[node] : __ldg(&ggd[node]));
+                    const float gd = TILE ? sc[node] : __ldg(&ggd[node]);
+                    A += c.w[oz][2] * gd;
+                    B += c.w2[oz][2] * gd;
                 }
+                const float ab = c.w2[ox][0] * c.w[oy][1] + c.w[ox][0] * c.w2[oy][1];
+                const float e = c.w[ox][0] * c.w[oy][1];
+                lap += ab * A + e * B;
             }
         lap *= (float)(prm.inv_dx * prm.inv_dx);
     }
@@ -302,7 +363,9 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
         t = t < pad ? pad : t;
         xn[a] = t > hi ? hi : t;
     }
-    float Fn[9], A[9];
+    float F[9], Fn[9], A[9];   // F is loaded after the gathers: fewer registers live across them
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = P.F[k * ps + p];
 #pragma unroll
     for (int k = 0; k < 9; ++k) A[k] = ((k % 4 == 0) ? 1.0f : 0.0f) + dt * nC[k];
     mm3(A, F, Fn);
@@ -326,7 +389,7 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
 }
 
 template <class SC>
-__global__ void __launch_bounds__(kG2PThreads, 4) k_g2p(const SC scn, const Parts P, const WS w) {
+__global__ void __launch_bounds__(kG2PThreads, 3) k_g2p(const SC scn, const Parts P, const WS w) {
     __shared__ float4 sq[kGTQ];
     __shared__ float sc[kGTC];
     __shared__ int s_box[6];
@@ -341,14 +404,12 @@ __global__ void __launch_bounds__(kG2PThreads, 4) k_g2p(const SC scn, const Part
     const int ng = prm.n_grid;
     const long long ps = P.ps;
     const float inv_dx = (float)prm.inv_dx;
-    float xp[3] = {0.0f, 0.0f, 0.0f}, F[9];
+    float xp[3] = {0.0f, 0.0f, 0.0f};
     int qb[3] = {0, 0, 0};
     bool reg = valid;
     if (valid) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) xp[a] = P.x[a * ps + p];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) F[k] = P.F[k * ps + p];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const float fb = floorf(__fsub_rn(__fmul_rn(xp[a], inv_dx), 0.5f));
@@ -397,9 +458,9 @@ __global__ void __launch_bounds__(kG2PThreads, 4) k_g2p(const SC scn, const Part
     __syncthreads();
     if (!valid) return;
     if (reg && tile)
-        g2p_particle<true>(prm, P, gvel, ggd, &w.ctrl[sid].nonfinite, p, xp, F, lo, qd, cd, sq, sc);
+        g2p_particle<true>(prm, P, gvel, ggd, &w.ctrl[sid].nonfinite, p, xp, lo, qd, cd, sq, sc);
     else
-        g2p_particle<false>(prm, P, gvel, ggd, &w.ctrl[sid].nonfinite, p, xp, F, lo, qd, cd, sq, sc);
+        g2p_particle<false>(prm, P, gvel, ggd, &w.ctrl[sid].nonfinite, p, xp, lo, qd, cd, sq, sc);
 }
 
 // n_ctas: CTAs over all scenes (each scene's particles start a new CTA); the
@@ -421,16 +482,10 @@ __global__ void __launch_bounds__(256) k_sym_eig(const float *__restrict__ A, lo
     float a[9], e[3], vv[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) a[k] = A[9 * p + k];
-    switch (sweeps) {
-        case 1: sym_eig3<1>(a, e, vv); break;
-        case 2: sym_eig3<2>(a, e, vv); break;
-        case 3: sym_eig3<3>(a, e, vv); break;
-        case 4: sym_eig3<4>(a, e, vv); break;
-        default: sym_eig3<5>(a, e, vv); break;
-        case 6: sym_eig3<6>(a, e, vv); break;
-        case 8: sym_eig3<8>(a, e, vv); break;
-        case 12: sym_eig3<12>(a, e, vv); break;
-    }
+    if (sweeps == 5)
+        sym_eig3<5>(a, e, vv);           // the substep's count, unrolled
+    else
+        sym_eig3<0>(a, e, vv, sweeps);   // any other count >= 0
 #pragma unroll
     for (int k = 0; k < 3; ++k) ev[3 * p + k] = e[k];
 #pragma unroll

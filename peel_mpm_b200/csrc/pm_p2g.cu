@@ -5,22 +5,27 @@
 // fixed-corotated Kirchhoff stress, anisotropic phase-field damage (the
 // Cauchy stress's eigensystem taken from the polar decomposition, a Jacobi
 // solve only for nearly singular F), degradation and the APIC affine term;
-// the P2G payload (5 float4) goes to the particle's slot in the sorted order.
+// the P2G payload (5 float4) goes to the particle's slot in the sorted order,
+// and the substep's bounds on one node contribution (momentum, mass, damage)
+// are raised in the control block.
 //
-// k_scatter, one CTA per range of consecutive sorted particles (the range is
-// a tunable, 64..4096), split into segments that share one 8^3-cell sort
-// block.  Each segment owns two shared-memory tiles: the quadratic momentum
-// tile (nodes [8b, 8b+10)^3, {mv, m}) and the cubic damage tile (nodes
-// [8b-1, 8b+11)^3, {sum w d, sum w}).  Sub-chunks stage their payload in shared
-// memory, then one work item per (cell, x-slab): all particles of a cell share
-// their quadratic base, so an item sums the cell's contributions to 9
-// quadratic nodes (3 slabs) or 25 cubic nodes (5 slabs; a cell's cubic
-// stencils span 5^3 nodes) in registers and adds each node once.  Lanes hold
-// distinct cells, so the float shared atomics rarely meet on one address.
-// The tiles are flushed over the segment's footprint with one vector atomic
-// per touched node, marking the touched 4^3 grid blocks.  Particles whose
-// stencil needs the reference's edge clamping (base cell outside
-// [1, n_grid-4]) scatter directly to global memory instead.
+// k_p2g_tiles, persistent CTAs taking work items from a list of the
+// non-empty 4^3-cell sub-blocks of the sort (the cells of a sub-block are a
+// contiguous run of the Morton-ordered sort).  A work item owns two
+// shared-memory tiles: the quadratic momentum tile (nodes [4s, 4s+6)^3,
+// {mv, m}) and the cubic damage tile (nodes [4s-1, 4s+7)^3, {sum w d,
+// sum w}).  Chunks of 256 particles stage their payload in shared memory,
+// then one work item per (cell, x-slab): all particles of a cell share their
+// quadratic base, so an item sums the cell's contributions to 9 quadratic
+// nodes (3 slabs) or 25 cubic nodes (5 slabs; a cell's cubic stencils span
+// 5^3 nodes) in float registers, in the sorted order, and adds each node
+// once.  Tiles and the global grid accumulate int64 fixed point (units from
+// the control block's bounds): integer addition is associative, so the grid
+// sums, and with them the whole substep, are the same bits whatever order the
+// atomics run in.  The tiles are flushed with one atomic per touched node and
+// component, marking the touched 4^3 grid blocks.  Particles whose stencil
+// needs the reference's edge clamping (base cell outside [1, n_grid-4])
+// scatter directly to the global grid instead.
 //
 // Reference: anisompm.py:601-724 (constitutive, damage, P2G) and 768-776
 // (cubic damage scatter).
@@ -77,9 +82,9 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             wn[j] = sqrtf(W[j] * W[j] + W[3 + j] * W[3 + j] + W[6 + j] * W[6 + j]);
-            const float nr = wn[j] + 1e-12f;
+            const float rn = 1.0f / (wn[j] + 1e-12f);                 // one division per column
 #pragma unroll
-            for (int i = 0; i < 3; ++i) W[3 * i + j] = W[3 * i + j] / nr;   // (620)
+            for (int i = 0; i < 3; ++i) W[3 * i + j] *= rn;          // (620)
         }
         u_ok = polar_u_ok(wn);
     }
@@ -123,8 +128,9 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
 
     if (do_damage) {                                                 // (647-685)
         float sg[9];
+        const float rJ = 1.0f / J;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) sg[k] = (tdev[k] + ((k % 4 == 0) ? tv : 0.0f)) / J;
+        for (int k = 0; k < 9; ++k) sg[k] = (tdev[k] + ((k % 4 == 0) ? tv : 0.0f)) * rJ;
         float sgs[9];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -326,6 +332,32 @@ __global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, c
     dst[2] = make_float4(aff[0], aff[1], aff[2], aff[3]);
     dst[3] = make_float4(aff[4], aff[5], aff[6], aff[7]);
     dst[4] = make_float4(aff[8], reg ? 1.0f : 0.0f, 0.0f, 0.0f);
+    {   // bounds of one node contribution: |w (m v + aff dpos)| with w <= 1 and |dpos| <= 1.5 dx per axis
+        const float hx = 1.5f * (float)prm.dx;
+        float bm = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            bm = fmaxf(bm, fabsf(m * v[c]) + hx * (fabsf(aff[3 * c]) + fabsf(aff[3 * c + 1]) + fabsf(aff[3 * c + 2])));
+        unsigned bmom = bound_bits(bm), bmass = bound_bits(m), bdmg = bound_bits(d_new);
+        Ctrl *cw = w.ctrl + sid;
+        // any partition of the warp is correct here: each group raises the
+        // bounds to its own maximum
+        const unsigned am = __activemask();
+        if (!SC::batched || __all_sync(am, sid == __shfl_sync(am, sid, __ffs(am) - 1))) {
+            bmom = __reduce_max_sync(am, bmom);
+            bmass = __reduce_max_sync(am, bmass);
+            bdmg = __reduce_max_sync(am, bdmg);
+            if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1)) {
+                atomicMax(&cw->mom_bound, bmom);
+                atomicMax(&cw->mass_bound, bmass);
+                atomicMax(&cw->dmg_bound, bdmg);
+            }
+        } else {
+            atomicMax(&cw->mom_bound, bmom);
+            atomicMax(&cw->mass_bound, bmass);
+            atomicMax(&cw->dmg_bound, bdmg);
+        }
+    }
     if (w.tape_aff) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) w.tape_aff[k * w.tape_aff_stride + p] = aff[k];
@@ -334,15 +366,22 @@ __global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, c
 
 // Scatter one particle straight into the global grid with the reference's
 // clamped node indices (anisompm.py:716-724, 771-776): the path for particles
-// whose stencil leaves the grid.
+// whose stencil leaves the grid.  `sc` holds the fixed-point scales of
+// {momentum, mass, w d, w}.
 __device__ __forceinline__ void mark_node_block(unsigned char *mask, int nbs, int x, int y, int z) {
     unsigned char *m = &mask[((long long)(x >> 2) * nbs + (y >> 2)) * nbs + (z >> 2)];
     if (*m == 0) *m = 1;
 }
 
+__device__ __forceinline__ void red_fix(long long *addr, float v, float scale) {
+    const long long q = to_fix(v, scale);
+    if (q != 0) atomicAdd((unsigned long long *)addr, (unsigned long long)q);
+}
+
 __device__ __noinline__ void scatter_particle_global(const float xp[3], const float mv[3], const float aff[9],
-                                                     float m, float d, float inv_dx, float dx, int ng, float4 *g_mom,
-                                                     float2 *g_dmg, unsigned char *mask, int nbs) {
+                                                     float m, float d, float inv_dx, float dx, int ng,
+                                                     const float sc[4], long long *g_mom, long long *g_dmg,
+                                                     unsigned char *mask, int nbs) {
     {
         Quad q;
         quad_weights(xp, inv_dx, ng, q);
@@ -350,8 +389,8 @@ __device__ __noinline__ void scatter_particle_global(const float xp[3], const fl
         float DX[3], DY[3], DZ[3];
 #pragma unroll
         for (int o = 0; o < 3; ++o) {
-            NX[o] = clampi(q.b[0] + o, 0, ng - 1) * ng * ng;
-            NY[o] = clampi(q.b[1] + o, 0, ng - 1) * ng;
+            NX[o] = clampi(q.b[0] + o, 0, ng - 1);
+            NY[o] = clampi(q.b[1] + o, 0, ng - 1);
             NZ[o] = clampi(q.b[2] + o, 0, ng - 1);
             DX[o] = ((float)o - q.fx[0]) * dx;
             DY[o] = ((float)o - q.fx[1]) * dx;
@@ -368,9 +407,12 @@ __device__ __noinline__ void scatter_particle_global(const float xp[3], const fl
                     const float a0 = aff[0] * DX[ox] + aff[1] * DY[oy] + aff[2] * DZ[oz];
                     const float a1 = aff[3] * DX[ox] + aff[4] * DY[oy] + aff[5] * DZ[oz];
                     const float a2 = aff[6] * DX[ox] + aff[7] * DY[oy] + aff[8] * DZ[oz];
-                    atomicAdd(&g_mom[NX[ox] + NY[oy] + NZ[oz]],
-                              make_float4(wk * (mv[0] + a0), wk * (mv[1] + a1), wk * (mv[2] + a2), wk * m));
-                    mark_node_block(mask, nbs, NX[ox] / (ng * ng), NY[oy] / ng, NZ[oz]);
+                    long long *g = g_mom + 4 * (((long long)NX[ox] * ng + NY[oy]) * ng + NZ[oz]);
+                    red_fix(g, wk * (mv[0] + a0), sc[0]);
+                    red_fix(g + 1, wk * (mv[1] + a1), sc[0]);
+                    red_fix(g + 2, wk * (mv[2] + a2), sc[0]);
+                    red_fix(g + 3, wk * m, sc[1]);
+                    mark_node_block(mask, nbs, NX[ox], NY[oy], NZ[oz]);
                 }
             }
     }
@@ -380,8 +422,8 @@ __device__ __noinline__ void scatter_particle_global(const float xp[3], const fl
         int NX[4], NY[4], NZ[4];
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
-            NX[o] = clampi(c.b[0] + o, 0, ng - 1) * ng * ng;
-            NY[o] = clampi(c.b[1] + o, 0, ng - 1) * ng;
+            NX[o] = clampi(c.b[0] + o, 0, ng - 1);
+            NY[o] = clampi(c.b[1] + o, 0, ng - 1);
             NZ[o] = clampi(c.b[2] + o, 0, ng - 1);
         }
 #pragma unroll
@@ -392,165 +434,103 @@ __device__ __noinline__ void scatter_particle_global(const float xp[3], const fl
 #pragma unroll
                 for (int oz = 0; oz < 4; ++oz) {
                     const float wk = wxy * c.w[oz][2];
-                    atomicAdd(&g_dmg[NX[ox] + NY[oy] + NZ[oz]], make_float2(wk * d, wk));
-                    mark_node_block(mask, nbs, NX[ox] / (ng * ng), NY[oy] / ng, NZ[oz]);
+                    long long *g = g_dmg + 2 * (((long long)NX[ox] * ng + NY[oy]) * ng + NZ[oz]);
+                    red_fix(g, wk * d, sc[2]);
+                    red_fix(g + 1, wk, sc[3]);
+                    mark_node_block(mask, nbs, NX[ox], NY[oy], NZ[oz]);
                 }
             }
     }
 }
 
-constexpr int kQE = kSortBlock + 2;            // 10: quadratic tile edge, nodes [8b, 8b+10)
-constexpr int kCE = kSortBlock + 4;            // 12: cubic tile edge, nodes [8b-1, 8b+11)
-constexpr int kQN = kQE * kQE * kQE;           // 1000
-constexpr int kCN = kCE * kCE * kCE;           // 1728
-constexpr int kP2GMaxRange = 4096;             // sorted particles per CTA at most
-constexpr int kP2GDefaultRange = 512;
-constexpr int kSub = kP2GThreads;              // particles per sub-chunk
+constexpr int kSubEdge = 4;                    // sub-block edge in cells (the P2G work unit)
+constexpr int kQE = kSubEdge + 2;              // 6: quadratic tile edge, nodes [4s, 4s+6)
+constexpr int kCE = kSubEdge + 4;              // 8: cubic tile edge, nodes [4s-1, 4s+7)
+constexpr int kQN = kQE * kQE * kQE;           // 216
+constexpr int kCN = kCE * kCE * kCE;           // 512
+constexpr int kSub = kP2GThreads;              // particles per chunk
 constexpr int kCW = 15;                        // expanded cubic weights per particle (5 per axis)
-constexpr size_t kP2GSmem = sizeof(float) * (4 * kQN + 2 * kCN + (kPay + kCW) * kPayStride) + sizeof(int) * (kSub + 2) +
-                            kSub + sizeof(short) * (kP2GMaxRange + 2);
+constexpr size_t kP2GSmem = sizeof(long long) * (4 * kQN + 2 * kCN) + sizeof(float) * (kPay + kCW) * kPayStride +
+                            sizeof(int) * (kSub + 2) + 2 * kSub;
 
-// Quadratic weights of one axis from fx (anisompm.py:549-556).
-__device__ __forceinline__ void qw(float f, float w[3]) {
-    const float t0 = 1.5f - f, t1 = f - 1.0f, t2 = f - 0.5f;
-    w[0] = 0.5f * (t0 * t0);
-    w[1] = 0.75f - t1 * t1;
-    w[2] = 0.5f * (t2 * t2);
-}
-// Cubic weights of one axis expanded onto the 5 nodes [qb-1, qb+3] of a cell:
-// with s = (fx >= 1) the particle's cubic base is qb - 1 + s and its fraction
-// f = fx - s (both exact), so node n takes weight w[n - s] (anisompm.py:575-583).
-__device__ __forceinline__ void cw5(float fx, float e[5]) {
-    const bool s1 = fx >= 1.0f;
-    const float f = s1 ? fx - 1.0f : fx;
-    const float one = 1.0f - f;
-    const float w0 = (1.0f / 6.0f) * (one * one * one);
-    const float w1 = (2.0f / 3.0f - f * f) + 0.5f * (f * f * f);
-    const float w2 = (2.0f / 3.0f - one * one) + 0.5f * (one * one * one);
-    const float w3 = (1.0f / 6.0f) * (f * f * f);
-    e[0] = s1 ? 0.0f : w0;
-    e[1] = s1 ? w0 : w1;
-    e[2] = s1 ? w1 : w2;
-    e[3] = s1 ? w2 : w3;
-    e[4] = s1 ? w3 : 0.0f;
-}
-
-// Ordered compaction of flagged positions [0, n) held PER per thread.
-template <int PER>
-__device__ __forceinline__ int compact_flags(int flags, int *out_short_or_int, bool as_short, int *s_wcnt) {
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int cnt = __popc(flags);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
+// Sorted index of the first particle of every non-empty 4^3-cell sub-block
+// (where key >> 6 changes), appended in any order: the accumulation is exact,
+// so the order in which work items run does not change the result.
+__global__ void __launch_bounds__(256) k_subblocks(const unsigned *__restrict__ keys, long long n,
+                                                   int *__restrict__ work, Ctrl *ctrl) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const long long i = base + threadIdx.x;
+        const bool st = i < n && (i == 0 || (keys[i] >> 6) != (keys[i - 1] >> 6));
+        const unsigned ball = __ballot_sync(0xffffffffu, st);
+        unsigned slot0 = 0;
+        if ((threadIdx.x & 31) == 0 && ball) slot0 = atomicAdd(&ctrl->n_work, (unsigned)__popc(ball));
+        slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+        const unsigned slot = slot0 + __popc(ball & lanemask_lt());
+        if (st && slot < (unsigned long long)n) work[slot] = (int)i;   // bounded even without a clock reset
     }
-    if (lane == 31) s_wcnt[wid] = incl;
-    __syncthreads();
-    int pos = incl - cnt, total = 0;
-#pragma unroll
-    for (int w2 = 0; w2 < kP2GThreads / 32; ++w2) {
-        pos += (w2 < wid) ? s_wcnt[w2] : 0;
-        total += s_wcnt[w2];
-    }
-#pragma unroll
-    for (int k = 0; k < PER; ++k)
-        if (flags & (1 << k)) {
-            if (as_short)
-                ((short *)out_short_or_int)[pos++] = (short)(tid * PER + k);
-            else
-                out_short_or_int[pos++] = tid * PER + k;
-        }
-    __syncthreads();
-    return total;
 }
 
 template <class SC>
-__global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const WS w, long long n,
-                                                             int range) {
-    extern __shared__ float4 s_raw[];
-    float *qt = (float *)s_raw;                                        // [4][kQN]
-    float *ct = qt + 4 * kQN;                                          // [2][kCN]
-    float (*pay)[kPayStride] = (float (*)[kPayStride])(ct + 2 * kCN);  // [kPay][kPayStride]
-    float (*cwt)[kPayStride] = (float (*)[kPayStride])(pay[kPay]);    // [kCW][kPayStride]
-    int *runs = (int *)(cwt[kCW]);                                     // [kSub + 2]
-    unsigned char *regular = (unsigned char *)(runs + kSub + 2);       // [kSub]
-    short *seg = (short *)(regular + kSub);                            // [kP2GRange + 2]
+__global__ void __launch_bounds__(kP2GThreads, 3) k_p2g_tiles(const SC sc, const WS w, long long n) {
+    extern __shared__ long long s_raw[];
+    long long *qt = s_raw;                                                // [4][kQN]
+    long long *ct = qt + 4 * kQN;                                         // [2][kCN]
+    float (*pay)[kPayStride] = (float (*)[kPayStride])(ct + 2 * kCN);   // [kPay][kPayStride]
+    float (*cwt)[kPayStride] = (float (*)[kPayStride])(pay[kPay]);     // [kCW][kPayStride]
+    int *runs = (int *)(cwt[kCW]);                                      // [kSub + 2]
+    unsigned char *regular = (unsigned char *)(runs + kSub + 2);        // [kSub]
+    unsigned char *lcell = regular + kSub;                              // [kSub] cell inside the sub-block
     __shared__ int s_wcnt[kP2GThreads / 32];
-    __shared__ unsigned char s_bmark[64];
-    __shared__ int s_cb[6];   // cell bounding box of the segment inside its block
+    __shared__ unsigned char s_bmark[27];
+    __shared__ unsigned s_item;
 
-    const int tid = threadIdx.x;
-    const long long r0 = (long long)blockIdx.x * range;
-    const int len = (int)min((long long)range, n - r0);
-    const unsigned *keys = w.sorted_keys + r0;
-
-    // ---- segments: runs of one sort block in [0, len)
-    int nseg;
-    {
-        constexpr int PER = kP2GMaxRange / kP2GThreads;
-        int flags = 0;
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const int i = tid * PER + k;
-            if (i < len && (i == 0 || (keys[i] >> kSortBlockBits) != (keys[i - 1] >> kSortBlockBits)))
-                flags |= 1 << k;
-        }
-        nseg = compact_flags<PER>(flags, (int *)seg, true, s_wcnt);
-    }
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const unsigned *keys = w.sorted_keys;
+    Ctrl *ctrl0 = w.ctrl;
+    const unsigned n_work = min(ctrl0->n_work, (unsigned)min(n, (long long)0x7fffffff));
 
     // tiles start zero; every flush clears what it visits, so they stay zero
-    for (int i = tid; i < 4 * kQN + 2 * kCN; i += kP2GThreads) qt[i] = 0.0f;   // qt and ct are contiguous
-    __syncthreads();
-    for (int sg = 0; sg < nseg; ++sg) {
-        const int a = seg[sg];
-        const int b = (sg + 1 < nseg) ? seg[sg + 1] : len;
-        const unsigned gblk = keys[a] >> kSortBlockBits;       // segments never span scenes
+    for (int i = tid; i < 4 * kQN + 2 * kCN; i += kP2GThreads) qt[i] = 0;
+    if (tid < 27) s_bmark[tid] = 0;
+    for (;;) {
+        __syncthreads();                  // the previous item's tiles, marks and shared state are done
+        if (tid == 0) s_item = atomicAdd(&ctrl0->work_next, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= n_work) break;
+        const long long a = w.work[item];
+        const unsigned key0 = keys[a];
+        const unsigned sbk = key0 >> 6;                      // sub-block id
+        const unsigned gblk = key0 >> kSortBlockBits;        // sub-blocks never span scenes
         const int sid = sc.of_sblock(gblk);
         const pm_params &prm = sc.params(sid);
+        const Ctrl *cs = w.ctrl + sid;
         const int ng = prm.n_grid;
         const int nb = sort_blocks_per_axis(ng);
         const int nbs = (ng + kBlockEdge - 1) / kBlockEdge;
         const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
-        float4 *g_mom = w.g_mom + sc.node_base(sid);
-        float2 *g_dmg = w.g_dmg + sc.node_base(sid);
+        const FixScale fm = fix_scale(cs->mom_bound), fma_ = fix_scale(cs->mass_bound),
+                       fd = fix_scale(cs->dmg_bound), fw = fix_scale(__float_as_uint(1.0f));
+        const float scl[4] = {fm.scale, fma_.scale, fd.scale, fw.scale};
+        long long *g_mom = w.g_mom + 4 * sc.node_base(sid);
+        long long *g_dmg = w.g_dmg + 2 * sc.node_base(sid);
         unsigned char *bmask = w.block_mask + sc.gblock_base(sid);
         const unsigned blk = gblk - sc.sblock_base(sid);
         const int bz = (int)(blk % nb), by = (int)((blk / nb) % nb), bx = (int)(blk / ((unsigned)nb * nb));
-        const int org[3] = {bx * kSortBlock, by * kSortBlock, bz * kSortBlock};   // quadratic tile origin
-        {   // the segment's cell bounding box (inside the block): the flush visits only its footprint
-            int lo[3] = {7, 7, 7}, hi[3] = {0, 0, 0};
-            for (int i = a + tid; i < b; i += kP2GThreads) {
-                const unsigned k = keys[i];
-                const int c[3] = {(int)((k >> 6) & 7), (int)((k >> 3) & 7), (int)(k & 7)};
-#pragma unroll
-                for (int ax = 0; ax < 3; ++ax) {
-                    lo[ax] = min(lo[ax], c[ax]);
-                    hi[ax] = max(hi[ax], c[ax]);
-                }
-            }
-            if (tid < 6) s_cb[tid] = tid < 3 ? 7 : 0;
-            __syncthreads();
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-                const int mn = __reduce_min_sync(0xffffffffu, lo[ax]), mx = __reduce_max_sync(0xffffffffu, hi[ax]);
-                if ((tid & 31) == 0) {
-                    atomicMin(&s_cb[ax], mn);
-                    atomicMax(&s_cb[3 + ax], mx);
-                }
-            }
-            __syncthreads();
-        }
-        const int cmin[3] = {s_cb[0], s_cb[1], s_cb[2]};
-        const int cext[3] = {s_cb[3] - s_cb[0] + 1, s_cb[4] - s_cb[1] + 1, s_cb[5] - s_cb[2] + 1};
+        const unsigned oct = (key0 >> 6) & 7u;               // Morton: the sub-block inside its 8^3 block
+        const int org[3] = {bx * kSortBlock + (int)((oct >> 2) & 1u) * kSubEdge,
+                            by * kSortBlock + (int)((oct >> 1) & 1u) * kSubEdge,
+                            bz * kSortBlock + (int)(oct & 1u) * kSubEdge};   // first cell of the sub-block
 
-        for (int sub = a; sub < b; sub += kSub) {
-            const int cnt = min(kSub, b - sub);
-            // ---------------- phase 1: the sub-chunk's payload (written by k_stress in
-            // sorted order) into shared memory: coalesced float4 loads
-            if (tid < cnt) {
-                const float4 *src = w.payload + 5 * (r0 + sub + tid);
+        for (long long sub = a;; sub += kSub) {
+            // ---------------- the chunk's payload (written by k_stress in sorted
+            // order) into shared memory: coalesced float4 loads
+            const long long i = sub + tid;
+            const unsigned key = i < n ? keys[i] : 0xffffffffu;
+            const bool valid = i < n && (key >> 6) == sbk;
+            if (valid) {
+                const float4 *src = w.payload + 5 * i;
                 const float4 q0 = src[0], q1 = src[1], q2 = src[2], q3 = src[3], q4 = src[4];
                 const int t = tid + (tid >> 5);
                 pay[0][t] = q0.x; pay[1][t] = q0.y; pay[2][t] = q0.z; pay[15][t] = q0.w;
@@ -559,6 +539,7 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const W
                 pay[10][t] = q3.x; pay[11][t] = q3.y; pay[12][t] = q3.z; pay[13][t] = q3.w;
                 pay[14][t] = q4.x;
                 regular[tid] = q4.y != 0.0f ? 1 : 0;
+                lcell[tid] = (unsigned char)(key & 63u);
                 if (q4.y != 0.0f) {   // the cubic weights of the cell's 5 node layers, once per particle
                     float e[5];
                     cw5(q0.x, e);
@@ -572,45 +553,59 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const W
                     for (int k = 0; k < 5; ++k) cwt[10 + k][t] = e[k];
                 }
             }
-            // runs of equal cell key inside the sub-chunk
-            int nruns;
+            // runs of equal cell key inside the chunk (ordered compaction), and
+            // the chunk's particle count (the valid lanes are a prefix)
+            int nruns, cnt;
             {
-                const int i = sub + tid;
-                const int flag = (tid < cnt && (tid == 0 || keys[i] != keys[i - 1])) ? 1 : 0;
-                nruns = compact_flags<1>(flag, runs, false, s_wcnt);   // also orders the payload writes
-                if (tid == 0) runs[nruns] = cnt;
+                const unsigned prev = (tid > 0 && i <= n) ? keys[i - 1] : 0xffffffffu;
+                const bool flag = valid && (tid == 0 || key != prev);
+                const unsigned fb = __ballot_sync(0xffffffffu, flag), vb = __ballot_sync(0xffffffffu, valid);
+                if (lane == 0) s_wcnt[wid] = (int)(__popc(fb) | (__popc(vb) << 16));
+                __syncthreads();
+                int pos = __popc(fb & lanemask_lt()), tot = 0, vt = 0;
+#pragma unroll
+                for (int w2 = 0; w2 < kP2GThreads / 32; ++w2) {
+                    const int c = s_wcnt[w2];
+                    pos += (w2 < wid) ? (c & 0xffff) : 0;
+                    tot += c & 0xffff;
+                    vt += c >> 16;
+                }
+                if (flag) runs[pos] = tid;
+                if (tid == 0) runs[tot] = vt;
+                nruns = tot;
+                cnt = vt;
                 __syncthreads();
             }
-            // ---------------- phase 2a: particles that need clamped nodes
-            if (tid < cnt && !regular[tid]) {
+            // ---------------- particles that need clamped nodes
+            if (valid && !regular[tid]) {
                 const int t = tid + (tid >> 5);
                 const float xp[3] = {pay[0][t], pay[1][t], pay[2][t]};   // positions for these particles
                 const float mv[3] = {pay[3][t], pay[4][t], pay[5][t]};
                 float aff[9];
 #pragma unroll
                 for (int k = 0; k < 9; ++k) aff[k] = pay[6 + k][t];
-                scatter_particle_global(xp, mv, aff, pay[15][t], pay[16][t], inv_dx, dx, ng, g_mom, g_dmg, bmask,
-                                        nbs);
+                scatter_particle_global(xp, mv, aff, pay[15][t], pay[16][t], inv_dx, dx, ng, scl, g_mom, g_dmg,
+                                        bmask, nbs);
             }
-            // ---------------- phase 2b: (cell, slab) items into the tiles
-            // items 0 .. 3*nruns-1 are quadratic x-slabs, then 5*nruns cubic x-slabs,
+            // ---------------- (cell, slab) items into the tiles: items
+            // 0 .. 3*nruns-1 are quadratic x-slabs, then 5*nruns cubic x-slabs,
             // so a warp mostly runs one kind
             for (int it = tid; it < nruns * 8; it += kP2GThreads) {
                 const bool quad = it < 3 * nruns;
                 const int r = quad ? it / 3 : (it - 3 * nruns) / 5;
                 const int sl = quad ? it - 3 * r : 3 + (it - 3 * nruns - 5 * r);
                 const int ja = runs[r], jb = runs[r + 1];
-                const unsigned key = keys[sub + ja];
-                const int cq[3] = {(int)((key >> 6) & 7), (int)((key >> 3) & 7), (int)(key & 7)};  // cell in block
+                int cq[3];
+                morton_decode(lcell[ja], cq);                    // cell inside the sub-block
                 if (sl < 3) {
                     const int ox = sl;
                     float acc[3][3][4];
 #pragma unroll
-                    for (int i = 0; i < 3; ++i)
+                    for (int i2 = 0; i2 < 3; ++i2)
 #pragma unroll
                         for (int j = 0; j < 3; ++j)
 #pragma unroll
-                            for (int c = 0; c < 4; ++c) acc[i][j][c] = 0.0f;
+                            for (int c = 0; c < 4; ++c) acc[i2][j][c] = 0.0f;
                     for (int j = ja; j < jb; ++j) {
                         if (!regular[j]) continue;
                         const int t = j + (j >> 5);
@@ -627,12 +622,12 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const W
                             az[c] = pay[8 + 3 * c][t];
                         }
                         const float wxs = ox == 0 ? wx[0] : (ox == 1 ? wx[1] : wx[2]);
-                        float bz[3][3];   // mv + aff (dpos_x, ., dpos_z) for each oz
+                        float bz3[3][3];   // mv + aff (dpos_x, ., dpos_z) for each oz
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
                             const float dz = ((float)oz - fx2) * dx;
 #pragma unroll
-                            for (int c = 0; c < 3; ++c) bz[oz][c] = base[c] + az[c] * dz;
+                            for (int c = 0; c < 3; ++c) bz3[oz][c] = base[c] + az[c] * dz;
                         }
 #pragma unroll
                         for (int oy = 0; oy < 3; ++oy) {
@@ -643,7 +638,7 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const W
                             for (int oz = 0; oz < 3; ++oz) {
                                 const float wk = wxy * wz[oz];
 #pragma unroll
-                                for (int c = 0; c < 3; ++c) acc[oy][oz][c] += wk * (bz[oz][c] + ady[c]);
+                                for (int c = 0; c < 3; ++c) acc[oy][oz][c] += wk * (bz3[oz][c] + ady[c]);
                                 acc[oy][oz][3] += wk * m;
                             }
                         }
@@ -654,17 +649,18 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const W
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
                             const int idx = (nx * kQE + cq[1] + oy) * kQE + cq[2] + oz;
-#pragma unroll
-                            for (int c = 0; c < 4; ++c)
-                                if (acc[oy][oz][c] != 0.0f) atomicAdd(&qt[c * kQN + idx], acc[oy][oz][c]);
+                            tile_add(&qt[idx], acc[oy][oz][0], scl[0]);
+                            tile_add(&qt[kQN + idx], acc[oy][oz][1], scl[0]);
+                            tile_add(&qt[2 * kQN + idx], acc[oy][oz][2], scl[0]);
+                            tile_add(&qt[3 * kQN + idx], acc[oy][oz][3], scl[1]);
                         }
                 } else {
                     const int nxs = sl - 3;
                     float adc[5][5], adw[5][5];
 #pragma unroll
-                    for (int i = 0; i < 5; ++i)
+                    for (int i2 = 0; i2 < 5; ++i2)
 #pragma unroll
-                        for (int j = 0; j < 5; ++j) adc[i][j] = adw[i][j] = 0.0f;
+                        for (int j = 0; j < 5; ++j) adc[i2][j] = adw[i2][j] = 0.0f;
                     for (int j = ja; j < jb; ++j) {
                         if (!regular[j]) continue;
                         const int t = j + (j >> 5);
@@ -687,64 +683,58 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_scatter(const SC sc, const W
                             }
                         }
                     }
-                    // cubic tile origin is 8b - 1, the cell's 5 nodes start at qb - 1
+                    // cubic tile origin is 4s - 1, the cell's 5 nodes start at qb - 1
                     const int nx = cq[0] + nxs;
 #pragma unroll
                     for (int ny = 0; ny < 5; ++ny)
 #pragma unroll
                         for (int nz = 0; nz < 5; ++nz) {
                             const int idx = (nx * kCE + cq[1] + ny) * kCE + cq[2] + nz;
-                            if (adc[ny][nz] != 0.0f) atomicAdd(&ct[idx], adc[ny][nz]);
-                            if (adw[ny][nz] != 0.0f) atomicAdd(&ct[kCN + idx], adw[ny][nz]);
+                            tile_add(&ct[idx], adc[ny][nz], scl[2]);
+                            tile_add(&ct[kCN + idx], adw[ny][nz], scl[3]);
                         }
                 }
             }
             __syncthreads();
+            if (cnt < kSub) break;                              // uniform: the last chunk of the sub-block
         }
-        // ---------------- flush: one vector atomic per touched node, and mark
-        // the touched 4^3 node blocks (tile nodes span blocks [2b-1, 2b+2] per
-        // axis; s_bmark is indexed from 2b-1)
-        if (tid < 64) s_bmark[tid] = 0;
-        __syncthreads();
-        {   // quadratic footprint: local nodes [cmin, cmin + cext + 2) per axis
-            const int ex = cext[0] + 2, ey = cext[1] + 2, ez = cext[2] + 2;
-            const FastDiv fyz = make_fastdiv(ey * ez), fz = make_fastdiv(ez);
-            for (int i = tid; i < ex * ey * ez; i += kP2GThreads) {
-                const int ix = fdiv(i, fyz), r = i - ix * fyz.d, iy = fdiv(r, fz);
-                const int tx = cmin[0] + ix, ty = cmin[1] + iy, tz = cmin[2] + r - iy * fz.d;
-                const int li = (tx * kQE + ty) * kQE + tz;
-                const float a0 = qt[li], a1 = qt[kQN + li], a2 = qt[2 * kQN + li], a3 = qt[3 * kQN + li];
-                if (a0 != 0.0f || a1 != 0.0f || a2 != 0.0f || a3 != 0.0f) {
-                    qt[li] = 0.0f; qt[kQN + li] = 0.0f; qt[2 * kQN + li] = 0.0f; qt[3 * kQN + li] = 0.0f;
-                    const int gx = org[0] + tx, gy = org[1] + ty, gz = org[2] + tz;   // in the grid: regular nodes only
-                    atomicAdd(&g_mom[((long long)gx * ng + gy) * ng + gz], make_float4(a0, a1, a2, a3));
-                    s_bmark[(((tx >> 2) + 1) * 4 + ((ty >> 2) + 1)) * 4 + ((tz >> 2) + 1)] = 1;   // node 8b+t: block 2b+(t>>2)
-                }
+        // ---------------- flush: one atomic per touched node and component, and
+        // mark the touched 4^3 grid blocks.  Quadratic node 4s+l lies in grid
+        // block s+(l>>2), cubic node 4s-1+l in block s-1+((l+3)>>2), sub-block s
+        // being grid block s; s_bmark is indexed from s-1 per axis.
+        for (int li = tid; li < kQN; li += kP2GThreads) {
+            const long long q0 = qt[li], q1 = qt[kQN + li], q2 = qt[2 * kQN + li], q3 = qt[3 * kQN + li];
+            if ((q0 | q1 | q2 | q3) != 0) {
+                qt[li] = 0; qt[kQN + li] = 0; qt[2 * kQN + li] = 0; qt[3 * kQN + li] = 0;
+                const int tx = li / (kQE * kQE), ty = (li / kQE) % kQE, tz = li % kQE;
+                long long *g = g_mom + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
+                if (q0) atomicAdd((unsigned long long *)g, (unsigned long long)q0);
+                if (q1) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q1);
+                if (q2) atomicAdd((unsigned long long *)(g + 2), (unsigned long long)q2);
+                if (q3) atomicAdd((unsigned long long *)(g + 3), (unsigned long long)q3);
+                s_bmark[(((tx >> 2) + 1) * 3 + ((ty >> 2) + 1)) * 3 + ((tz >> 2) + 1)] = 1;
             }
         }
-        {   // cubic footprint: local nodes [cmin, cmin + cext + 4) per axis (tile origin 8b-1)
-            const int ex = cext[0] + 4, ey = cext[1] + 4, ez = cext[2] + 4;
-            const FastDiv fyz = make_fastdiv(ey * ez), fz = make_fastdiv(ez);
-            for (int i = tid; i < ex * ey * ez; i += kP2GThreads) {
-                const int ix = fdiv(i, fyz), r = i - ix * fyz.d, iy = fdiv(r, fz);
-                const int tx = cmin[0] + ix, ty = cmin[1] + iy, tz = cmin[2] + r - iy * fz.d;
-                const int li = (tx * kCE + ty) * kCE + tz;
-                const float a4 = ct[li], a5 = ct[kCN + li];
-                if (a4 != 0.0f || a5 != 0.0f) {
-                    ct[li] = 0.0f; ct[kCN + li] = 0.0f;
-                    const int gx = org[0] - 1 + tx, gy = org[1] - 1 + ty, gz = org[2] - 1 + tz;
-                    atomicAdd(&g_dmg[((long long)gx * ng + gy) * ng + gz], make_float2(a4, a5));
-                    s_bmark[(((tx + 3) >> 2) * 4 + ((ty + 3) >> 2)) * 4 + ((tz + 3) >> 2)] = 1;   // node 8b-1+t: block 2b-1+((t+3)>>2)
-                }
+        for (int li = tid; li < kCN; li += kP2GThreads) {
+            const long long q0 = ct[li], q1 = ct[kCN + li];
+            if ((q0 | q1) != 0) {
+                ct[li] = 0; ct[kCN + li] = 0;
+                const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
+                long long *g = g_dmg + 2 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
+                                            (org[2] - 1 + tz));
+                if (q0) atomicAdd((unsigned long long *)g, (unsigned long long)q0);
+                if (q1) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q1);
+                s_bmark[(((tx + 3) >> 2) * 3 + ((ty + 3) >> 2)) * 3 + ((tz + 3) >> 2)] = 1;
             }
         }
         __syncthreads();
-        if (tid < 64 && s_bmark[tid]) {
-            const int bxx = 2 * bx - 1 + (tid >> 4), byy = 2 * by - 1 + ((tid >> 2) & 3), bzz = 2 * bz - 1 + (tid & 3);
+        if (tid < 27 && s_bmark[tid]) {
+            s_bmark[tid] = 0;
+            const int sbx = org[0] >> 2, sby = org[1] >> 2, sbz = org[2] >> 2;   // the sub-block's grid block
+            const int bxx = sbx - 1 + tid / 9, byy = sby - 1 + (tid / 3) % 3, bzz = sbz - 1 + tid % 3;
             if (bxx >= 0 && byy >= 0 && bzz >= 0 && bxx < nbs && byy < nbs && bzz < nbs)
                 bmask[((long long)bxx * nbs + byy) * nbs + bzz] = 1;
         }
-        __syncthreads();
     }
 }
 
@@ -773,23 +763,37 @@ void prepare_p2g() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(k_scatter<PlainScenes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
-        cudaFuncSetAttribute(k_scatter<BatchScenes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        cudaFuncSetAttribute(k_p2g_tiles<PlainScenes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        cudaFuncSetAttribute(k_p2g_tiles<BatchScenes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
         done[dev] = 1;
     }
 }
 
+// Persistent P2G CTAs: every resident slot of the device (work items are
+// taken from the list dynamically); `ctas_per_sm` caps the CTAs per SM (0: as
+// many as fit).
 template <class SC>
-void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int range) {
+void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int ctas_per_sm) {
     if (P.n <= 0) return;
-    k_stress<SC><<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(sc, P, w);
     prepare_p2g();
-    // small fixed ranges let the hardware scheduler balance CTAs whose segment
-    // structure differs (measured: 512 beats one balanced wave by 18% at 1M)
-    if (range <= 0) range = kP2GDefaultRange;
-    range = std::max(64, std::min(range, kP2GMaxRange)) / 32 * 32;
-    const long long blocks = (P.n + range - 1) / range;
-    k_scatter<SC><<<(unsigned)blocks, kP2GThreads, kP2GSmem, s>>>(sc, w, P.n, range);
+    const int lb = (int)std::min<long long>((P.n + 255) / 256, 148LL * 8);
+    k_subblocks<<<lb, 256, 0, s>>>(w.sorted_keys, P.n, w.work, w.ctrl);
+    k_stress<SC><<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(sc, P, w);
+    static int slots_dev[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int slots = (dev >= 0 && dev < 64) ? slots_dev[dev] : 0;
+    if (slots <= 0) {
+        slots = resident_slots((const void *)k_p2g_tiles<SC>, kP2GThreads, kP2GSmem);
+        if (dev >= 0 && dev < 64) slots_dev[dev] = slots;
+    }
+    if (ctas_per_sm > 0) {   // the tunable
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        slots = std::min(slots, sms * ctas_per_sm);
+    }
+    const long long blocks = std::min<long long>(slots, (P.n + 63) / 64);
+    k_p2g_tiles<SC><<<(unsigned)std::max<long long>(1, blocks), kP2GThreads, kP2GSmem, s>>>(sc, w, P.n);
 }
 template void launch_p2g<PlainScenes>(const PlainScenes &, const Parts &, const WS &, cudaStream_t, int);
 template void launch_p2g<BatchScenes>(const BatchScenes &, const Parts &, const WS &, cudaStream_t, int);

@@ -56,7 +56,7 @@ def bin_sort(x: Tensor, n_grid: int, inv_dx: float) -> Tuple[Tensor, Tensor]:
     if x.stride(0) != 1:
         x = x.t().contiguous().t()
     ps = x.stride(1)
-    need = _lib.workspace_size(n, n_grid)
+    need = _lib.bin_workspace_size(n, n_grid)   # the sort buffers only, no grids
     ws = torch.empty(need, dtype=torch.uint8, device=x.device)
     keys = torch.empty(n, dtype=torch.int32, device=x.device)
     perm = torch.empty(n, dtype=torch.int32, device=x.device)

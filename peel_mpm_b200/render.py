@@ -38,13 +38,18 @@ class Camera:
 
     def _struct(self):
         # R and T live on the device; their host copy is read back only when a
-        # tensor is replaced or modified in place (identity and version
-        # counter), so rendering a sequence of frames does not synchronise
-        key = (id(self.R), self.R._version, id(self.T), self.T._version)
-        if getattr(self, "_rt_key", None) != key:
-            self._rt_host = (self.R.detach().cpu().numpy().reshape(-1).tolist(),
-                             self.T.detach().cpu().numpy().reshape(-1).tolist())
-            self._rt_key = key
+        # tensor is replaced (the cache holds the tensor objects themselves and
+        # compares identity), modified in place (version counter) or given new
+        # storage through .data (data pointer), so rendering a sequence of
+        # frames does not synchronise
+        cached = getattr(self, "_rt_cache", None)
+        R, T = self.R, self.T
+        fresh = cached is not None and cached[0] is R and cached[1] is T and \
+            cached[2] == (R._version, T._version, R.data_ptr(), T.data_ptr())
+        if not fresh:
+            self._rt_host = (R.detach().cpu().numpy().reshape(-1).tolist(),
+                             T.detach().cpu().numpy().reshape(-1).tolist())
+            self._rt_cache = (R, T, (R._version, T._version, R.data_ptr(), T.data_ptr()))
         c = _lib.pm_camera()
         for k, v in enumerate(self._rt_host[0]):
             c.R[k] = v
@@ -112,14 +117,21 @@ def carry_gaussians(sim, bind, off0, cov0, color0, sim_to_world=None, crack_tint
     ``sim_to_world`` is ``(A (3,3), t (3,))``, a (3, 4) device tensor from
     ``world_map`` (no host-to-device copy per call), or None (identity).
     ``check_bind`` range-checks the bindings, which synchronises the host once;
-    a caller that checked them already passes False (an out-of-range id then
-    gives NaN outputs)."""
+    a caller that checked them already passes False together with ``bind`` as
+    an int32 tensor on the solver's device (an out-of-range id then gives NaN
+    outputs; a wider integer type is rejected on that path, since narrowing
+    it unchecked could wrap an id into range).  Arrays given as numpy are
+    copied to the device on every call: keep ``off0``, ``cov0`` and ``color0``
+    as device tensors for per-frame use."""
     dev = sim.device
     f32 = lambda a: torch.as_tensor(a, device=dev).to(torch.float32).contiguous()
     bind = torch.as_tensor(bind, device=dev)
     g = bind.shape[0]
-    if check_bind and g and (int(bind.min()) < 0 or int(bind.max()) >= sim.n):   # torch indexing would raise too
-        raise IndexError(f"gaussian bindings must lie in [0, {sim.n})")
+    if check_bind:
+        if g and (int(bind.min()) < 0 or int(bind.max()) >= sim.n):   # torch indexing would raise too
+            raise IndexError(f"gaussian bindings must lie in [0, {sim.n})")
+    elif bind.dtype != torch.int32:
+        raise TypeError("with check_bind=False, bind must be an int32 tensor (ids checked by the caller)")
     bind = bind.to(torch.int32).contiguous()
     off0, cov0, color0 = f32(off0), f32(cov0).reshape(-1, 9), f32(color0)
     if off0.shape != (g, 3) or cov0.shape != (g, 9) or color0.shape != (g, 3):

@@ -1,9 +1,13 @@
 """Generate golden fixtures by running the reference solver itself.
 
-Run in a container where the reference checkout is mounted (it is read, never
-written):
+Run where a checkout of the reference is available (it is read, never
+written); its ``anisompm_py/src`` directory is given by ``--ref`` or by the
+environment variable PEELMPM_REFERENCE_SRC:
 
-    python tests/golden/make_golden.py [--ref /root/reference/anisompm_py/src]
+    python tests/golden/make_golden.py --ref <checkout>/anisompm_py/src [--part all|sweeps]
+
+``--part sweeps`` writes only ``reference_sym_eig_sweeps.npz``: the reference
+``sym_eig`` at sweep counts other than the default 5.
 
 For each seeded scene of ``peel_mpm_b200.scenes`` the reference ``AnisoMPM``
 (anisompm.py:303-807) runs on the CPU in float32 (and float64 where listed),
@@ -160,6 +164,24 @@ def sym_eig_golden(mod, out, n=4096, seed=0):
     out["sym_eig/evecs"] = V.numpy()
 
 
+SWEEP_COUNTS = (0, 1, 3, 7, 12)
+
+
+def sym_eig_sweeps_golden(mod, out, n=2048, seed=3):
+    """The reference sym_eig with `sweeps` other than 5 (anisompm.py:48, 68)."""
+    g = torch.Generator().manual_seed(seed)
+    B = torch.randn(n, 3, 3, generator=g, dtype=torch.float64)
+    A = 0.5 * (B + B.transpose(1, 2))
+    A[0] = torch.diag(torch.tensor([2.0, 2.0, 5.0], dtype=torch.float64))
+    A[1] = torch.tensor([[0.0, 2, 0], [2, 0, 0], [0, 0, 0]], dtype=torch.float64)
+    A32 = A.to(torch.float32)
+    out["sym_eig_sweeps/A"] = A32.numpy()
+    for k in SWEEP_COUNTS:
+        ev, V = mod.sym_eig(A32, sweeps=k)
+        out[f"sym_eig_sweeps/{k}/evals"] = ev.numpy()
+        out[f"sym_eig_sweeps/{k}/evecs"] = V.numpy()
+
+
 def bin_golden(mod, out):
     for name in ("plain_small", "tiny_bar"):
         sc = scenes.SCENES[name]()
@@ -176,13 +198,23 @@ def bin_golden(mod, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/anisompm_py/src")
+    ap.add_argument("--ref", default=os.environ.get("PEELMPM_REFERENCE_SRC"),
+                    help="the reference's anisompm_py/src directory (default: $PEELMPM_REFERENCE_SRC)")
     ap.add_argument("--skip-noise", action="store_true")
+    ap.add_argument("--part", default="all", choices=["all", "sweeps"])
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set PEELMPM_REFERENCE_SRC")
     sys.path.insert(0, args.ref)
     import anisompm as mod  # the reference solver, unmodified
 
     torch.set_num_threads(os.cpu_count() or 1)
+    if args.part == "sweeps":
+        out = {}
+        sym_eig_sweeps_golden(mod, out)
+        np.savez_compressed(os.path.join(HERE, "reference_sym_eig_sweeps.npz"), **out)
+        print("wrote", len(out), "arrays")
+        return
     out = {}
     meta = {"torch": torch.__version__, "numpy": np.__version__, "scenes": {}}
     for name, (s32, s64, stride, diag) in PLAN.items():

@@ -1,8 +1,10 @@
 """Golden gradients from the reference solver's own PyTorch autograd.
 
-Run where the reference checkout is mounted (it is read, never written):
+Run where a checkout of the reference is available (it is read, never
+written); its ``anisompm_py/src`` directory is given by ``--ref`` or by the
+environment variable PEELMPM_REFERENCE_SRC:
 
-    python tests/golden/make_grad_golden.py [--ref /root/reference/anisompm_py/src]
+    python tests/golden/make_grad_golden.py --ref <checkout>/anisompm_py/src
 
 For each case the reference ``AnisoMPM`` (anisompm.py:303-807) runs on the
 CPU in float64 with per-particle Young's modulus E, fiber directions,
@@ -153,9 +155,12 @@ def onestep(mod, name, factory, pre_steps, out, meta, tag):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/anisompm_py/src")
+    ap.add_argument("--ref", default=os.environ.get("PEELMPM_REFERENCE_SRC"),
+                    help="the reference's anisompm_py/src directory (default: $PEELMPM_REFERENCE_SRC)")
     ap.add_argument("--out", default=os.path.join(HERE, "reference_grads.npz"))
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set PEELMPM_REFERENCE_SRC")
     sys.path.insert(0, args.ref)
     import anisompm as mod  # the unmodified reference module
     mod.sym_eig = guarded_sym_eig

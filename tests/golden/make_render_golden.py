@@ -1,8 +1,10 @@
 """Golden images from the reference's own Gaussian-splat renderer.
 
-Run where the reference checkout is mounted (it is read, never written):
+Run where a checkout of the reference is available (it is read, never
+written); its ``anisompm_py/src`` directory is given by ``--ref`` or by the
+environment variable PEELMPM_REFERENCE_SRC:
 
-    python tests/golden/make_render_golden.py [--ref /root/reference/anisompm_py/src]
+    python tests/golden/make_render_golden.py --ref <checkout>/anisompm_py/src
 
 The reference ``render_gaussians`` (render.py:71-162: EWA projection, soft
 z-buffer in two passes, coverage compositing) renders seeded synthetic
@@ -56,9 +58,12 @@ CASES = {
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/anisompm_py/src")
+    ap.add_argument("--ref", default=os.environ.get("PEELMPM_REFERENCE_SRC"),
+                    help="the reference's anisompm_py/src directory (default: $PEELMPM_REFERENCE_SRC)")
     ap.add_argument("--out", default=os.path.join(HERE, "reference_render.npz"))
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set PEELMPM_REFERENCE_SRC")
     sys.path.insert(0, args.ref)
     import render as ref   # the unmodified reference module
     out = {}

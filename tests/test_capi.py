@@ -39,12 +39,16 @@ def test_abi_version():
 def test_workspace_layout_is_aligned_and_disjoint(n, ng):
     L = _lib.workspace_layout(n, ng)
     offs = [L.ctrl, L.keys_a, L.keys_b, L.vals_a, L.vals_b, L.hist, L.block_mask, L.block_list, L.g_mom, L.g_dmg,
-            L.g_vel, L.g_gd, L.payload, L.inv_perm, L.total]
+            L.g_vel, L.g_gd, L.payload, L.inv_perm, L.work, L.total]
     assert all(o % 256 == 0 for o in offs)
     assert offs == sorted(offs) and len(set(offs)) == len(offs)
     nn = max(n, 1)
     G = ng ** 3
-    assert L.keys_b - L.keys_a >= 4 * nn and L.g_dmg - L.g_mom >= 16 * G and L.payload - L.g_gd >= 4 * G and L.inv_perm - L.payload >= 80 * nn and L.total - L.inv_perm >= 4 * nn
+    # int64 fixed-point accumulators: 4 per node for momentum and mass, 2 for the damage sums
+    assert L.keys_b - L.keys_a >= 4 * nn and L.g_dmg - L.g_mom >= 32 * G and L.g_vel - L.g_dmg >= 16 * G
+    assert L.payload - L.g_gd >= 4 * G and L.inv_perm - L.payload >= 80 * nn and L.work - L.inv_perm >= 4 * nn
+    assert L.total - L.work >= 4 * nn
+    assert _lib.bin_workspace_size(n, ng) == L.block_mask
     key_bits = max(max(_bits(ng ** 3), 1), _bits(((ng + 7) // 8) ** 3) + 9)
     assert L.sort_passes == _radix_passes(key_bits)
     assert _lib.workspace_size(n, ng) == L.total
@@ -91,11 +95,11 @@ def test_batch_layout_packs_scenes(ns, gs):
     assert L.ws.sort_passes == _radix_passes(_bits(L.n_sort_blocks) + 9)
     w = L.ws
     offs = [w.ctrl, w.keys_a, w.keys_b, w.vals_a, w.vals_b, w.hist, w.block_mask, w.block_list, w.g_mom, w.g_dmg,
-            w.g_vel, w.g_gd, w.payload, w.inv_perm, L.params, L.tables, w.total]
+            w.g_vel, w.g_gd, w.payload, w.inv_perm, w.work, L.params, L.tables, w.total]
     assert all(o % 256 == 0 for o in offs)
     assert offs == sorted(offs) and len(set(offs)) == len(offs)
     assert w.keys_a - w.ctrl >= 224 * len(ns)                      # one control block per scene
-    assert w.g_dmg - w.g_mom >= 16 * L.n_nodes and w.block_list - w.block_mask >= L.n_grid_blocks
+    assert w.g_dmg - w.g_mom >= 32 * L.n_nodes and w.block_list - w.block_mask >= L.n_grid_blocks
     assert L.tables - L.params >= C.sizeof(_lib.pm_params) * len(ns)
     assert w.total - L.tables >= 5 * 8 * (len(ns) + 1)
     assert _lib.batch_workspace_size(ns, gs) == w.total

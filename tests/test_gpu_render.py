@@ -79,9 +79,12 @@ def test_carried_gaussians_match_torch_restatement():
     assert torch.allclose(col, col_ref, rtol=1e-6, atol=1e-7)
     # the same map prepared once on the device, bindings not re-checked: identical
     from peel_mpm_b200.render import world_map
-    p2, c2, k2 = carry_gaussians(sim, bind, off0, cov0, col0, world_map(A, t, "cuda:0"), crack_tint=0.7,
-                                 check_bind=False)
+    p2, c2, k2 = carry_gaussians(sim, bind.to(torch.int32), off0, cov0, col0, world_map(A, t, "cuda:0"),
+                                 crack_tint=0.7, check_bind=False)
     assert torch.equal(p2, pos) and torch.equal(c2, cov) and torch.equal(k2, col)
+    # unchecked ids must already be int32: a wider type could wrap into range when narrowed
+    with pytest.raises(TypeError):
+        carry_gaussians(sim, bind, off0, cov0, col0, world_map(A, t, "cuda:0"), check_bind=False)
 
 
 def test_carry_rejects_unbound_gaussians():

@@ -16,6 +16,11 @@ def test_camera_struct_follows_in_place_and_replaced_R_T():
     assert list(c._struct().T) == [0.5, 0.5, 0.5]
     c.R = torch.diag(torch.tensor([2.0, 3.0, 4.0]))   # replaced
     assert list(c._struct().R) == [2, 0, 0, 0, 3, 0, 0, 0, 4]
+    c.R.data = torch.diag(torch.tensor([5.0, 6.0, 7.0]))   # new storage behind the same tensor
+    assert list(c._struct().R) == [5, 0, 0, 0, 6, 0, 0, 0, 7]
+    del c.R                                                # a replacement that may reuse a freed id
+    c.R = torch.eye(3) * 9.0
+    assert list(c._struct().R) == [9, 0, 0, 0, 9, 0, 0, 0, 9]
 
 
 def test_world_map_layout():

@@ -32,8 +32,10 @@ def _static_bin(x_planes, n_grid, inv_dx):
     return rc, keys, perm
 
 
-@pytest.mark.parametrize("n_grid", [128, 36])
+@pytest.mark.parametrize("n_grid", [128, 36, 1024])
 def test_static_binning_matches_workspace_binning_on_two_calls(n_grid):
+    # the grids give keys of 21, 16 and 30 bits: 3, 2 and 4 radix passes, so
+    # the result ends in either half of the static scratch
     # two calls in a row on different inputs: the second reuses the scratch the
     # first left behind and must still match the workspace entry point exactly
     for seed, n in ((11, 200_003), (12, _lib.PM_BIN_STATIC_MAX_N)):
