@@ -119,7 +119,8 @@ typedef struct pm_particles {
 /* Device-side status counters (a copy is read back by pm_read_status). */
 typedef struct pm_status_info {
     uint32_t nonfinite;              /* particles whose new x or F is not finite (sticky) */
-    uint32_t tile_fallbacks;         /* P2G CTAs that scattered straight to global memory */
+    uint32_t dense_subblocks;        /* 4^3-cell sub-blocks of more than 16,383 particles: their grid
+                                        nodes may exceed the exact fixed-point sums' headroom */
     uint32_t n_active_blocks;        /* active 4^3 grid blocks in the last substep */
     int32_t any_allow;               /* allow.any() seen by the last substep */
 } pm_status_info;

@@ -69,7 +69,7 @@ class pm_particles(C.Structure):
 
 
 class pm_status_info(C.Structure):
-    _fields_ = [("nonfinite", C.c_uint32), ("tile_fallbacks", C.c_uint32), ("n_active_blocks", C.c_uint32),
+    _fields_ = [("nonfinite", C.c_uint32), ("dense_subblocks", C.c_uint32), ("n_active_blocks", C.c_uint32),
                 ("any_allow", C.c_int32)]
 
 

@@ -569,15 +569,19 @@ class AnisoMPM:
             _lib.check(self._lib.pm_read_status(self._ws.data_ptr(), self._ws_bytes, self.n, self.n_grid,
                                                 C.byref(info), torch.cuda.current_stream().cuda_stream),
                        "pm_read_status")
-        return {"nonfinite": int(info.nonfinite), "tile_fallbacks": int(info.tile_fallbacks),
+        return {"nonfinite": int(info.nonfinite), "dense_subblocks": int(info.dense_subblocks),
                 "n_active_blocks": int(info.n_active_blocks), "any_allow": int(info.any_allow)}
 
     def check(self):
         """Raise if any particle's position or deformation gradient went
-        non-finite since the workspace was created."""
+        non-finite since the workspace was created, or if a 4^3-cell
+        sub-block held more particles than the exact grid sums allow for
+        (16,383: about 256 per cell)."""
         st = self.status()
         if st["nonfinite"]:
             raise FloatingPointError(f"{st['nonfinite']} particle updates produced non-finite x or F")
+        if st["dense_subblocks"]:
+            raise OverflowError(f"{st['dense_subblocks']} P2G sub-blocks exceeded the fixed-point headroom")
         return st
 
 

@@ -257,7 +257,8 @@ class BatchedAnisoMPM:
         st = torch.cuda.current_stream(self.device).cuda_stream
         _lib.check(self._lib.pm_batch_read_status(self._ws.data_ptr(), self._ws_bytes, S, self._n_arr, self._g_arr,
                                                   out, st), "pm_batch_read_status")
-        return [{"nonfinite": int(o.nonfinite), "n_active_blocks": int(o.n_active_blocks),
+        return [{"nonfinite": int(o.nonfinite), "dense_subblocks": int(o.dense_subblocks),
+                 "n_active_blocks": int(o.n_active_blocks),
                  "any_allow": int(o.any_allow)} for o in out]
 
     def check(self):
@@ -265,6 +266,9 @@ class BatchedAnisoMPM:
         bad = [k for k, s in enumerate(st) if s["nonfinite"]]
         if bad:
             raise FloatingPointError(f"scenes {bad} produced non-finite x or F")
+        dense = [k for k, s in enumerate(st) if s["dense_subblocks"]]
+        if dense:
+            raise OverflowError(f"scenes {dense} exceeded the fixed-point headroom of their P2G sub-blocks")
         return st
 
 

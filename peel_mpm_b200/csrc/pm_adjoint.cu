@@ -262,10 +262,10 @@ __device__ __noinline__ void adj_scatter_global(const float xp[3], const float v
             for (int oz = 0; oz < 4; ++oz) {
                 const float wk = wxy * wq[2][oz];
                 long long *g = acc + 4 * (row + clampi(c.b[2] + oz, 0, ng - 1));
-                tile_add(g, wk * (b0 + U[2][oz][0]), smom);
-                tile_add(g + 1, wk * (b1 + U[2][oz][1]), smom);
-                tile_add(g + 2, wk * (b2 + U[2][oz][2]), smom);
-                tile_add(g + 3, ab * c.w[oz][2] + e * c.w2[oz][2], slap);
+                red_fix(g, wk * (b0 + U[2][oz][0]), smom);
+                red_fix(g + 1, wk * (b1 + U[2][oz][1]), smom);
+                red_fix(g + 2, wk * (b2 + U[2][oz][2]), smom);
+                red_fix(g + 3, ab * c.w[oz][2] + e * c.w2[oz][2], slap);
             }
         }
 }
@@ -1010,7 +1010,7 @@ __device__ __forceinline__ void adj_gather(const float xp[3], float inv_dx, floa
 // the gather state live.  The output adjoint of F is written in two parts:
 // (I + dt C')^T Fbar' before the gathers, the constitutive part added at the
 // end (same thread, same address).
-__global__ void __launch_bounds__(128, 3) k_adj_particle(const pm_params prm, const Parts pre, const Parts post,
+__global__ void __launch_bounds__(128, 4) k_adj_particle(const pm_params prm, const Parts pre, const Parts post,
                                                          const pm_state_adj ain, const pm_state_adj aout,
                                                          const pm_param_adj grads, const TapeHead *head,
                                                          const float4 *__restrict__ gvel,

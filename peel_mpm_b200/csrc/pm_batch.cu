@@ -281,7 +281,7 @@ int pm_batch_read_status(const void *ws, size_t ws_bytes, int32_t n_scenes, cons
         return pm::api_cuda_check("pm_batch_read_status");
     for (int i = 0; i < bp.S; ++i) {
         out[i].nonfinite = c[i].nonfinite;
-        out[i].tile_fallbacks = c[i].tile_fallbacks;
+        out[i].dense_subblocks = c[i].dense_subblocks;
         out[i].n_active_blocks = c[0].n_active;   // one counter for the whole batch
         out[i].any_allow = c[i].any_allow;
     }

@@ -396,7 +396,7 @@ int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, p
         cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
         return cuda_check("pm_read_status");
     out->nonfinite = c.nonfinite;
-    out->tile_fallbacks = c.tile_fallbacks;
+    out->dense_subblocks = c.dense_subblocks;
     out->n_active_blocks = c.n_active;
     out->any_allow = c.any_allow;
     return PM_OK;

@@ -46,7 +46,7 @@ struct Ctrl {
     int any_allow;
     unsigned n_active;
     unsigned nonfinite;
-    unsigned tile_fallbacks;
+    unsigned dense_subblocks;   // sub-blocks beyond the fixed-point headroom (status error)
     unsigned mom_bound, mass_bound, dmg_bound;
     unsigned n_work, work_next;
     unsigned pad_;
@@ -375,18 +375,22 @@ __device__ __forceinline__ unsigned blocked_key(const int b[3], int ng) {
 // depend on the order of the atomic additions: a substep is bit-reproducible
 // run to run, which the adjoint's checkpoint re-runs rely on.  The unit of a
 // quantity is 2^(e - kFixBits) with 2^e above the substep's bound on one
-// contribution; a node total then holds 2^(63 - kFixBits) worst-case
-// contributions before it could overflow, and every contribution is resolved
-// to 2^-kFixBits of the bound (far finer than its own float32 rounding).
-constexpr int kFixBits = 36;
+// contribution; a node total then holds 2^(63 - kFixBits) = 131,072
+// worst-case contributions before it could overflow (a node's contributions
+// come from at most 8 of the 4^3-cell sub-blocks, so the P2G kernel counts
+// sub-blocks of more than kDenseSubblock particles as a status error), and
+// every contribution is resolved to 2^-kFixBits of the bound: a node whose
+// sum is 1e-6 of the largest contribution still gets float32's precision.
+constexpr int kFixBits = 46;
+constexpr int kDenseSubblock = 16383;
 // Scale (2^(kFixBits - e)) and unit (its inverse) from a bound's float bits;
-// bounds below 2^-90 (including zero) or not finite use 2^-90 / 2^127.
+// bounds below 2^-75 (including zero) or not finite use 2^-75 / 2^127.
 struct FixScale {
     float scale, unit;
 };
 __device__ __forceinline__ FixScale fix_scale(unsigned bound_bits) {
     float b = __uint_as_float(bound_bits);
-    if (!(b >= 8.0779e-28f)) b = 8.0779e-28f;           // 2^-90; also NaN
+    if (!(b >= 2.6470e-23f)) b = 2.6470e-23f;           // 2^-75; also NaN
     if (!(b <= 1.0e38f)) b = 1.0e38f;
     const int e = (int)((__float_as_uint(b) >> 23) & 0xffu) - 126;   // 2^(e-1) <= b < 2^e
     FixScale f;
@@ -588,10 +592,26 @@ __device__ __forceinline__ void cw5_2(float fx, float e[5]) {
     e[4] = s1 ? w3 : 0.0f;
 }
 
-// Adds a float partial sum to an int64 fixed-point tile entry.
+// Adds a float partial sum to an int64 fixed-point entry of a shared-memory
+// tile.  The entry is held as two 32-bit words {lo, hi}: the low word takes a
+// native 32-bit atomic add (64-bit shared atomics are several times slower
+// on this part) and the carry out of it goes to the high word with the value's
+// upper half.  The number of carries over all additions equals the number of
+// times the low word wraps, whatever their order, so the pair holds the exact
+// 64-bit sum once every addition is done.
 __device__ __forceinline__ void tile_add(long long *t, float v, float scale) {
     const long long q = to_fix(v, scale);
-    if (q != 0) atomicAdd((unsigned long long *)t, (unsigned long long)q);
+    if (q == 0) return;
+    unsigned *w = (unsigned *)t;
+    const unsigned lo = (unsigned)q;
+    const unsigned old = atomicAdd(w, lo);
+    const unsigned hi = (unsigned)((unsigned long long)q >> 32) + ((old + lo) < old ? 1u : 0u);
+    if (hi != 0u) atomicAdd(w + 1, hi);
+}
+// The same for an entry in global memory: one 64-bit atomic.
+__device__ __forceinline__ void red_fix(long long *addr, float v, float scale) {
+    const long long q = to_fix(v, scale);
+    if (q != 0) atomicAdd((unsigned long long *)addr, (unsigned long long)q);
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {

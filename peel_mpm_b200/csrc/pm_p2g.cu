@@ -373,11 +373,6 @@ __device__ __forceinline__ void mark_node_block(unsigned char *mask, int nbs, in
     if (*m == 0) *m = 1;
 }
 
-__device__ __forceinline__ void red_fix(long long *addr, float v, float scale) {
-    const long long q = to_fix(v, scale);
-    if (q != 0) atomicAdd((unsigned long long *)addr, (unsigned long long)q);
-}
-
 __device__ __noinline__ void scatter_particle_global(const float xp[3], const float mv[3], const float aff[9],
                                                      float m, float d, float inv_dx, float dx, int ng,
                                                      const float sc[4], long long *g_mom, long long *g_dmg,
@@ -523,6 +518,7 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_p2g_tiles(const SC sc, const
                             by * kSortBlock + (int)((oct >> 1) & 1u) * kSubEdge,
                             bz * kSortBlock + (int)(oct & 1u) * kSubEdge};   // first cell of the sub-block
 
+        long long item_n = 0;                               // particles of the sub-block
         for (long long sub = a;; sub += kSub) {
             // ---------------- the chunk's payload (written by k_stress in sorted
             // order) into shared memory: coalesced float4 loads
@@ -574,6 +570,7 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_p2g_tiles(const SC sc, const
                 if (tid == 0) runs[tot] = vt;
                 nruns = tot;
                 cnt = vt;
+                item_n += vt;
                 __syncthreads();
             }
             // ---------------- particles that need clamped nodes
@@ -698,6 +695,9 @@ __global__ void __launch_bounds__(kP2GThreads, 3) k_p2g_tiles(const SC sc, const
             __syncthreads();
             if (cnt < kSub) break;                              // uniform: the last chunk of the sub-block
         }
+        // a sub-block denser than the fixed-point headroom allows: its nodes'
+        // sums are not guaranteed exact; counted for the status
+        if (tid == 0 && item_n > kDenseSubblock) atomicAdd(&w.ctrl[sid].dense_subblocks, 1u);
         // ---------------- flush: one atomic per touched node and component, and
         // mark the touched 4^3 grid blocks.  Quadratic node 4s+l lies in grid
         // block s+(l>>2), cubic node 4s-1+l in block s-1+((l+3)>>2), sub-block s

