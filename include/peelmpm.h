@@ -77,8 +77,9 @@ typedef struct pm_params {
     double f_clamp_hi;
     int32_t n_grips;
     int32_t n_colliders;
-    int32_t p2g_ctas_per_sm;    /* resident P2G CTAs per SM (0: as many as fit, else 1..8); a tuning
-                                   knob with no effect on results (the grid sums are exact) */
+    int32_t p2g_ctas_per_sm;    /* resident P2G CTAs per SM (0: the 80-register build, as many as fit;
+                                   4 or more: the 64-register build at 4 per SM; 1..3: a cap); a
+                                   tuning knob with no effect on results (the grid sums are exact) */
     int32_t grid_ctas_per_sm;   /* grid-update CTAs per SM (0: the library default, else 1..64); a
                                    tuning knob with no effect on results */
     pm_grip grips[PM_MAX_GRIPS];

@@ -4,8 +4,9 @@ Two knobs shape the launches and never the results (the P2G grid sums are
 exact integers, the grid update is one thread per node row either way):
 
 * ``p2g_ctas_per_sm``: resident CTAs per SM of the persistent P2G kernel,
-  which takes 4^3-cell sub-blocks from a work list.  More CTAs hide more
-  latency; fewer leave each CTA more L1/shared-memory bandwidth.
+  which takes 4^3-cell sub-blocks from a work list (0: the 80-register build
+  at 3 per SM; 4: the 64-register build at 4 per SM).  More CTAs hide more
+  latency; fewer registers spill a little.
 * ``grid_ctas_per_sm``: CTAs per SM of the grid update over the active 4^3
   node blocks (a grid-stride cap; 0 gives every 4-node row its own thread).
 
@@ -24,7 +25,7 @@ from typing import Optional
 
 import torch
 
-P2G_CANDIDATES = (0, 1, 2, 3)          # 0: as many as fit (3 at the kernel's register and shared-memory use)
+P2G_CANDIDATES = (0, 2, 4)             # 0: as many as fit of the 80-register build (3 per SM)
 GRID_CANDIDATES = (0, 4, 8, 16, 32)    # 0: one thread per node row
 _CACHE: dict = {}
 

@@ -49,6 +49,7 @@ struct TapeHead {
 // contributions (float bits) and the dynamic work cursor.
 struct AdjCtrl {
     unsigned mom_bound, lap_bound, work_next, pad;
+    unsigned slots[2][kBoundSlots];   // per-warp-slot bounds, folded by k_adj_bounds
 };
 
 // Quadratic weights with their derivatives wrt the local coordinate fx.
@@ -214,8 +215,27 @@ __global__ void __launch_bounds__(256) k_adj_pre(const pm_params prm, const Part
     bmom = __reduce_max_sync(am, bmom);
     blap = __reduce_max_sync(am, blap);
     if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1)) {
-        atomicMax(&actl->mom_bound, bmom);
-        atomicMax(&actl->lap_bound, blap);
+        const int slot = (int)(((blockIdx.x << 3) + (threadIdx.x >> 5)) & (kBoundSlots - 1));
+        atomicMax(&actl->slots[0][slot], bmom);
+        atomicMax(&actl->slots[1][slot], blap);
+    }
+}
+
+__global__ void __launch_bounds__(kBoundSlots) k_adj_bounds(AdjCtrl *actl) {
+    __shared__ unsigned s_m[2][kBoundSlots / 32];
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+        const unsigned m = __reduce_max_sync(0xffffffffu, actl->slots[v][t]);
+        if ((t & 31) == 0) s_m[v][t >> 5] = m;
+    }
+    __syncthreads();
+    if (t < 2) {
+        unsigned m = 0u;
+#pragma unroll
+        for (int k = 0; k < kBoundSlots / 32; ++k) m = max(m, s_m[t][k]);
+        if (t == 0) actl->mom_bound = m;
+        else actl->lap_bound = m;
     }
 }
 
@@ -1292,6 +1312,7 @@ void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, c
     prepare_adjoint();
     cudaMemsetAsync(actl, 0, sizeof(AdjCtrl), s);
     k_adj_pre<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prm, pre, post, ain, (const int *)(b + T.iperm), apay, actl);
+    k_adj_bounds<<<1, kBoundSlots, 0, s>>>(actl);
     {
         static int slots_dev[64] = {0};
         int dev = 0;

@@ -33,13 +33,16 @@ __host__ __device__ inline int radix_passes(int key_bits) {
 constexpr int kG2PThreads = 256;     // G2P particles per CTA
 
 // Device control block: per-substep inputs and status counters.  The three
-// bounds are float bit patterns (non-negative floats order like their bits)
-// raised with atomicMax by the constitutive kernel: the largest magnitude of a
-// particle's momentum contribution to one node, of a particle mass and of a
-// particle damage; they fix the units of the grid's fixed-point accumulators
-// for the substep (see fix_scale).  n_work / work_next: the P2G work list of
-// non-empty 4^3-cell sub-blocks and its dynamic cursor (control block 0 of a
-// batch serves all scenes).
+// bounds are float bit patterns (non-negative floats order like their bits):
+// the largest magnitude of a particle's momentum contribution to one node, of
+// a particle mass and of a particle damage; they fix the units of the grid's
+// fixed-point accumulators for the substep (see fix_scale).  The constitutive
+// kernel raises them with atomicMax into kBoundSlots slots per quantity (warps
+// spread over the slots, so the atomics do not queue on one address) and a
+// one-block kernel folds the slots into the bounds.  n_work / work_next: the
+// P2G work list of non-empty 4^3-cell sub-blocks and its dynamic cursor
+// (control block 0 of a batch serves all scenes).
+constexpr int kBoundSlots = 128;
 struct Ctrl {
     double time;
     long long step;
@@ -52,6 +55,7 @@ struct Ctrl {
     unsigned pad_;
     float col_origin[PM_MAX_COLLIDERS][3];
     float col_vel[PM_MAX_COLLIDERS][3];
+    unsigned bound_slots[3][kBoundSlots];   // zero between substeps
 };
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -228,6 +232,7 @@ __device__ __forceinline__ int upper_index(const long long *a, int n, long long 
 struct PlainScenes {
     pm_params prm;
     static constexpr bool batched = false;
+    int count() const { return 1; }
     __device__ __forceinline__ int of_particle(long long) const { return 0; }
     __device__ __forceinline__ int of_sblock(unsigned) const { return 0; }
     __device__ __forceinline__ int of_gblock(long long) const { return 0; }
@@ -250,6 +255,7 @@ struct BatchScenes {
     const long long *ctab;        // first G2P CTA, [n + 1]
     int n;
     static constexpr bool batched = true;
+    int count() const { return n; }
     __device__ __forceinline__ int of_particle(long long p) const { return upper_index(pb, n, p); }
     __device__ __forceinline__ int of_sblock(unsigned b) const { return upper_index(sblk, n, (long long)b); }
     __device__ __forceinline__ int of_gblock(long long b) const { return upper_index(gblk, n, b); }
@@ -425,6 +431,36 @@ __device__ __forceinline__ void mmt3(const float *A, const float *B, float *Cm) 
 #pragma unroll
         for (int j = 0; j < 3; ++j)
             T[3 * i + j] = A[3 * i] * B[3 * j] + A[3 * i + 1] * B[3 * j + 1] + A[3 * i + 2] * B[3 * j + 2];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Cm[k] = T[k];
+}
+
+// The same products with every multiply and add rounded separately, k = 0,
+// 1, 2 in order, as the reference's float32 matrix products round them: for
+// updates applied to every particle every substep (the f_clamp rebuild of F,
+// whose near-identity factor V diag(Sc/S) V^T is I up to rounding) contraction
+// into FMAs would let F drift from the reference's by a rounding-level random
+// walk.
+__device__ __forceinline__ float dot3_rn(float a0, float b0, float a1, float b1, float a2, float b2) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1)), __fmul_rn(a2, b2));
+}
+__device__ __forceinline__ void mm3_rn(const float *A, const float *B, float *Cm) {
+    float T[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            T[3 * i + j] = dot3_rn(A[3 * i], B[j], A[3 * i + 1], B[3 + j], A[3 * i + 2], B[6 + j]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Cm[k] = T[k];
+}
+__device__ __forceinline__ void mmt3_rn(const float *A, const float *B, float *Cm) {   // A B^T
+    float T[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            T[3 * i + j] = dot3_rn(A[3 * i], B[3 * j], A[3 * i + 1], B[3 * j + 1], A[3 * i + 2], B[3 * j + 2]);
 #pragma unroll
     for (int k = 0; k < 9; ++k) Cm[k] = T[k];
 }

@@ -354,12 +354,14 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
             }
         lap *= (float)(prm.inv_dx * prm.inv_dx);
     }
-    // advection, F update, domain clamp (793-802)
+    // advection, F update, domain clamp (793-802).  These accumulate over every
+    // substep, so each multiply and add is rounded separately as in the
+    // reference's tensor ops (x + dt v, (I + dt C) F), without FMA contraction.
     const float pad = (float)(2.0 * prm.dx), hi = (float)(prm.grid_lim - 2.0 * prm.dx);
     float xn[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        float t = xp[a] + dt * nv[a];
+        float t = __fadd_rn(xp[a], __fmul_rn(dt, nv[a]));
         t = t < pad ? pad : t;
         xn[a] = t > hi ? hi : t;
     }
@@ -367,8 +369,8 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
 #pragma unroll
     for (int k = 0; k < 9; ++k) F[k] = P.F[k * ps + p];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) A[k] = ((k % 4 == 0) ? 1.0f : 0.0f) + dt * nC[k];
-    mm3(A, F, Fn);
+    for (int k = 0; k < 9; ++k) A[k] = __fadd_rn((k % 4 == 0) ? 1.0f : 0.0f, __fmul_rn(dt, nC[k]));
+    mm3_rn(A, F, Fn);
     bool finite = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a) finite = finite && isfinite(xn[a]);
@@ -389,7 +391,7 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
 }
 
 template <class SC>
-__global__ void __launch_bounds__(kG2PThreads, 3) k_g2p(const SC scn, const Parts P, const WS w) {
+__global__ void __launch_bounds__(kG2PThreads, SC::batched ? 3 : 4) k_g2p(const SC scn, const Parts P, const WS w) {
     __shared__ float4 sq[kGTQ];
     __shared__ float sc[kGTC];
     __shared__ int s_box[6];

@@ -110,8 +110,8 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
             for (int r = 0; r < 3; ++r) D[3 * r + i] = V[3 * r + i] * ratio;
             S[i] = sc;
         }
-        mmt3(D, V, corr);
-        mm3(F, corr, F);
+        mmt3_rn(D, V, corr);                                         // V diag(Sc/S) V^T
+        mm3_rn(F, corr, F);
 #pragma unroll
         for (int k = 0; k < 9; ++k) P.F[k * ps + p] = F[k];
     }
@@ -341,21 +341,22 @@ __global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, c
         unsigned bmom = bound_bits(bm), bmass = bound_bits(m), bdmg = bound_bits(d_new);
         Ctrl *cw = w.ctrl + sid;
         // any partition of the warp is correct here: each group raises the
-        // bounds to its own maximum
+        // bounds to its own maximum, in the slot of its warp
         const unsigned am = __activemask();
+        const int slot = (int)(((blockIdx.x << 3) + (threadIdx.x >> 5)) & (kBoundSlots - 1));
         if (!SC::batched || __all_sync(am, sid == __shfl_sync(am, sid, __ffs(am) - 1))) {
             bmom = __reduce_max_sync(am, bmom);
             bmass = __reduce_max_sync(am, bmass);
             bdmg = __reduce_max_sync(am, bdmg);
             if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1)) {
-                atomicMax(&cw->mom_bound, bmom);
-                atomicMax(&cw->mass_bound, bmass);
-                atomicMax(&cw->dmg_bound, bdmg);
+                atomicMax(&cw->bound_slots[0][slot], bmom);
+                atomicMax(&cw->bound_slots[1][slot], bmass);
+                atomicMax(&cw->bound_slots[2][slot], bdmg);
             }
         } else {
-            atomicMax(&cw->mom_bound, bmom);
-            atomicMax(&cw->mass_bound, bmass);
-            atomicMax(&cw->dmg_bound, bdmg);
+            atomicMax(&cw->bound_slots[0][slot], bmom);
+            atomicMax(&cw->bound_slots[1][slot], bmass);
+            atomicMax(&cw->bound_slots[2][slot], bdmg);
         }
     }
     if (w.tape_aff) {
@@ -448,6 +449,29 @@ constexpr int kCW = 15;                        // expanded cubic weights per par
 constexpr size_t kP2GSmem = sizeof(long long) * (4 * kQN + 2 * kCN) + sizeof(float) * (kPay + kCW) * kPayStride +
                             sizeof(int) * (kSub + 2) + 2 * kSub;
 
+// Folds control block blockIdx.x's bound slots into its three bounds and
+// clears the slots for the next substep.
+__global__ void __launch_bounds__(kBoundSlots) k_bounds(Ctrl *ctrl) {
+    Ctrl *c = ctrl + blockIdx.x;
+    __shared__ unsigned s_m[3][kBoundSlots / 32];
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const unsigned m = __reduce_max_sync(0xffffffffu, c->bound_slots[v][t]);
+        c->bound_slots[v][t] = 0u;
+        if ((t & 31) == 0) s_m[v][t >> 5] = m;
+    }
+    __syncthreads();
+    if (t < 3) {
+        unsigned m = 0u;
+#pragma unroll
+        for (int k = 0; k < kBoundSlots / 32; ++k) m = max(m, s_m[t][k]);
+        if (t == 0) c->mom_bound = m;
+        if (t == 1) c->mass_bound = m;
+        if (t == 2) c->dmg_bound = m;
+    }
+}
+
 // Sorted index of the first particle of every non-empty 4^3-cell sub-block
 // (where key >> 6 changes), appended in any order: the accumulation is exact,
 // so the order in which work items run does not change the result.
@@ -466,8 +490,10 @@ __global__ void __launch_bounds__(256) k_subblocks(const unsigned *__restrict__ 
     }
 }
 
-template <class SC>
-__global__ void __launch_bounds__(kP2GThreads, 3) k_p2g_tiles(const SC sc, const WS w, long long n) {
+// MINB: resident CTAs per SM the registers are budgeted for (3: 80
+// registers; 4: 64 registers with a few spills), a tunable.
+template <class SC, int MINB>
+__global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, const WS w, long long n) {
     extern __shared__ long long s_raw[];
     long long *qt = s_raw;                                                // [4][kQN]
     long long *ct = qt + 4 * kQN;                                         // [2][kCN]
@@ -763,15 +789,18 @@ void prepare_p2g() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        cudaFuncSetAttribute(k_p2g_tiles<PlainScenes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
-        cudaFuncSetAttribute(k_p2g_tiles<BatchScenes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        cudaFuncSetAttribute(k_p2g_tiles<PlainScenes, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        cudaFuncSetAttribute(k_p2g_tiles<BatchScenes, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        cudaFuncSetAttribute(k_p2g_tiles<PlainScenes, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
+        cudaFuncSetAttribute(k_p2g_tiles<BatchScenes, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmem);
         done[dev] = 1;
     }
 }
 
 // Persistent P2G CTAs: every resident slot of the device (work items are
-// taken from the list dynamically); `ctas_per_sm` caps the CTAs per SM (0: as
-// many as fit).
+// taken from the list dynamically).  `ctas_per_sm`: 0 = the 80-register
+// kernel with as many CTAs as fit (3 per SM); 4 = the 64-register kernel at 4
+// per SM; 1..3 = the 80-register kernel capped at that many per SM.
 template <class SC>
 void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int ctas_per_sm) {
     if (P.n <= 0) return;
@@ -779,21 +808,27 @@ void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int c
     const int lb = (int)std::min<long long>((P.n + 255) / 256, 148LL * 8);
     k_subblocks<<<lb, 256, 0, s>>>(w.sorted_keys, P.n, w.work, w.ctrl);
     k_stress<SC><<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(sc, P, w);
-    static int slots_dev[64] = {0};
+    k_bounds<<<sc.count(), kBoundSlots, 0, s>>>(w.ctrl);
+    static int slots_dev[64][2] = {{0}};
     int dev = 0;
     cudaGetDevice(&dev);
-    int slots = (dev >= 0 && dev < 64) ? slots_dev[dev] : 0;
+    const bool wide = ctas_per_sm >= 4;
+    int slots = (dev >= 0 && dev < 64) ? slots_dev[dev][wide] : 0;
     if (slots <= 0) {
-        slots = resident_slots((const void *)k_p2g_tiles<SC>, kP2GThreads, kP2GSmem);
-        if (dev >= 0 && dev < 64) slots_dev[dev] = slots;
+        slots = wide ? resident_slots((const void *)k_p2g_tiles<SC, 4>, kP2GThreads, kP2GSmem)
+                     : resident_slots((const void *)k_p2g_tiles<SC, 3>, kP2GThreads, kP2GSmem);
+        if (dev >= 0 && dev < 64) slots_dev[dev][wide] = slots;
     }
-    if (ctas_per_sm > 0) {   // the tunable
+    if (ctas_per_sm > 0 && !wide) {   // the cap
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         slots = std::min(slots, sms * ctas_per_sm);
     }
-    const long long blocks = std::min<long long>(slots, (P.n + 63) / 64);
-    k_p2g_tiles<SC><<<(unsigned)std::max<long long>(1, blocks), kP2GThreads, kP2GSmem, s>>>(sc, w, P.n);
+    const unsigned blocks = (unsigned)std::max<long long>(1, std::min<long long>(slots, (P.n + 63) / 64));
+    if (wide)
+        k_p2g_tiles<SC, 4><<<blocks, kP2GThreads, kP2GSmem, s>>>(sc, w, P.n);
+    else
+        k_p2g_tiles<SC, 3><<<blocks, kP2GThreads, kP2GSmem, s>>>(sc, w, P.n);
 }
 template void launch_p2g<PlainScenes>(const PlainScenes &, const Parts &, const WS &, cudaStream_t, int);
 template void launch_p2g<BatchScenes>(const BatchScenes &, const Parts &, const WS &, cudaStream_t, int);
