@@ -80,7 +80,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--form", default="all", choices=["all", "plain", "batched", "adjoint", "render"])
-    ap.add_argument("--fd-dirs", type=int, default=0,
+    ap.add_argument("--fd-dirs", type=int, default=32,
                     help="central-difference directions of the adjoint check, on a pre-fracture window of the 1M "
                          "scene (the first --fd-window substeps; the forward is bit-reproducible, so the float32 "
                          "differences are not blurred by summation order)")

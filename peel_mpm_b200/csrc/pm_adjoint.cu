@@ -304,7 +304,7 @@ constexpr int kASub = 4, kAQE = 6, kACE = 8, kAQN = 216, kACN = 512;
 constexpr size_t kAdjTileSmem = sizeof(long long) * (3 * kAQN + kACN) + sizeof(float) * (17 + kAdjCW) * kAPayStride +
                                 sizeof(int) * (kATh + 2) + 2 * kATh;
 
-__global__ void __launch_bounds__(kATh, 2) k_adj_tiles(const pm_params prm, const unsigned *__restrict__ keys,
+__global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, const unsigned *__restrict__ keys,
                                                        const int *__restrict__ work, const TapeHead *head,
                                                        const float4 *__restrict__ pay, AdjCtrl *actl,
                                                        long long *__restrict__ acc, long long n) {
@@ -948,12 +948,39 @@ __device__ __forceinline__ void adj_gather(const float xp[3], float inv_dx, floa
                                            const float4 *__restrict__ A, const float4 *__restrict__ B,
                                            float xb[3], float vsum[3], float mvb[3], float affb[9], float &d1b) {
     {
+        // Per node o: wbar = g . u + an . c + an.w m with u = vt + K Ct dpos and
+        // c = mv + aff dpos; the sums over the 27 nodes are contracted over z
+        // first (Z0 = sum_z wz wbar, Z1 = sum_z w'z wbar, Gz = sum_z wz g,
+        // Az = sum_z wz an, Azd = sum_z wz dpos_z an), then folded with the x
+        // and y weights per (x, y) row.
         QuadD q;
         quad_weights_d(xp, inv_dx, ng, q);
+        float DX[3], DY[3], DZ[3];
 #pragma unroll
-        for (int ox = 0; ox < 3; ++ox)
+        for (int o = 0; o < 3; ++o) {
+            DX[o] = ((float)o - q.fx[0]) * dx;
+            DY[o] = ((float)o - q.fx[1]) * dx;
+            DZ[o] = ((float)o - q.fx[2]) * dx;
+        }
+        float z0[3] = {0.0f, 0.0f, 0.0f}, z1[3] = {0.0f, 0.0f, 0.0f};   // per axis of xbar
 #pragma unroll
-            for (int oy = 0; oy < 3; ++oy)
+        for (int ox = 0; ox < 3; ++ox) {
+            float ux[3], cx[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                ux[i] = vt[i] + K * Ct[3 * i] * DX[ox];
+                cx[i] = mv[i] + aff[3 * i] * DX[ox];
+            }
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy) {
+                float uxy[3], cxy[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    uxy[i] = ux[i] + K * Ct[3 * i + 1] * DY[oy];
+                    cxy[i] = cx[i] + aff[3 * i + 1] * DY[oy];
+                }
+                float Z0 = 0.0f, Z1 = 0.0f, Gz[3] = {0.0f, 0.0f, 0.0f}, Az[3] = {0.0f, 0.0f, 0.0f},
+                      Azd[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
                     float4 g, an;
@@ -966,28 +993,36 @@ __device__ __forceinline__ void adj_gather(const float xp[3], float inv_dx, floa
                         g = __ldg(&gvel[node]);
                         an = __ldg(&A[node]);
                     }
-                    const float wx = q.w[ox][0], wy = q.w[oy][1], wz = q.w[oz][2];
-                    const float wk = wx * wy * wz;
-                    const float dp0 = ((float)ox - q.fx[0]) * dx, dp1 = ((float)oy - q.fx[1]) * dx,
-                                dp2 = ((float)oz - q.fx[2]) * dx;
-                    const float u0 = vt[0] + K * (Ct[0] * dp0 + Ct[1] * dp1 + Ct[2] * dp2);
-                    const float u1 = vt[1] + K * (Ct[3] * dp0 + Ct[4] * dp1 + Ct[5] * dp2);
-                    const float u2 = vt[2] + K * (Ct[6] * dp0 + Ct[7] * dp1 + Ct[8] * dp2);
-                    const float c0 = mv[0] + aff[0] * dp0 + aff[1] * dp1 + aff[2] * dp2;
-                    const float c1 = mv[1] + aff[3] * dp0 + aff[4] * dp1 + aff[5] * dp2;
-                    const float c2 = mv[2] + aff[6] * dp0 + aff[7] * dp1 + aff[8] * dp2;
+                    const float u0 = uxy[0] + K * Ct[2] * DZ[oz], u1 = uxy[1] + K * Ct[5] * DZ[oz],
+                                u2 = uxy[2] + K * Ct[8] * DZ[oz];
+                    const float c0 = cxy[0] + aff[2] * DZ[oz], c1 = cxy[1] + aff[5] * DZ[oz],
+                                c2 = cxy[2] + aff[8] * DZ[oz];
                     const float wbar = (g.x * u0 + g.y * u1 + g.z * u2) + (an.x * c0 + an.y * c1 + an.z * c2) + an.w * m;
-                    const float wb = wbar * inv_dx;
-                    xb[0] += wb * q.dw[ox][0] * wy * wz;
-                    xb[1] += wb * wx * q.dw[oy][1] * wz;
-                    xb[2] += wb * wx * wy * q.dw[oz][2];
-                    vsum[0] += wk * g.x; vsum[1] += wk * g.y; vsum[2] += wk * g.z;
-                    const float a0 = wk * an.x, a1 = wk * an.y, a2 = wk * an.z;
-                    mvb[0] += a0; mvb[1] += a1; mvb[2] += a2;
-                    affb[0] += a0 * dp0; affb[1] += a0 * dp1; affb[2] += a0 * dp2;
-                    affb[3] += a1 * dp0; affb[4] += a1 * dp1; affb[5] += a1 * dp2;
-                    affb[6] += a2 * dp0; affb[7] += a2 * dp1; affb[8] += a2 * dp2;
+                    const float wz = q.w[oz][2], wzd = wz * DZ[oz];
+                    Z0 += wz * wbar;
+                    Z1 += q.dw[oz][2] * wbar;
+                    Gz[0] += wz * g.x; Gz[1] += wz * g.y; Gz[2] += wz * g.z;
+                    Az[0] += wz * an.x; Az[1] += wz * an.y; Az[2] += wz * an.z;
+                    Azd[0] += wzd * an.x; Azd[1] += wzd * an.y; Azd[2] += wzd * an.z;
                 }
+                const float wx = q.w[ox][0], wy = q.w[oy][1], wxy = wx * wy;
+                z0[0] += q.dw[ox][0] * wy * Z0;
+                z0[1] += wx * q.dw[oy][1] * Z0;
+                z1[2] += wxy * Z1;
+                const float wxyx = wxy * DX[ox], wxyy = wxy * DY[oy];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    vsum[i] += wxy * Gz[i];
+                    mvb[i] += wxy * Az[i];
+                    affb[3 * i] += wxyx * Az[i];
+                    affb[3 * i + 1] += wxyy * Az[i];
+                    affb[3 * i + 2] += wxy * Azd[i];
+                }
+            }
+        }
+        xb[0] += inv_dx * z0[0];
+        xb[1] += inv_dx * z0[1];
+        xb[2] += inv_dx * z1[2];
     }
     {
         CubicD cw;

@@ -92,20 +92,22 @@ __device__ __forceinline__ void resolve(float v[3], const float vc[3], const flo
         v[0] = vc[0]; v[1] = vc[1]; v[2] = vc[2];
         return;
     }
-    const float r0 = v[0] - vc[0], r1 = v[1] - vc[1], r2 = v[2] - vc[2];
-    const float vn = r0 * nn[0] + r1 * nn[1] + r2 * nn[2];
+    // every op rounded separately, as the reference's tensor ops round them
+    const float r0 = __fsub_rn(v[0], vc[0]), r1 = __fsub_rn(v[1], vc[1]), r2 = __fsub_rn(v[2], vc[2]);
+    const float vn = dot3_rn(r0, nn[0], r1, nn[1], r2, nn[2]);
     const float inward = vn < 0.0f ? vn : 0.0f;
-    float t0 = r0 - vn * nn[0], t1 = r1 - vn * nn[1], t2 = r2 - vn * nn[2];
+    float t0 = __fsub_rn(r0, __fmul_rn(vn, nn[0])), t1 = __fsub_rn(r1, __fmul_rn(vn, nn[1])),
+          t2 = __fsub_rn(r2, __fmul_rn(vn, nn[2]));
     if (fr > 0.0f) {
-        const float vtm = sqrtf(t0 * t0 + t1 * t1 + t2 * t2);
-        float sc = 1.0f + fr * inward / (vtm + 1e-9f);
+        const float vtm = sqrtf(dot3_rn(t0, t0, t1, t1, t2, t2));
+        float sc = __fadd_rn(1.0f, __fdiv_rn(__fmul_rn(fr, inward), __fadd_rn(vtm, 1e-9f)));
         sc = sc < 0.0f ? 0.0f : sc;
-        t0 *= sc; t1 *= sc; t2 *= sc;
+        t0 = __fmul_rn(t0, sc); t1 = __fmul_rn(t1, sc); t2 = __fmul_rn(t2, sc);
     }
-    const float keep = vn - inward;
-    v[0] = vc[0] + t0 + keep * nn[0];
-    v[1] = vc[1] + t1 + keep * nn[1];
-    v[2] = vc[2] + t2 + keep * nn[2];
+    const float keep = __fsub_rn(vn, inward);
+    v[0] = __fadd_rn(__fadd_rn(vc[0], t0), __fmul_rn(keep, nn[0]));
+    v[1] = __fadd_rn(__fadd_rn(vc[1], t1), __fmul_rn(keep, nn[1]));
+    v[2] = __fadd_rn(__fadd_rn(vc[2], t2), __fmul_rn(keep, nn[2]));
 }
 
 // One thread per z-row of 4 nodes of an active 4^3 block: the row's scene,
@@ -169,7 +171,9 @@ __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
             *(longlong2 *)(w.g_dmg + 2 * node) = make_longlong2(0, 0);
             const bool active = mom[k].w > 1e-12f;
             const float inv_m = active ? 1.0f / mom[k].w : 0.0f;
-            float v[3] = {mom[k].x * inv_m + gdt[0], mom[k].y * inv_m + gdt[1], mom[k].z * inv_m + gdt[2]};
+            // (mv * inv_m) + dt g, each op rounded as the reference's tensor ops (727-733)
+            float v[3] = {__fadd_rn(__fmul_rn(mom[k].x, inv_m), gdt[0]), __fadd_rn(__fmul_rn(mom[k].y, inv_m), gdt[1]),
+                          __fadd_rn(__fmul_rn(mom[k].z, inv_m), gdt[2])};
             if (do_damp) {
                 v[0] *= damp; v[1] *= damp; v[2] *= damp;
             }
@@ -182,11 +186,12 @@ __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
                     const float *vc = ctrl->col_vel[c];
                     if (col.kind == 0) {   // halfspace_collider (847-867)
                         const float nn[3] = {(float)col.normal[0], (float)col.normal[1], (float)col.normal[2]};
-                        const float sd = (pos[0] - o[0]) * nn[0] + (pos[1] - o[1]) * nn[1] + (pos[2] - o[2]) * nn[2];
+                        const float sd = dot3_rn(__fsub_rn(pos[0], o[0]), nn[0], __fsub_rn(pos[1], o[1]), nn[1],
+                                                 __fsub_rn(pos[2], o[2]), nn[2]);
                         if (sd < 0.0f) resolve(v, vc, nn, col.mode == 1, (float)col.friction);
                     } else {               // sphere_collider (828-844)
                         const float r0 = pos[0] - o[0], r1 = pos[1] - o[1], r2 = pos[2] - o[2];
-                        const float dist = sqrtf(r0 * r0 + r1 * r1 + r2 * r2);
+                        const float dist = sqrtf(dot3_rn(r0, r0, r1, r1, r2, r2));
                         if (dist < (float)col.radius) {
                             const float den = dist + 1e-9f;
                             const float nn[3] = {r0 / den, r1 / den, r2 / den};

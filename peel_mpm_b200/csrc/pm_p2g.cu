@@ -645,24 +645,26 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                             az[c] = pay[8 + 3 * c][t];
                         }
                         const float wxs = ox == 0 ? wx[0] : (ox == 1 ? wx[1] : wx[2]);
-                        float bz3[3][3];   // mv + aff (dpos_x, ., dpos_z) for each oz
+                        // w (mv + aff dpos) = wxy [wz (mv + aff (dx, ., dz))] + [wxy aff_y dy] wz:
+                        // the bracketed factors per oz and per oy, then 2 FMAs per node and component
+                        float bz3[3][4];
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
                             const float dz = ((float)oz - fx2) * dx;
 #pragma unroll
-                            for (int c = 0; c < 3; ++c) bz3[oz][c] = base[c] + az[c] * dz;
+                            for (int c = 0; c < 3; ++c) bz3[oz][c] = wz[oz] * (base[c] + az[c] * dz);
+                            bz3[oz][3] = wz[oz] * m;
                         }
 #pragma unroll
                         for (int oy = 0; oy < 3; ++oy) {
                             const float dy = ((float)oy - fx1) * dx;
                             const float wxy = wxs * wy[oy];
-                            const float ady[3] = {ay[0] * dy, ay[1] * dy, ay[2] * dy};
+                            const float ady[3] = {wxy * ay[0] * dy, wxy * ay[1] * dy, wxy * ay[2] * dy};
 #pragma unroll
                             for (int oz = 0; oz < 3; ++oz) {
-                                const float wk = wxy * wz[oz];
 #pragma unroll
-                                for (int c = 0; c < 3; ++c) acc[oy][oz][c] += wk * (bz3[oz][c] + ady[c]);
-                                acc[oy][oz][3] += wk * m;
+                                for (int c = 0; c < 3; ++c) acc[oy][oz][c] += wxy * bz3[oz][c] + ady[c] * wz[oz];
+                                acc[oy][oz][3] += wxy * bz3[oz][3];
                             }
                         }
                     }
@@ -695,14 +697,16 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                             ez[k] = cwt[10 + k][t];
                         }
                         const float d = pay[16][t];
+                        float ezd[5];   // d wz, hoisted: 2 FMAs per node
+#pragma unroll
+                        for (int k = 0; k < 5; ++k) ezd[k] = d * ez[k];
 #pragma unroll
                         for (int ny = 0; ny < 5; ++ny) {
                             const float wxy = wxs * ey[ny];
 #pragma unroll
                             for (int nz = 0; nz < 5; ++nz) {
-                                const float wk = wxy * ez[nz];
-                                adc[ny][nz] += wk * d;
-                                adw[ny][nz] += wk;
+                                adc[ny][nz] += wxy * ezd[nz];
+                                adw[ny][nz] += wxy * ez[nz];
                             }
                         }
                     }
