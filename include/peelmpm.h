@@ -231,9 +231,13 @@ int pm_tape_size(int64_t n, int32_t n_grid, int32_t slots, size_t *bytes);
 int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32_t slots, void *stream);
 
 /* pm_substep that also records the substep's grid state into tape slot
- * `slot`.  The particle state P advances in place as in pm_substep. */
-int pm_substep_record(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, const pm_clock *clk,
-                      void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream);
+ * `slot`.  out == NULL: the particle state P advances in place as in
+ * pm_substep.  Otherwise the updated state (x, v, F, C, d, lap, D_hist) is
+ * written to out's planes (same n and plane_stride, planes disjoint from P's)
+ * and P's state is left as it was: a recorded segment keeps every substep's
+ * state without copying it. */
+int pm_substep_record(const pm_params *prm, const pm_particles *P, const pm_particles *out, void *ws, size_t ws_bytes,
+                      const pm_clock *clk, void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream);
 
 /* Adjoint of the substep recorded in `slot`: pre is the state before it and
  * post the state after it (same material planes), adj_in the adjoint of the

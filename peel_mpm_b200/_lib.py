@@ -153,8 +153,8 @@ def load():
         "pm_batch_read_status": (C.c_int, [vp, sz, i32, vp, vp, C.POINTER(pm_status_info), vp]),
         "pm_tape_size": (C.c_int, [i64, i32, i32, C.POINTER(sz)]),
         "pm_tape_init": (C.c_int, [vp, sz, i64, i32, i32, vp]),
-        "pm_substep_record": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), vp, sz, C.POINTER(pm_clock),
-                                        vp, sz, i32, i32, vp]),
+        "pm_substep_record": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), C.POINTER(pm_particles), vp,
+                                        sz, C.POINTER(pm_clock), vp, sz, i32, i32, vp]),
         "pm_render_workspace_size": (C.c_int, [i64, i32, i32, i32, C.POINTER(sz)]),
         "pm_carry_gaussians": (C.c_int, [C.POINTER(pm_particles), vp, vp, vp, vp, i64, vp, C.c_float, vp, vp, vp,
                                          vp]),

@@ -301,8 +301,10 @@ __device__ __noinline__ void adj_scatter_global(const float xp[3], const float v
 constexpr int kATh = 256;
 constexpr int kAPayStride = kATh + kATh / 32;
 constexpr int kASub = 4, kAQE = 6, kACE = 8, kAQN = 216, kACN = 512;
-constexpr size_t kAdjTileSmem = sizeof(long long) * (3 * kAQN + kACN) + sizeof(float) * (17 + kAdjCW) * kAPayStride +
-                                sizeof(int) * (kATh + 2) + 2 * kATh;
+// chunk planes with the forward P2G's conflict-free strides (z 1, y 8, x 52 / 68)
+constexpr int kAQSY = 8, kAQSX = 52, kAQPl = 312, kACSY = 8, kACSX = 68, kACPl = 544;
+constexpr size_t kAdjTileSmem = sizeof(long long) * (3 * kAQN + kACN) + sizeof(unsigned) * 2 * (3 * kAQPl + kACPl) +
+                                sizeof(float) * (17 + kAdjCW) * kAPayStride + sizeof(int) * (kATh + 2) + 2 * kATh;
 
 __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, const unsigned *__restrict__ keys,
                                                        const int *__restrict__ work, const TapeHead *head,
@@ -311,7 +313,11 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
     extern __shared__ long long s_adj[];
     long long *qt = s_adj;                                                 // [3][kAQN]
     long long *ct = qt + 3 * kAQN;                                         // [kACN]
-    float (*sp)[kAPayStride] = (float (*)[kAPayStride])(ct + kACN);      // [17][kAPayStride]
+    unsigned (*qlo)[kAQPl] = (unsigned (*)[kAQPl])(ct + kACN);            // [3][kAQPl] chunk planes
+    int (*qhi)[kAQPl] = (int (*)[kAQPl])(qlo[3]);                         // [3][kAQPl]
+    unsigned *clo = (unsigned *)(qhi[3]);                                 // [kACPl]
+    int *chi = (int *)(clo + kACPl);                                      // [kACPl]
+    float (*sp)[kAPayStride] = (float (*)[kAPayStride])(chi + kACPl);    // [17][kAPayStride]
     float (*cw)[kAPayStride] = (float (*)[kAPayStride])(sp[17]);        // [kAdjCW][kAPayStride]
     int *runs = (int *)(cw[kAdjCW]);                                      // [kATh + 2]
     unsigned char *regular = (unsigned char *)(runs + kATh + 2);          // [kATh]
@@ -325,6 +331,7 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
     const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
     const float smom = fix_scale(actl->mom_bound).scale, slap = fix_scale(actl->lap_bound).scale;
     for (int i = tid; i < 3 * kAQN + kACN; i += kATh) qt[i] = 0;
+    for (int i = tid; i < 2 * (3 * kAQPl + kACPl); i += kATh) qlo[0][i] = 0u;
     for (;;) {
         __syncthreads();
         if (tid == 0) s_item = atomicAdd(&actl->work_next, 1u);
@@ -407,10 +414,12 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
                 for (int k = 0; k < 9; ++k) kc[k] = sp[6 + k][t];
                 adj_scatter_global(xp, vt, kc, sp[16][t], inv_dx, dx, ng, smom, slap, acc);
             }
-            for (int it = tid; it < nruns * 8; it += kATh) {
+            for (int it = tid; it < nruns * 8; it += kATh) {   // slab-major, as the forward P2G
                 const bool quad = it < 3 * nruns;
-                const int r = quad ? it / 3 : (it - 3 * nruns) / 5;
-                const int sl = quad ? it - 3 * r : 3 + (it - 3 * nruns - 5 * r);
+                const int k = quad ? it : it - 3 * nruns;
+                const int s8 = k / nruns;
+                const int r = k - s8 * nruns;
+                const int sl = quad ? s8 : 3 + s8;
                 const int ja = runs[r], jb = runs[r + 1];
                 int cq[3];
                 morton_decode(lcell[ja], cq);
@@ -463,10 +472,9 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
                     for (int oy = 0; oy < 3; ++oy)
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
-                            const int idx = (nx * kAQE + cq[1] + oy) * kAQE + cq[2] + oz;
-                            tile_add(&qt[idx], acc3[oy][oz][0], smom);
-                            tile_add(&qt[kAQN + idx], acc3[oy][oz][1], smom);
-                            tile_add(&qt[2 * kAQN + idx], acc3[oy][oz][2], smom);
+                            const int sidx = nx * kAQSX + (cq[1] + oy) * kAQSY + cq[2] + oz;
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) plane_add(&qlo[c][sidx], &qhi[c][sidx], acc3[oy][oz][c], smom);
                         }
                 } else {
                     const int nxs = sl - 3;
@@ -500,32 +508,64 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
                     for (int ny = 0; ny < 5; ++ny)
 #pragma unroll
                         for (int nz = 0; nz < 5; ++nz)
-                            tile_add(&ct[(nx * kACE + cq[1] + ny) * kACE + cq[2] + nz], al[ny][nz], slap);
+                        {
+                            const int sidx = nx * kACSX + (cq[1] + ny) * kACSY + cq[2] + nz;
+                            plane_add(&clo[sidx], &chi[sidx], al[ny][nz], slap);
+                        }
                 }
             }
             __syncthreads();
-            if (cnt < kATh) break;
-        }
-        for (int li = tid; li < kAQN; li += kATh) {
-            const long long q0 = qt[li], q1 = qt[kAQN + li], q2 = qt[2 * kAQN + li];
-            if ((q0 | q1 | q2) != 0) {
-                qt[li] = 0; qt[kAQN + li] = 0; qt[2 * kAQN + li] = 0;
+            const bool last = cnt < kATh;
+            // fold the chunk planes into the int64 sums; flush after the last chunk
+            for (int li = tid; li < kAQN; li += kATh) {
                 const int tx = li / (kAQE * kAQE), ty = (li / kAQE) % kAQE, tz = li % kAQE;
-                long long *g = acc + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
-                if (q0) atomicAdd((unsigned long long *)g, (unsigned long long)q0);
-                if (q1) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q1);
-                if (q2) atomicAdd((unsigned long long *)(g + 2), (unsigned long long)q2);
+                const int sidx = tx * kAQSX + ty * kAQSY + tz;
+                long long q[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const unsigned lo = qlo[c][sidx];
+                    const int hi = qhi[c][sidx];
+                    q[c] = qt[c * kAQN + li];
+                    if ((lo | (unsigned)hi) != 0u) {
+                        qlo[c][sidx] = 0u;
+                        qhi[c][sidx] = 0;
+                        q[c] += plane_value(lo, hi);
+                    }
+                }
+                if (!last) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) qt[c * kAQN + li] = q[c];
+                } else if ((q[0] | q[1] | q[2]) != 0) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) qt[c * kAQN + li] = 0;
+                    long long *g = acc + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        if (q[c]) atomicAdd((unsigned long long *)(g + c), (unsigned long long)q[c]);
+                }
             }
-        }
-        for (int li = tid; li < kACN; li += kATh) {
-            const long long q3 = ct[li];
-            if (q3 != 0) {
-                ct[li] = 0;
+            for (int li = tid; li < kACN; li += kATh) {
                 const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
-                long long *g = acc + 4 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
-                                          (org[2] - 1 + tz));
-                atomicAdd((unsigned long long *)(g + 3), (unsigned long long)q3);
+                const int sidx = tx * kACSX + ty * kACSY + tz;
+                const unsigned lo = clo[sidx];
+                const int hi = chi[sidx];
+                long long q3 = ct[li];
+                if ((lo | (unsigned)hi) != 0u) {
+                    clo[sidx] = 0u;
+                    chi[sidx] = 0;
+                    q3 += plane_value(lo, hi);
+                }
+                if (!last) {
+                    ct[li] = q3;
+                } else if (q3 != 0) {
+                    ct[li] = 0;
+                    long long *g = acc + 4 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
+                                              (org[2] - 1 + tz));
+                    atomicAdd((unsigned long long *)(g + 3), (unsigned long long)q3);
+                }
             }
+            if (last) break;
+            __syncthreads();
         }
     }
 }

@@ -278,18 +278,26 @@ int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32
     return cuda_check("pm_tape_init");
 }
 
-int pm_substep_record(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_bytes, const pm_clock *clk,
-                      void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream) {
+int pm_substep_record(const pm_params *prm, const pm_particles *P, const pm_particles *out, void *ws, size_t ws_bytes,
+                      const pm_clock *clk, void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream) {
     int rc;
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
     if ((rc = check_adjoint_params(prm, P))) return rc;
     if (!clk) return fail(PM_ERR_ARG, "clock is NULL");
+    if (out) {
+        if (out->n != P->n || out->plane_stride != P->plane_stride)
+            return fail(PM_ERR_ARG, "out differs from P in n or plane_stride");
+        if (!out->x || !out->v || !out->F || !out->C || !out->d || !out->lap || !out->D_hist)
+            return fail(PM_ERR_ARG, "an out state plane is NULL");
+        if (out->x == P->x || out->F == P->F || out->d == P->d)
+            return fail(PM_ERR_ARG, "out must not alias P's state (pass NULL to advance in place)");
+    }
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
     pm::TapeLayout T;
     if ((rc = get_tape(tape, tape_bytes, P->n, prm->n_grid, slots, slot, &T))) return rc;
     pm::record_redirect(T, tape, slot, w);
-    const pm::Parts parts = pm::make_parts(P);
+    const pm::Parts parts = out ? pm::make_parts_out(P, out) : pm::make_parts(P);
     cudaStream_t s = (cudaStream_t)stream;
     pm::launch_set_clock(*prm, w, *clk, s);
     if (P->n > 0) {

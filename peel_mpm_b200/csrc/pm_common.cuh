@@ -189,9 +189,13 @@ inline WS make_ws(void *base, const Layout &L) {
 }
 
 // Particle pointers as kernels see them (plane stride folded in).
+// Mutable state is read from x .. D_hist and written to xo .. Dho: the same
+// planes for an in-place substep, another state's planes for an out-of-place
+// one (a recorded substep writing the next state of its segment).
 struct Parts {
     long long n, ps;
     float *x, *v, *F, *C, *d, *lap, *D_hist;
+    float *xo, *vo, *Fo, *Co, *d_o, *lapo, *Dho;
     const float *vol0, *mass, *mu, *lam, *sigma_c, *eta, *zeta, *l0, *residual, *A0;
     const unsigned char *allow;
     const float *n_interface;
@@ -209,6 +213,13 @@ inline Parts make_parts(const pm_particles *P) {
     q.allow = P->allow; q.n_interface = P->n_interface; q.interface_mask = P->interface_mask;
     q.grip_tag = (const signed char *)P->grip_tag; q.phi = P->phi; q.phi_shear = P->phi_shear;
     q.tau_last = P->tau_last; q.J_last = P->J_last;
+    q.xo = q.x; q.vo = q.v; q.Fo = q.F; q.Co = q.C; q.d_o = q.d; q.lapo = q.lap; q.Dho = q.D_hist;
+    return q;
+}
+// The same particles writing their updated state to O's planes (O->plane_stride equals P's).
+inline Parts make_parts_out(const pm_particles *P, const pm_particles *O) {
+    Parts q = make_parts(P);
+    q.xo = O->x; q.vo = O->v; q.Fo = O->F; q.Co = O->C; q.d_o = O->d; q.lapo = O->lap; q.Dho = O->D_hist;
     return q;
 }
 
@@ -628,21 +639,22 @@ __device__ __forceinline__ void cw5_2(float fx, float e[5]) {
     e[4] = s1 ? w3 : 0.0f;
 }
 
-// Adds a float partial sum to an int64 fixed-point entry of a shared-memory
-// tile.  The entry is held as two 32-bit words {lo, hi}: the low word takes a
-// native 32-bit atomic add (64-bit shared atomics are several times slower
-// on this part) and the carry out of it goes to the high word with the value's
-// upper half.  The number of carries over all additions equals the number of
-// times the low word wraps, whatever their order, so the pair holds the exact
-// 64-bit sum once every addition is done.
-__device__ __forceinline__ void tile_add(long long *t, float v, float scale) {
+// A node's fixed-point sum over one chunk of work, split over two 32-bit
+// planes: `lo` sums the low kSplitBits bits of every contribution (unsigned,
+// so at most 2^(32 - kSplitBits) = 256 contributions per node and chunk) and
+// `hi` the rest (q >> kSplitBits, signed; a contribution is below 2^kFixBits
+// per particle, so a chunk of 256 particles keeps |hi| under 2^31).  Both
+// adds are fire-and-forget (no returned value, no carry chain) and
+// unconditional (a branch per add costs more than adding a zero); the pair
+// is folded into an int64 tile after every chunk, exactly.
+constexpr int kSplitBits = 24;
+__device__ __forceinline__ void plane_add(unsigned *lo, int *hi, float v, float scale) {
     const long long q = to_fix(v, scale);
-    if (q == 0) return;
-    unsigned *w = (unsigned *)t;
-    const unsigned lo = (unsigned)q;
-    const unsigned old = atomicAdd(w, lo);
-    const unsigned hi = (unsigned)((unsigned long long)q >> 32) + ((old + lo) < old ? 1u : 0u);
-    if (hi != 0u) atomicAdd(w + 1, hi);
+    atomicAdd(lo, (unsigned)q & ((1u << kSplitBits) - 1u));
+    atomicAdd(hi, (int)(q >> kSplitBits));
+}
+__device__ __forceinline__ long long plane_value(unsigned lo, int hi) {
+    return (long long)hi * (1LL << kSplitBits) + (long long)lo;
 }
 // The same for an entry in global memory: one 64-bit atomic.
 __device__ __forceinline__ void red_fix(long long *addr, float v, float scale) {

@@ -371,8 +371,9 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
         xn[a] = t > hi ? hi : t;
     }
     float F[9], Fn[9], A[9];   // F is loaded after the gathers: fewer registers live across them
+    const float *Fin = prm.use_f_clamp ? P.Fo : P.F;   // the constitutive update wrote the clamped F there
 #pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = P.F[k * ps + p];
+    for (int k = 0; k < 9; ++k) F[k] = Fin[k * ps + p];
 #pragma unroll
     for (int k = 0; k < 9; ++k) A[k] = __fadd_rn((k % 4 == 0) ? 1.0f : 0.0f, __fmul_rn(dt, nC[k]));
     mm3_rn(A, F, Fn);
@@ -384,15 +385,15 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
     if (!finite) atomicAdd(nonfinite, 1u);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        P.x[a * ps + p] = xn[a];
-        P.v[a * ps + p] = nv[a];
+        P.xo[a * ps + p] = xn[a];
+        P.vo[a * ps + p] = nv[a];
     }
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        P.F[k * ps + p] = Fn[k];
-        P.C[k * ps + p] = nC[k];
+        P.Fo[k * ps + p] = Fn[k];
+        P.Co[k * ps + p] = nC[k];
     }
-    P.lap[p] = lap;
+    P.lapo[p] = lap;
 }
 
 template <class SC>

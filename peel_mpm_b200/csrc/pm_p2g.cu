@@ -113,7 +113,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
         mmt3_rn(D, V, corr);                                         // V diag(Sc/S) V^T
         mm3_rn(F, corr, F);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) P.F[k * ps + p] = F[k];
+        for (int k = 0; k < 9; ++k) P.Fo[k * ps + p] = F[k];
     }
     const float J = clamp_min(S[0] * S[1] * S[2], 1e-6f);            // (637)
     const float mu = in.mu, lam = in.lam;
@@ -185,7 +185,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
         const float drive = in.zeta * relu(phi - 1.0f);
         const float dh0 = in.Dh;
         const float Dh = tmax(dh0, drive);
-        P.D_hist[p] = Dh;                                            // history max (679)
+        P.Dho[p] = Dh;                                               // history max (679)
         const float d = in.d;
         const float l0 = in.l0;
         const float resist = d - (l0 * l0) * in.lap;
@@ -196,7 +196,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
         dn = dn > 1.0f ? 1.0f : dn;                                  // (683-684)
         if (in.allow) {                                              // monotone, where allowed (685)
             d_out = tmax(dn, d);
-            P.d[p] = d_out;
+            P.d_o[p] = d_out;
         }
     }
     const float d = d_out;
@@ -300,6 +300,10 @@ __global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, c
     float tau[9];
     float d_new = in.d;
     constitutive(prm, P, p, do_damage, in, tau, d_new, w.tape_pol, w.tape_aff_stride);
+    if (P.d_o != P.d) {   // out of place: every particle's d and D_hist go to the output state
+        P.d_o[p] = d_new;
+        if (!do_damage) P.Dho[p] = in.Dh;
+    }
     float v[3] = {in.v[0], in.v[1], in.v[2]};
     {                                                                // particle BCs (601-602)
         const int g = in.grip;
@@ -446,8 +450,16 @@ constexpr int kQN = kQE * kQE * kQE;           // 216
 constexpr int kCN = kCE * kCE * kCE;           // 512
 constexpr int kSub = kP2GThreads;              // particles per chunk
 constexpr int kCW = 15;                        // expanded cubic weights per particle (5 per axis)
-constexpr size_t kP2GSmem = sizeof(long long) * (4 * kQN + 2 * kCN) + sizeof(float) * (kPay + kCW) * kPayStride +
-                            sizeof(int) * (kSub + 2) + 2 * kSub;
+// Chunk planes (32-bit words, one node per word) are laid out with z stride
+// 1, y stride 8 and x stride 52 (quadratic) / 68 (cubic): the 32 cells of a
+// chunk of a sub-block (x in one half, all y and z) then land on 32 distinct
+// banks for every node offset, so a warp of items over distinct cells adds
+// without bank conflicts.
+constexpr int kQSY = 8, kQSX = 52, kQPl = 312;   // 5*52 + 5*8 + 6 = 306 <= 312
+constexpr int kCSY = 8, kCSX = 68, kCPl = 544;   // 7*68 + 7*8 + 8 = 540 <= 544
+constexpr size_t kP2GSmem = sizeof(long long) * (4 * kQN + 2 * kCN) +
+                            sizeof(unsigned) * 2 * (4 * kQPl + 2 * kCPl) +
+                            sizeof(float) * (kPay + kCW) * kPayStride + sizeof(int) * (kSub + 2) + 2 * kSub;
 
 // Folds control block blockIdx.x's bound slots into its three bounds and
 // clears the slots for the next substep.
@@ -495,9 +507,13 @@ __global__ void __launch_bounds__(256) k_subblocks(const unsigned *__restrict__ 
 template <class SC, int MINB>
 __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, const WS w, long long n) {
     extern __shared__ long long s_raw[];
-    long long *qt = s_raw;                                                // [4][kQN]
+    long long *qt = s_raw;                                                // [4][kQN] int64 sub-block sums
     long long *ct = qt + 4 * kQN;                                         // [2][kCN]
-    float (*pay)[kPayStride] = (float (*)[kPayStride])(ct + 2 * kCN);   // [kPay][kPayStride]
+    unsigned (*qlo)[kQPl] = (unsigned (*)[kQPl])(ct + 2 * kCN);          // [4][kQPl] chunk planes
+    int (*qhi)[kQPl] = (int (*)[kQPl])(qlo[4]);                         // [4][kQPl]
+    unsigned (*clo)[kCPl] = (unsigned (*)[kCPl])(qhi[4]);                // [2][kCPl]
+    int (*chi)[kCPl] = (int (*)[kCPl])(clo[2]);                         // [2][kCPl]
+    float (*pay)[kPayStride] = (float (*)[kPayStride])(chi[2]);         // [kPay][kPayStride]
     float (*cwt)[kPayStride] = (float (*)[kPayStride])(pay[kPay]);     // [kCW][kPayStride]
     int *runs = (int *)(cwt[kCW]);                                      // [kSub + 2]
     unsigned char *regular = (unsigned char *)(runs + kSub + 2);        // [kSub]
@@ -511,8 +527,9 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
     Ctrl *ctrl0 = w.ctrl;
     const unsigned n_work = min(ctrl0->n_work, (unsigned)min(n, (long long)0x7fffffff));
 
-    // tiles start zero; every flush clears what it visits, so they stay zero
+    // tiles and planes start zero; every fold and flush clears what it visits
     for (int i = tid; i < 4 * kQN + 2 * kCN; i += kP2GThreads) qt[i] = 0;
+    for (int i = tid; i < 2 * (4 * kQPl + 2 * kCPl); i += kP2GThreads) qlo[0][i] = 0u;
     if (tid < 27) s_bmark[tid] = 0;
     for (;;) {
         __syncthreads();                  // the previous item's tiles, marks and shared state are done
@@ -610,16 +627,30 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                 scatter_particle_global(xp, mv, aff, pay[15][t], pay[16][t], inv_dx, dx, ng, scl, g_mom, g_dmg,
                                         bmask, nbs);
             }
-            // ---------------- (cell, slab) items into the tiles: items
+            // ---------------- (cell, slab) items into the chunk planes: items
             // 0 .. 3*nruns-1 are quadratic x-slabs, then 5*nruns cubic x-slabs,
-            // so a warp mostly runs one kind
+            // slab-major, so the lanes of a warp mostly run one kind and one
+            // slab over distinct cells (distinct nodes at every step)
             for (int it = tid; it < nruns * 8; it += kP2GThreads) {
                 const bool quad = it < 3 * nruns;
-                const int r = quad ? it / 3 : (it - 3 * nruns) / 5;
-                const int sl = quad ? it - 3 * r : 3 + (it - 3 * nruns - 5 * r);
+                const int k = quad ? it : it - 3 * nruns;
+                const int s8 = k / nruns;
+                const int r = k - s8 * nruns;
+                const int sl = quad ? s8 : 3 + s8;
                 const int ja = runs[r], jb = runs[r + 1];
                 int cq[3];
                 morton_decode(lcell[ja], cq);                    // cell inside the sub-block
+                if (sl == 0) {
+                    // the cell's stencils (quadratic nodes c..c+2, cubic c-1..c+3 per
+                    // axis) span grid blocks s-1+b .. s+b with b = (c > 0): marked
+                    // whatever the sums, so that the grid update writes every node a
+                    // gather reads (a node whose contributions all round to zero
+                    // still gets its zero velocity and damage)
+                    const int b0 = cq[0] > 0, b1 = cq[1] > 0, b2 = cq[2] > 0;
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        s_bmark[((b0 + (k >> 2)) * 3 + b1 + ((k >> 1) & 1)) * 3 + b2 + (k & 1)] = 1;
+                }
                 if (sl < 3) {
                     const int ox = sl;
                     float acc[3][3][4];
@@ -673,11 +704,10 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                     for (int oy = 0; oy < 3; ++oy)
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
-                            const int idx = (nx * kQE + cq[1] + oy) * kQE + cq[2] + oz;
-                            tile_add(&qt[idx], acc[oy][oz][0], scl[0]);
-                            tile_add(&qt[kQN + idx], acc[oy][oz][1], scl[0]);
-                            tile_add(&qt[2 * kQN + idx], acc[oy][oz][2], scl[0]);
-                            tile_add(&qt[3 * kQN + idx], acc[oy][oz][3], scl[1]);
+                            const int sidx = nx * kQSX + (cq[1] + oy) * kQSY + cq[2] + oz;
+#pragma unroll
+                            for (int c = 0; c < 4; ++c)
+                                plane_add(&qlo[c][sidx], &qhi[c][sidx], acc[oy][oz][c], scl[c == 3 ? 1 : 0]);
                         }
                 } else {
                     const int nxs = sl - 3;
@@ -716,47 +746,77 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                     for (int ny = 0; ny < 5; ++ny)
 #pragma unroll
                         for (int nz = 0; nz < 5; ++nz) {
-                            const int idx = (nx * kCE + cq[1] + ny) * kCE + cq[2] + nz;
-                            tile_add(&ct[idx], adc[ny][nz], scl[2]);
-                            tile_add(&ct[kCN + idx], adw[ny][nz], scl[3]);
+                            const int sidx = nx * kCSX + (cq[1] + ny) * kCSY + cq[2] + nz;
+                            plane_add(&clo[0][sidx], &chi[0][sidx], adc[ny][nz], scl[2]);
+                            plane_add(&clo[1][sidx], &chi[1][sidx], adw[ny][nz], scl[3]);
                         }
                 }
             }
             __syncthreads();
-            if (cnt < kSub) break;                              // uniform: the last chunk of the sub-block
+            const bool last = cnt < kSub;                       // uniform: the last chunk of the sub-block
+            // ---------------- fold the chunk planes into the int64 sums; after
+            // the last chunk, flush those with one atomic per nonzero node
+            // component.
+            for (int li = tid; li < kQN; li += kP2GThreads) {
+                const int tx = li / (kQE * kQE), ty = (li / kQE) % kQE, tz = li % kQE;
+                const int sidx = tx * kQSX + ty * kQSY + tz;
+                long long q[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const unsigned lo = qlo[c][sidx];
+                    const int hi = qhi[c][sidx];
+                    q[c] = qt[c * kQN + li];
+                    if ((lo | (unsigned)hi) != 0u) {
+                        qlo[c][sidx] = 0u;
+                        qhi[c][sidx] = 0;
+                        q[c] += plane_value(lo, hi);
+                    }
+                }
+                if (!last) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) qt[c * kQN + li] = q[c];
+                } else if ((q[0] | q[1] | q[2] | q[3]) != 0) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) qt[c * kQN + li] = 0;
+                    long long *g = g_mom + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (q[c]) atomicAdd((unsigned long long *)(g + c), (unsigned long long)q[c]);
+                }
+            }
+            for (int li = tid; li < kCN; li += kP2GThreads) {
+                const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
+                const int sidx = tx * kCSX + ty * kCSY + tz;
+                long long q[2];
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const unsigned lo = clo[c][sidx];
+                    const int hi = chi[c][sidx];
+                    q[c] = ct[c * kCN + li];
+                    if ((lo | (unsigned)hi) != 0u) {
+                        clo[c][sidx] = 0u;
+                        chi[c][sidx] = 0;
+                        q[c] += plane_value(lo, hi);
+                    }
+                }
+                if (!last) {
+                    ct[li] = q[0];
+                    ct[kCN + li] = q[1];
+                } else if ((q[0] | q[1]) != 0) {
+                    ct[li] = 0;
+                    ct[kCN + li] = 0;
+                    long long *g = g_dmg + 2 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
+                                                (org[2] - 1 + tz));
+                    if (q[0]) atomicAdd((unsigned long long *)g, (unsigned long long)q[0]);
+                    if (q[1]) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q[1]);
+                }
+            }
+            if (last) break;
+            __syncthreads();                                    // the planes are clear for the next chunk
         }
         // a sub-block denser than the fixed-point headroom allows: its nodes'
         // sums are not guaranteed exact; counted for the status
         if (tid == 0 && item_n > kDenseSubblock) atomicAdd(&w.ctrl[sid].dense_subblocks, 1u);
-        // ---------------- flush: one atomic per touched node and component, and
-        // mark the touched 4^3 grid blocks.  Quadratic node 4s+l lies in grid
-        // block s+(l>>2), cubic node 4s-1+l in block s-1+((l+3)>>2), sub-block s
-        // being grid block s; s_bmark is indexed from s-1 per axis.
-        for (int li = tid; li < kQN; li += kP2GThreads) {
-            const long long q0 = qt[li], q1 = qt[kQN + li], q2 = qt[2 * kQN + li], q3 = qt[3 * kQN + li];
-            if ((q0 | q1 | q2 | q3) != 0) {
-                qt[li] = 0; qt[kQN + li] = 0; qt[2 * kQN + li] = 0; qt[3 * kQN + li] = 0;
-                const int tx = li / (kQE * kQE), ty = (li / kQE) % kQE, tz = li % kQE;
-                long long *g = g_mom + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
-                if (q0) atomicAdd((unsigned long long *)g, (unsigned long long)q0);
-                if (q1) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q1);
-                if (q2) atomicAdd((unsigned long long *)(g + 2), (unsigned long long)q2);
-                if (q3) atomicAdd((unsigned long long *)(g + 3), (unsigned long long)q3);
-                s_bmark[(((tx >> 2) + 1) * 3 + ((ty >> 2) + 1)) * 3 + ((tz >> 2) + 1)] = 1;
-            }
-        }
-        for (int li = tid; li < kCN; li += kP2GThreads) {
-            const long long q0 = ct[li], q1 = ct[kCN + li];
-            if ((q0 | q1) != 0) {
-                ct[li] = 0; ct[kCN + li] = 0;
-                const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
-                long long *g = g_dmg + 2 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
-                                            (org[2] - 1 + tz));
-                if (q0) atomicAdd((unsigned long long *)g, (unsigned long long)q0);
-                if (q1) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q1);
-                s_bmark[(((tx + 3) >> 2) * 3 + ((ty + 3) >> 2)) * 3 + ((tz + 3) >> 2)] = 1;
-            }
-        }
         __syncthreads();
         if (tid < 27 && s_bmark[tid]) {
             s_bmark[tid] = 0;

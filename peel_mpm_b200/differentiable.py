@@ -2,8 +2,9 @@
 
 ``rollout(sim, n_steps, mu=..., lam=..., sigma_c=..., A0=..., v0=...)``
 writes the given per-particle parameters (and initial velocity) into ``sim``,
-advances it ``n_steps`` substeps and returns the final positions (N,3) as a
-tensor that carries the autograd graph back to those inputs.  The backward
+advances it ``n_steps`` substeps and returns the final positions (N,3) (with
+``outputs="xv"``, the final positions and velocities) as tensors that carry
+the autograd graph back to those inputs.  The backward
 pass never stores the whole trajectory: the forward keeps the mutable state
 (x, v, F, C, d, lap, D_hist) every ``checkpoint_every`` substeps; the backward
 re-runs each segment from its checkpoint while recording every substep's grid
@@ -93,15 +94,15 @@ class _Recorder:
 
     def record(self, state0, k: int, time0: float, step0: int):
         """Run k substeps from state0 (recording slots 0..k-1); states[j] is
-        the state before substep j, states[k] the final one."""
+        the state before substep j, states[k] the final one.  Each recorded
+        substep reads states[j] and writes states[j + 1] (out of place)."""
         sim, lib = self.sim, self.lib
         self.states[0].copy_(state0)
         for j in range(k):
-            self.states[j + 1].copy_(self.states[j])
             clk = sim._clock(time0 + j * sim.dt, step0 + j)
-            _lib.check(lib.pm_substep_record(C.byref(self.prm), C.byref(self.descr[j + 1]), sim._ws.data_ptr(),
-                                             sim._ws_bytes, C.byref(clk), self.tape.data_ptr(), self.tape_bytes,
-                                             self.slots, j, self.stream), "pm_substep_record")
+            _lib.check(lib.pm_substep_record(C.byref(self.prm), C.byref(self.descr[j]), C.byref(self.descr[j + 1]),
+                                             sim._ws.data_ptr(), sim._ws_bytes, C.byref(clk), self.tape.data_ptr(),
+                                             self.tape_bytes, self.slots, j, self.stream), "pm_substep_record")
 
 
 class _Rollout(torch.autograd.Function):
@@ -135,10 +136,10 @@ class _Rollout(torch.autograd.Function):
         ctx.meta = (n_steps, time0, every, step0)
         ctx.checkpoints = checkpoints
         ctx.rec = rec
-        return sim.x.clone()
+        return sim.x.clone(), sim.v.clone()
 
     @staticmethod
-    def backward(ctx, gx):
+    def backward(ctx, gx, gv):
         sim, rec = ctx.sim, ctx.rec
         n_steps, time0, every, step0 = ctx.meta
         lib = rec.lib
@@ -146,7 +147,9 @@ class _Rollout(torch.autograd.Function):
         n, stride = sim.n, sim._S.stride(0)
         a_in = torch.zeros((_MUTABLE, stride), device=dev, dtype=torch.float32)
         a_out = torch.zeros_like(a_in)
+        o = _PLANES["v"][0]
         a_in[0:3, :n] = gx.t().to(torch.float32)
+        a_in[o:o + 3, :n] = gv.t().to(torch.float32)
         pg = torch.zeros((12, stride), device=dev, dtype=torch.float32)   # mu lam sigma_c A0(9)
         grads = _lib.pm_param_adj()
         grads.plane_stride = stride
@@ -165,7 +168,6 @@ class _Rollout(torch.autograd.Function):
                                                   C.byref(ai), C.byref(ao), C.byref(grads), rec.tape.data_ptr(),
                                                   rec.tape_bytes, rec.slots, j, rec.stream), "pm_substep_adjoint")
                 a_in, a_out = a_out, a_in
-        o = _PLANES["v"][0]
         g_mu = pg[0, :n].clone()
         g_lam = pg[1, :n].clone()
         g_sc = pg[2, :n].clone()
@@ -202,10 +204,12 @@ def auto_segment(sim: AnisoMPM, n_steps: int, memory_fraction: float = 0.5) -> i
 
 
 def rollout(sim: AnisoMPM, n_steps: int, mu=None, lam=None, sigma_c=None, A0=None, v0=None,
-            time0: float = 0.0, checkpoint_every=10):
+            time0: float = 0.0, checkpoint_every=10, outputs: str = "x"):
     """Final positions after ``n_steps`` substeps, differentiable with respect
     to the given per-particle mu, lam, sigma_c, A0 and initial velocity v0
-    (any left as None is taken from ``sim`` as a constant).
+    (any left as None is taken from ``sim`` as a constant).  ``outputs``:
+    "x" returns the final positions (N,3), "v" the final velocities, "xv"
+    the pair (a loss may use both).
 
     ``checkpoint_every`` = k: the forward keeps the state every k substeps and
     records the last segment; the backward re-runs every other segment from
@@ -217,12 +221,15 @@ def rollout(sim: AnisoMPM, n_steps: int, mu=None, lam=None, sigma_c=None, A0=Non
         checkpoint_every = auto_segment(sim, n_steps)
     if not isinstance(checkpoint_every, int) or checkpoint_every < 1:
         raise ValueError("checkpoint_every must be an int >= 1 or 'auto'")
+    if outputs not in ("x", "v", "xv"):
+        raise ValueError("outputs must be 'x', 'v' or 'xv'")
     mu = sim.mu.detach().clone() if mu is None else mu
     lam = sim.lam.detach().clone() if lam is None else lam
     sigma_c = sim.sigma_c.detach().clone() if sigma_c is None else sigma_c
     A0 = sim.A0.detach().clone() if A0 is None else A0
     v0 = sim.v.detach().clone() if v0 is None else v0
-    return _Rollout.apply(mu, lam, sigma_c, A0, v0, sim, int(n_steps), float(time0), int(checkpoint_every))
+    xT, vT = _Rollout.apply(mu, lam, sigma_c, A0, v0, sim, int(n_steps), float(time0), int(checkpoint_every))
+    return {"x": xT, "v": vT, "xv": (xT, vT)}[outputs]
 
 
 STATE_FIELDS = ("x", "v", "F", "C", "d", "lap", "D_hist")
@@ -250,11 +257,10 @@ def substep_vjp(sim: AnisoMPM, time: float, bars: dict):
     _lib.check(lib.pm_tape_init(tape.data_ptr(), tape_bytes, n, sim.n_grid, 1, st), "pm_tape_init")
     states = torch.empty((2, _MUTABLE, stride), device=dev, dtype=torch.float32)
     states[0].copy_(sim._S[:_MUTABLE])
-    states[1].copy_(states[0])
     pre, post = _particles_at(sim, P, states[0]), _particles_at(sim, P, states[1])
     clk = sim._clock(time, sim._step)
-    _lib.check(lib.pm_substep_record(C.byref(prm), C.byref(post), sim._ws.data_ptr(), sim._ws_bytes, C.byref(clk),
-                                     tape.data_ptr(), tape_bytes, 1, 0, st), "pm_substep_record")
+    _lib.check(lib.pm_substep_record(C.byref(prm), C.byref(pre), C.byref(post), sim._ws.data_ptr(), sim._ws_bytes,
+                                     C.byref(clk), tape.data_ptr(), tape_bytes, 1, 0, st), "pm_substep_record")
     a_in = torch.zeros((_MUTABLE, stride), device=dev, dtype=torch.float32)
     a_out = torch.zeros_like(a_in)
     for f, val in bars.items():
