@@ -532,12 +532,12 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
                         q[c] += plane_value(lo, hi);
                     }
                 }
-                if (!last) {
+                // cleared after the last chunk whatever the value (a partial that
+                // the last chunk cancels exactly must not leak into the CTA's
+                // next sub-block)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) qt[c * kAQN + li] = q[c];
-                } else if ((q[0] | q[1] | q[2]) != 0) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) qt[c * kAQN + li] = 0;
+                for (int c = 0; c < 3; ++c) qt[c * kAQN + li] = last ? 0 : q[c];
+                if (last && (q[0] | q[1] | q[2]) != 0) {
                     long long *g = acc + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
 #pragma unroll
                     for (int c = 0; c < 3; ++c)
@@ -555,10 +555,8 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
                     chi[sidx] = 0;
                     q3 += plane_value(lo, hi);
                 }
-                if (!last) {
-                    ct[li] = q3;
-                } else if (q3 != 0) {
-                    ct[li] = 0;
+                ct[li] = last ? 0 : q3;
+                if (last && q3 != 0) {
                     long long *g = acc + 4 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
                                               (org[2] - 1 + tz));
                     atomicAdd((unsigned long long *)(g + 3), (unsigned long long)q3);

@@ -772,12 +772,12 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                         q[c] += plane_value(lo, hi);
                     }
                 }
-                if (!last) {
+                // the running sums are kept between chunks and cleared after the
+                // last one whatever their value (a partial that the last chunk
+                // cancels exactly must not leak into the CTA's next sub-block)
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) qt[c * kQN + li] = q[c];
-                } else if ((q[0] | q[1] | q[2] | q[3]) != 0) {
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) qt[c * kQN + li] = 0;
+                for (int c = 0; c < 4; ++c) qt[c * kQN + li] = last ? 0 : q[c];
+                if (last && (q[0] | q[1] | q[2] | q[3]) != 0) {
                     long long *g = g_mom + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
 #pragma unroll
                     for (int c = 0; c < 4; ++c)
@@ -799,12 +799,9 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                         q[c] += plane_value(lo, hi);
                     }
                 }
-                if (!last) {
-                    ct[li] = q[0];
-                    ct[kCN + li] = q[1];
-                } else if ((q[0] | q[1]) != 0) {
-                    ct[li] = 0;
-                    ct[kCN + li] = 0;
+                ct[li] = last ? 0 : q[0];
+                ct[kCN + li] = last ? 0 : q[1];
+                if (last && (q[0] | q[1]) != 0) {
                     long long *g = g_dmg + 2 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
                                                 (org[2] - 1 + tz));
                     if (q[0]) atomicAdd((unsigned long long *)g, (unsigned long long)q[0]);
