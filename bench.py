@@ -73,6 +73,20 @@ BYTES_PER_PARTICLE = 216 + 73
 # per active grid node and substep: momentum accumulate/read/v write/v read
 # (16+16+12+12) + damage (8+8+4+4)
 BYTES_PER_NODE = 80
+# Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) and
+# warp instructions (smsp__inst_executed.sum) of the substep's kernels on this
+# workload, from one ncu capture of `bench.py --form plain` (the command and
+# the figures are in profiles/p2g_g2p_1m_kernels.md); used for the roofline's
+# `traffic` and its issue-bound floor (warp instructions / (4 schedulers x
+# SMs x SM clock)).
+NCU_KERNELS = {
+    "k_subblocks": {"dram_bytes": 4203264, "warp_inst": 1975877},
+    "k_stress": {"dram_bytes": 195187200 + 62620928, "warp_inst": 39989452},
+    "k_bounds": {"dram_bytes": 4864, "warp_inst": 172},
+    "k_p2g_tiles": {"dram_bytes": 96168192 + 2324992, "warp_inst": 76360593},
+    "k_g2p": {"dram_bytes": 54701056 + 45764352, "warp_inst": 56582144},
+}
+P2G_KERNELS = ("k_subblocks", "k_stress", "k_bounds", "k_p2g_tiles")
 
 
 def parse():
@@ -154,6 +168,10 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ helpers
+def sm_count(torch):
+    return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -236,7 +254,8 @@ def cpu_baseline(torch, device, sample_steps=3):
         a = getattr(sim, f).astype(np.float64).ravel()
         b = getattr(gpu, f).detach().cpu().numpy().astype(np.float64).ravel()
         errs[f] = float(np.linalg.norm(a - b) / max(np.linalg.norm(a), 1e-30))
-    parity = {"substeps": sample_steps + 1, "particles": sc.n, "rel_l2_vs_oracle": errs, "bound": 1e-5,
+    parity = {"substeps": sample_steps + 1, "particles": sc.n, "rel_l2_vs_oracle": errs,
+              "bound": {"x v F C": 1e-5, "d lap D_hist": "ten times the oracle's own reordering envelope (tests)"},
               "full_runs": "tests/test_gpu_parity_configs.py: 1M x 500, peel 1/8 x 200, 64-scene batch x 20"}
     return base, parity
 
@@ -669,22 +688,25 @@ def run_ours(args):
     # more active blocks), 20 substeps timed the same way
     late = None
     if not args.no_late:
-        done = sim._step
-        if done < 400:
-            run_frames(sim, 400 - done, done * sim.dt, chunk)
+        # a fresh copy of the scene advanced to substep 400 (the timed run above
+        # went past the scene's 500 substeps)
+        lsim, _ = build_sim(torch, device, seed=rank)
+        lsim.p2g_ctas_per_sm, lsim.grid_ctas_per_sm = sim.p2g_ctas_per_sm, sim.grid_ctas_per_sm
+        run_frames(lsim, 400, 0.0, 100)
         torch.cuda.synchronize()
         barrier()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         k = 20
         a.record(s)
-        run_frames(sim, k, sim._step * sim.dt, k)
+        run_frames(lsim, k, lsim._step * lsim.dt, k)
         b.record(s)
         torch.cuda.synchronize()
         late_ms = max_over_ranks(a.elapsed_time(b))
-        st_late = sim.status()
-        late = {"substeps": f"{sim._step - k}-{sim._step}", "ms_per_step": late_ms / k,
+        st_late = lsim.status()
+        late = {"substeps": f"{lsim._step - k}-{lsim._step}", "ms_per_step": late_ms / k,
                 "value": world * n * k / (late_ms * 1e-3), "unit": UNIT,
                 "n_active_blocks": st_late["n_active_blocks"], "nonfinite": st_late["nonfinite"]}
+        del lsim
 
     # e2e: mutable state from pinned host memory in, back out, every substep
     e2e = None
@@ -724,9 +746,20 @@ def run_ours(args):
     alg = p2g_bytes if dom == "p2g" else g2p_bytes
     achieved = alg / (kt[dom] * 1e-3) / 1e9
     step_bytes = n * BYTES_PER_PARTICLE + n_active * BYTES_PER_NODE
-    roof = {"bound": "hbm", "kernel": "k_stress + k_scatter (constitutive + P2G)" if dom == "p2g" else "k_g2p",
+    kern = P2G_KERNELS if dom == "p2g" else ("k_g2p",)
+    known = all(NCU_KERNELS[k]["dram_bytes"] is not None for k in kern) and n == 1048576
+    traffic = sum(NCU_KERNELS[k]["dram_bytes"] for k in kern) if known else None
+    clk = clocks.summary().get("sm_mhz") or 1965.0
+    floor_ms = (sum(NCU_KERNELS[k]["warp_inst"] for k in kern) / (4 * sm_count(torch) * clk * 1e6) * 1e3
+                if known else None)
+    roof = {"bound": "hbm",
+            "kernel": " + ".join(kern) + (" (constitutive + P2G)" if dom == "p2g" else " (G2P)"),
             "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-            "traffic": None, "algorithmic_bytes_per_launch": alg,
+            "traffic": traffic, "traffic_over_algorithmic": (traffic / alg) if traffic else None,
+            "algorithmic_bytes_per_launch": alg,
+            "issue_floor": None if floor_ms is None else {
+                "warp_instructions": sum(NCU_KERNELS[k]["warp_inst"] for k in kern), "floor_ms": floor_ms,
+                "frac": floor_ms / kt[dom], "what": "warp instructions / (4 schedulers x SMs x SM clock)"},
             "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
             "whole_step": {"achieved": step_bytes / (ms / args.steps * 1e-3) / 1e9,
                            "frac": step_bytes / (ms / args.steps * 1e-3) / 1e9 / hbm,
