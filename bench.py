@@ -692,11 +692,14 @@ def run_ours(args):
         # went past the scene's 500 substeps)
         lsim, _ = build_sim(torch, device, seed=rank)
         lsim.p2g_ctas_per_sm, lsim.grid_ctas_per_sm = sim.p2g_ctas_per_sm, sim.grid_ctas_per_sm
-        run_frames(lsim, 400, 0.0, 100)
+        k = 20
+        run_frames(lsim, 400 - k, 0.0, 100)
+        # substeps 380-400 as one k-substep frame: captures the frame's graph
+        # outside the timed region
+        run_frames(lsim, k, lsim._step * lsim.dt, k)
         torch.cuda.synchronize()
         barrier()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        k = 20
         a.record(s)
         run_frames(lsim, k, lsim._step * lsim.dt, k)
         b.record(s)

@@ -476,6 +476,13 @@ __device__ __forceinline__ void mmt3_rn(const float *A, const float *B, float *C
     for (int k = 0; k < 9; ++k) Cm[k] = T[k];
 }
 
+// Packed float32 pairs: sm_100's FFMA2 / FMUL2 / FADD2 issue two independent
+// IEEE round-to-nearest operations as one instruction (each lane rounds as
+// the scalar operation would), halving the issue slots of paired arithmetic.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+
 __device__ __forceinline__ float nan_to_num(float a) {
     if (a != a) return 0.0f;
     if (a > 3.402823466e38f) return 3.402823466e38f;

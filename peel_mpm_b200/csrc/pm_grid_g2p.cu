@@ -265,65 +265,11 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
     const long long ps = P.ps;
     const int ng = prm.n_grid;
     const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx, dt = (float)prm.dt;
-    // Quadratic gather (anisompm.py:749-760) as a contraction over z, then y,
-    // then x: with u = w g and dpos_j = (o_j - fx_j) dx,
-    //   v = sum_x wx T[x],  C_.x = sum_x wx DX T[x],  C_.y = sum_x wx Ty[x],
-    //   C_.z = sum_x wx Tz[x],  where T[x] = sum_{y,z} wy wz g,
-    //   Ty[x] = sum_{y,z} wy DY wz g and Tz[x] = sum_{y,z} wy wz DZ g,
-    // so every node costs 9 FMAs and one float4 load.
-    float nv[3] = {0.0f, 0.0f, 0.0f}, nC[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) nC[k] = 0.0f;
-    {
-        Quad q;
-        quad_weights(xp, inv_dx, ng, q);
-        int NX[3], NY[3], NZ[3];
-        float DX[3], DY[3], DZ[3];
-#pragma unroll
-        for (int o = 0; o < 3; ++o) {
-            if (TILE) {
-                NX[o] = (q.b[0] + o - lo[0]) * qd[1] * qd[2];
-                NY[o] = (q.b[1] + o - lo[1]) * qd[2];
-                NZ[o] = q.b[2] + o - lo[2];
-            } else {
-                NX[o] = clampi(q.b[0] + o, 0, ng - 1) * ng * ng;
-                NY[o] = clampi(q.b[1] + o, 0, ng - 1) * ng;
-                NZ[o] = clampi(q.b[2] + o, 0, ng - 1);
-            }
-            DX[o] = ((float)o - q.fx[0]) * dx;
-            DY[o] = ((float)o - q.fx[1]) * dx;
-            DZ[o] = ((float)o - q.fx[2]) * dx;
-        }
-#pragma unroll
-        for (int ox = 0; ox < 3; ++ox) {
-            float T[3] = {0.0f, 0.0f, 0.0f}, Ty[3] = {0.0f, 0.0f, 0.0f}, Tz[3] = {0.0f, 0.0f, 0.0f};
-#pragma unroll
-            for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                for (int oz = 0; oz < 3; ++oz) {
-                    const int node = NX[ox] + NY[oy] + NZ[oz];
-                    const float4 g = TILE ? sq[node] : __ldg(&gvel[node]);
-                    const float wyz = q.w[oy][1] * q.w[oz][2], wyzy = wyz * DY[oy], wyzz = wyz * DZ[oz];
-                    T[0] += wyz * g.x; T[1] += wyz * g.y; T[2] += wyz * g.z;
-                    Ty[0] += wyzy * g.x; Ty[1] += wyzy * g.y; Ty[2] += wyzy * g.z;
-                    Tz[0] += wyzz * g.x; Tz[1] += wyzz * g.y; Tz[2] += wyzz * g.z;
-                }
-            const float wx = q.w[ox][0], wxd = wx * DX[ox];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                nv[i] += wx * T[i];
-                nC[3 * i] += wxd * T[i];
-                nC[3 * i + 1] += wx * Ty[i];
-                nC[3 * i + 2] += wx * Tz[i];
-            }
-        }
-        const float cfac = (float)(4.0 * prm.inv_dx * prm.inv_dx);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) nC[k] *= cfac;
-    }
-    // Cubic Laplacian gather (anisompm.py:781-791): for each (x, y) column
-    // A = sum_z wz gd and B = sum_z w''z gd, then
-    // lap = sum_{x,y} (w''x wy + wx w''y) A + wx wy B.
+    // Cubic Laplacian gather first (anisompm.py:781-791; only lap stays live
+    // across the quadratic gather): for each (x, y) column
+    // A = sum_z wz gd and B = sum_z w''z gd; per x, SA = sum_y wy A,
+    // SA2 = sum_y w''y A, SB = sum_y wy B; then
+    // lap = sum_x w''x SA + wx (SA2 + SB).
     float lap = 0.0f;
     {
         Cubic c;
@@ -342,7 +288,8 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
             }
         }
 #pragma unroll
-        for (int ox = 0; ox < 4; ++ox)
+        for (int ox = 0; ox < 4; ++ox) {
+            float SA = 0.0f, SA2 = 0.0f, SB = 0.0f;
 #pragma unroll
             for (int oy = 0; oy < 4; ++oy) {
                 float A = 0.0f, B = 0.0f;
@@ -353,11 +300,77 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
                     A += c.w[oz][2] * gd;
                     B += c.w2[oz][2] * gd;
                 }
-                const float ab = c.w2[ox][0] * c.w[oy][1] + c.w[ox][0] * c.w2[oy][1];
-                const float e = c.w[ox][0] * c.w[oy][1];
-                lap += ab * A + e * B;
+                SA += c.w[oy][1] * A;
+                SA2 += c.w2[oy][1] * A;
+                SB += c.w[oy][1] * B;
             }
+            lap += c.w2[ox][0] * SA + c.w[ox][0] * (SA2 + SB);
+        }
         lap *= (float)(prm.inv_dx * prm.inv_dx);
+    }
+    // Quadratic gather (anisompm.py:749-760) as a contraction over z, then y,
+    // then x: with dpos_j = (o_j - fx_j) dx,
+    //   Z0[x,y] = sum_z wz g,  Zd[x,y] = sum_z (wz DZ) g         (per column)
+    //   T[x] = sum_y wy Z0,  Ty[x] = sum_y (wy DY) Z0,  Tz[x] = sum_y wy Zd
+    //   v = sum_x wx T,  C_.x = sum_x (wx DX) T,  C_.y = sum_x wx Ty,  C_.z = sum_x wx Tz
+    // so every node costs 6 FMAs and one float4 load, every column 9 more.
+    float nv[3] = {0.0f, 0.0f, 0.0f}, nC[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) nC[k] = 0.0f;
+    {
+        Quad q;
+        quad_weights(xp, inv_dx, ng, q);
+        int NX[3], NY[3], NZ[3];
+        float wzd[3], wyd[3], wxd[3];
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            if (TILE) {
+                NX[o] = (q.b[0] + o - lo[0]) * qd[1] * qd[2];
+                NY[o] = (q.b[1] + o - lo[1]) * qd[2];
+                NZ[o] = q.b[2] + o - lo[2];
+            } else {
+                NX[o] = clampi(q.b[0] + o, 0, ng - 1) * ng * ng;
+                NY[o] = clampi(q.b[1] + o, 0, ng - 1) * ng;
+                NZ[o] = clampi(q.b[2] + o, 0, ng - 1);
+            }
+            wxd[o] = q.w[o][0] * (((float)o - q.fx[0]) * dx);
+            wyd[o] = q.w[o][1] * (((float)o - q.fx[1]) * dx);
+            wzd[o] = q.w[o][2] * (((float)o - q.fx[2]) * dx);
+        }
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox) {
+            float T[3] = {0.0f, 0.0f, 0.0f}, Ty[3] = {0.0f, 0.0f, 0.0f}, Tz[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy) {
+                float Z0[3] = {0.0f, 0.0f, 0.0f}, Zd[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) {
+                    const int node = NX[ox] + NY[oy] + NZ[oz];
+                    const float4 g = TILE ? sq[node] : __ldg(&gvel[node]);
+                    const float wz = q.w[oz][2], wd = wzd[oz];
+                    Z0[0] += wz * g.x; Z0[1] += wz * g.y; Z0[2] += wz * g.z;
+                    Zd[0] += wd * g.x; Zd[1] += wd * g.y; Zd[2] += wd * g.z;
+                }
+                const float wy = q.w[oy][1], wd = wyd[oy];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    T[i] += wy * Z0[i];
+                    Ty[i] += wd * Z0[i];
+                    Tz[i] += wy * Zd[i];
+                }
+            }
+            const float wx = q.w[ox][0], wd = wxd[ox];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                nv[i] += wx * T[i];
+                nC[3 * i] += wd * T[i];
+                nC[3 * i + 1] += wx * Ty[i];
+                nC[3 * i + 2] += wx * Tz[i];
+            }
+        }
+        const float cfac = (float)(4.0 * prm.inv_dx * prm.inv_dx);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) nC[k] *= cfac;
     }
     // advection, F update, domain clamp (793-802).  These accumulate over every
     // substep, so each multiply and add is rounded separately as in the

@@ -18,8 +18,8 @@
 // then one work item per (cell, x-slab): all particles of a cell share their
 // quadratic base, so an item sums the cell's contributions to 9 quadratic
 // nodes (3 slabs) or 25 cubic nodes (5 slabs; a cell's cubic stencils span
-// 5^3 nodes) in float registers, in the sorted order, and adds each node
-// once.  Tiles and the global grid accumulate int64 fixed point (units from
+// 5^3 nodes) in float registers (packed pairs: sm_100's FFMA2 issues two
+// FMAs per instruction), in the sorted order, and adds each node once.  Tiles and the global grid accumulate int64 fixed point (units from
 // the control block's bounds): integer addition is associative, so the grid
 // sums, and with them the whole substep, are the same bits whatever order the
 // atomics run in.  The tiles are flushed with one atomic per touched node and
@@ -35,7 +35,12 @@ namespace pm {
 
 constexpr int kP2GThreads = 256;
 constexpr int kPay = 17;         // payload floats: x(3) mv(3) affine(9) m d
+// Payload rows are padded by one word per 32 particles: the lanes of an item
+// warp read particle j of 32 different cells, whose sorted positions are
+// close to multiples of the cell occupancy (8): unpadded, those fall on 4
+// banks; padded, on distinct ones.
 constexpr int kPayStride = kP2GThreads + kP2GThreads / 32;
+__device__ __forceinline__ int pay_col(int j) { return j + (j >> 5); }
 
 __device__ __forceinline__ float clamp_min(float v, float lo) { return v < lo ? lo : v; }   // torch.clamp(min=)
 __device__ __forceinline__ float relu(float v) { return v > 0.0f ? v : (v != v ? v : 0.0f); }
@@ -47,14 +52,15 @@ __device__ __forceinline__ float tmax(float a, float b) { return (a != a || b !=
 // When `rec` is set (recording a substep for the adjoint) the polar
 // decomposition (R, V, S) and, on damage steps, phi are written to its planes:
 // rec[k * rs + p] for R (k 0..8), V (9..17), S (18..20), phi (21).
-// Per-particle inputs of k_stress, all loaded before any store: the state
-// planes share one buffer, so a store would otherwise keep later loads from
-// being issued early.
+// Per-particle inputs of the constitutive update, all loaded before any
+// store (the state planes share one buffer, so a store would otherwise keep
+// later loads from being issued early).  The inputs of the affine term and
+// the payload (C, v, x, vol0, mass, grip) are loaded after it: they are not
+// needed earlier, and holding them across the eigensolve costs registers.
 struct StressIn {
-    float F[9], C[9], A0[9], v[3], x[3];
-    float d, lap, Dh, mu, lam, sc, eta, zeta, l0, res, vol0, m;
+    float F[9], A0[9];
+    float d, lap, Dh, mu, lam, sc, eta, zeta, l0, res;
     bool allow;
-    int grip;
 };
 
 __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &P, long long p, bool do_damage,
@@ -275,13 +281,7 @@ __global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, c
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
         in.F[k] = P.F[k * ps + p];
-        in.C[k] = P.C[k * ps + p];
         in.A0[k] = do_damage ? P.A0[k * ps + p] : 0.0f;
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        in.v[k] = P.v[k * ps + p];
-        in.x[k] = P.x[k * ps + p];
     }
     in.d = P.d[p];
     in.lap = P.lap[p];
@@ -293,10 +293,7 @@ __global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, c
     in.zeta = P.zeta[p];
     in.l0 = P.l0[p];
     in.res = P.residual[p];
-    in.vol0 = P.vol0[p];
-    in.m = P.mass[p];
     in.allow = P.allow[p] != 0;
-    in.grip = P.grip_tag ? P.grip_tag[p] : -1;
     float tau[9];
     float d_new = in.d;
     constitutive(prm, P, p, do_damage, in, tau, d_new, w.tape_pol, w.tape_aff_stride);
@@ -304,27 +301,33 @@ __global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, c
         P.d_o[p] = d_new;
         if (!do_damage) P.Dho[p] = in.Dh;
     }
-    float v[3] = {in.v[0], in.v[1], in.v[2]};
+    float Cp[9], v[3], xp[3];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Cp[k] = P.C[k * ps + p];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v[k] = P.v[k * ps + p];
+        xp[k] = P.x[k * ps + p];
+    }
+    const float vol0 = P.vol0[p], m = P.mass[p];
     {                                                                // particle BCs (601-602)
-        const int g = in.grip;
+        const int g = P.grip_tag ? P.grip_tag[p] : -1;
         if (g >= 0 && g < prm.n_grips) {
             const double f = prm.grips[g].ramp > 0.0 ? fmin(ctrl->time / prm.grips[g].ramp, 1.0) : 1.0;
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) v[ax] = (float)(prm.grips[g].vel[ax] * f);
         }
     }
-    const float m = in.m;
     // stress_coeff = -dt*vol0*4*inv_dx*inv_dx; affine = coeff*tau + m*C (711-713)
     const float coeff =
-        __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), in.vol0), 4.0f), inv_dx), inv_dx);
+        __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn((float)(-prm.dt), vol0), 4.0f), inv_dx), inv_dx);
     float aff[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) aff[k] = coeff * tau[k] + m * in.C[k];
-    float xp[3], fx[3];
+    for (int k = 0; k < 9; ++k) aff[k] = coeff * tau[k] + m * Cp[k];
+    float fx[3];
     bool reg = true;
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        xp[ax] = in.x[ax];
         const float X = __fmul_rn(xp[ax], inv_dx);
         const float fb = floorf(__fsub_rn(X, 0.5f));
         reg = reg && (fb >= 1.0f) && (fb <= (float)(ng - 4));
@@ -571,7 +574,7 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
             if (valid) {
                 const float4 *src = w.payload + 5 * i;
                 const float4 q0 = src[0], q1 = src[1], q2 = src[2], q3 = src[3], q4 = src[4];
-                const int t = tid + (tid >> 5);
+                const int t = pay_col(tid);
                 pay[0][t] = q0.x; pay[1][t] = q0.y; pay[2][t] = q0.z; pay[15][t] = q0.w;
                 pay[3][t] = q1.x; pay[4][t] = q1.y; pay[5][t] = q1.z; pay[16][t] = q1.w;
                 pay[6][t] = q2.x; pay[7][t] = q2.y; pay[8][t] = q2.z; pay[9][t] = q2.w;
@@ -618,7 +621,7 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
             }
             // ---------------- particles that need clamped nodes
             if (valid && !regular[tid]) {
-                const int t = tid + (tid >> 5);
+                const int t = pay_col(tid);
                 const float xp[3] = {pay[0][t], pay[1][t], pay[2][t]};   // positions for these particles
                 const float mv[3] = {pay[3][t], pay[4][t], pay[5][t]};
                 float aff[9];
@@ -653,49 +656,44 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                 }
                 if (sl < 3) {
                     const int ox = sl;
-                    float acc[3][3][4];
+                    // packed pairs: components (0, 1) and (2, mass) of every node
+                    float2 acc[3][3][2];
 #pragma unroll
                     for (int i2 = 0; i2 < 3; ++i2)
 #pragma unroll
-                        for (int j = 0; j < 3; ++j)
-#pragma unroll
-                            for (int c = 0; c < 4; ++c) acc[i2][j][c] = 0.0f;
-                    for (int j = ja; j < jb; ++j) {
-                        if (!regular[j]) continue;
-                        const int t = j + (j >> 5);
+                        for (int j = 0; j < 3; ++j) acc[i2][j][0] = acc[i2][j][1] = make_float2(0.0f, 0.0f);
+                    const int jend = regular[ja] ? jb : ja;
+                    for (int j = ja; j < jend; ++j) {
+                        const int t = pay_col(j);
                         const float fx0 = pay[0][t], fx1 = pay[1][t], fx2 = pay[2][t];
                         float wx[3], wy[3], wz[3];
                         qw(fx0, wx); qw(fx1, wy); qw(fx2, wz);
                         const float dxo = ((float)ox - fx0) * dx;
                         const float m = pay[15][t];
-                        float base[3], ay[3], az[3];
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            base[c] = pay[3 + c][t] + pay[6 + 3 * c][t] * dxo;
-                            ay[c] = pay[7 + 3 * c][t];
-                            az[c] = pay[8 + 3 * c][t];
-                        }
+                        const float2 base01 = fma2(make_float2(pay[6][t], pay[9][t]), bc2(dxo),
+                                                   make_float2(pay[3][t], pay[4][t]));
+                        const float base2 = pay[5][t] + pay[12][t] * dxo;
+                        const float2 ay01 = make_float2(pay[7][t], pay[10][t]), az01 = make_float2(pay[8][t], pay[11][t]);
+                        const float ay2 = pay[13][t], az2 = pay[14][t];
                         const float wxs = ox == 0 ? wx[0] : (ox == 1 ? wx[1] : wx[2]);
-                        // w (mv + aff dpos) = wxy [wz (mv + aff (dx, ., dz))] + [wxy aff_y dy] wz:
-                        // the bracketed factors per oz and per oy, then 2 FMAs per node and component
-                        float bz3[3][4];
+                        float2 bz[3][2], wz2[3];
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
                             const float dz = ((float)oz - fx2) * dx;
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) bz3[oz][c] = wz[oz] * (base[c] + az[c] * dz);
-                            bz3[oz][3] = wz[oz] * m;
+                            wz2[oz] = bc2(wz[oz]);
+                            bz[oz][0] = mul2(wz2[oz], fma2(az01, bc2(dz), base01));
+                            bz[oz][1] = mul2(wz2[oz], make_float2(base2 + az2 * dz, m));
                         }
 #pragma unroll
                         for (int oy = 0; oy < 3; ++oy) {
-                            const float dy = ((float)oy - fx1) * dx;
                             const float wxy = wxs * wy[oy];
-                            const float ady[3] = {wxy * ay[0] * dy, wxy * ay[1] * dy, wxy * ay[2] * dy};
+                            const float wdy = wxy * (((float)oy - fx1) * dx);
+                            const float2 w2 = bc2(wxy);
+                            const float2 ady01 = mul2(bc2(wdy), ay01), ady2 = make_float2(wdy * ay2, 0.0f);
 #pragma unroll
                             for (int oz = 0; oz < 3; ++oz) {
-#pragma unroll
-                                for (int c = 0; c < 3; ++c) acc[oy][oz][c] += wxy * bz3[oz][c] + ady[c] * wz[oz];
-                                acc[oy][oz][3] += wxy * bz3[oz][3];
+                                acc[oy][oz][0] = fma2(ady01, wz2[oz], fma2(w2, bz[oz][0], acc[oy][oz][0]));
+                                acc[oy][oz][1] = fma2(ady2, wz2[oz], fma2(w2, bz[oz][1], acc[oy][oz][1]));
                             }
                         }
                     }
@@ -705,50 +703,44 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
                             const int sidx = nx * kQSX + (cq[1] + oy) * kQSY + cq[2] + oz;
-#pragma unroll
-                            for (int c = 0; c < 4; ++c)
-                                plane_add(&qlo[c][sidx], &qhi[c][sidx], acc[oy][oz][c], scl[c == 3 ? 1 : 0]);
+                            plane_add(&qlo[0][sidx], &qhi[0][sidx], acc[oy][oz][0].x, scl[0]);
+                            plane_add(&qlo[1][sidx], &qhi[1][sidx], acc[oy][oz][0].y, scl[0]);
+                            plane_add(&qlo[2][sidx], &qhi[2][sidx], acc[oy][oz][1].x, scl[0]);
+                            plane_add(&qlo[3][sidx], &qhi[3][sidx], acc[oy][oz][1].y, scl[1]);
                         }
                 } else {
                     const int nxs = sl - 3;
-                    float adc[5][5], adw[5][5];
+                    float2 acw[5][5];   // packed pairs (sum w d, sum w) of every node
 #pragma unroll
                     for (int i2 = 0; i2 < 5; ++i2)
 #pragma unroll
-                        for (int j = 0; j < 5; ++j) adc[i2][j] = adw[i2][j] = 0.0f;
-                    for (int j = ja; j < jb; ++j) {
-                        if (!regular[j]) continue;
-                        const int t = j + (j >> 5);
+                        for (int j = 0; j < 5; ++j) acw[i2][j] = make_float2(0.0f, 0.0f);
+                    const int jend = regular[ja] ? jb : ja;
+                    for (int j = ja; j < jend; ++j) {
+                        const int t = pay_col(j);
                         const float wxs = cwt[nxs][t];
-                        float ey[5], ez[5];
+                        const float d = pay[16][t];
+                        float2 ez2[5];
 #pragma unroll
                         for (int k = 0; k < 5; ++k) {
-                            ey[k] = cwt[5 + k][t];
-                            ez[k] = cwt[10 + k][t];
+                            const float ez = cwt[10 + k][t];
+                            ez2[k] = make_float2(d * ez, ez);
                         }
-                        const float d = pay[16][t];
-                        float ezd[5];   // d wz, hoisted: 2 FMAs per node
-#pragma unroll
-                        for (int k = 0; k < 5; ++k) ezd[k] = d * ez[k];
 #pragma unroll
                         for (int ny = 0; ny < 5; ++ny) {
-                            const float wxy = wxs * ey[ny];
+                            const float2 w2 = bc2(wxs * cwt[5 + ny][t]);
 #pragma unroll
-                            for (int nz = 0; nz < 5; ++nz) {
-                                adc[ny][nz] += wxy * ezd[nz];
-                                adw[ny][nz] += wxy * ez[nz];
-                            }
+                            for (int nz = 0; nz < 5; ++nz) acw[ny][nz] = fma2(w2, ez2[nz], acw[ny][nz]);
                         }
                     }
-                    // cubic tile origin is 4s - 1, the cell's 5 nodes start at qb - 1
                     const int nx = cq[0] + nxs;
 #pragma unroll
                     for (int ny = 0; ny < 5; ++ny)
 #pragma unroll
                         for (int nz = 0; nz < 5; ++nz) {
                             const int sidx = nx * kCSX + (cq[1] + ny) * kCSY + cq[2] + nz;
-                            plane_add(&clo[0][sidx], &chi[0][sidx], adc[ny][nz], scl[2]);
-                            plane_add(&clo[1][sidx], &chi[1][sidx], adw[ny][nz], scl[3]);
+                            plane_add(&clo[0][sidx], &chi[0][sidx], acw[ny][nz].x, scl[2]);
+                            plane_add(&clo[1][sidx], &chi[1][sidx], acw[ny][nz].y, scl[3]);
                         }
                 }
             }
