@@ -106,6 +106,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-late", action="store_true", help="skip the late-run (substeps 400-420) sample")
+    ap.add_argument("--adj-steps", type=int, default=100,
+                    help="substeps of the differentiable rollout (the workload's 100; fewer for profiling)")
     return ap.parse_args()
 
 
@@ -691,7 +693,8 @@ def run_ours(args):
         # a fresh copy of the scene advanced to substep 400 (the timed run above
         # went past the scene's 500 substeps)
         lsim, _ = build_sim(torch, device, seed=rank)
-        lsim.p2g_ctas_per_sm, lsim.grid_ctas_per_sm = sim.p2g_ctas_per_sm, sim.grid_ctas_per_sm
+        for knob in autotune.KNOBS:
+            setattr(lsim, knob, getattr(sim, knob))
         k = 20
         run_frames(lsim, 400 - k, 0.0, 100)
         # substeps 380-400 as one k-substep frame: captures the frame's graph
@@ -774,7 +777,8 @@ def run_ours(args):
     if rank == 0 and args.form in ("all", "render"):
         forms["render"] = bench_render(torch, device, sim)
     if rank == 0 and args.form in ("all", "adjoint"):
-        forms["fwd_adjoint"] = bench_adjoint(torch, device, fd_dirs=args.fd_dirs, fd_window=args.fd_window)
+        forms["fwd_adjoint"] = bench_adjoint(torch, device, n_steps=args.adj_steps, every=min(10, args.adj_steps),
+                                             fd_dirs=args.fd_dirs, fd_window=args.fd_window)
 
     cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

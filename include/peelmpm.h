@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define PM_ABI_VERSION 1
+#define PM_ABI_VERSION 2
 #define PM_MAX_GRIPS 32
 #define PM_MAX_COLLIDERS 8
 
@@ -82,6 +82,12 @@ typedef struct pm_params {
                                    tuning knob with no effect on results (the grid sums are exact) */
     int32_t grid_ctas_per_sm;   /* grid-update CTAs per SM (0: the library default, else 1..64); a
                                    tuning knob with no effect on results */
+    int32_t stress_ctas_per_sm; /* resident constitutive-update CTAs per SM: 0 or 3 (the 80-register
+                                   build), 4 (the 64-register build); a tuning knob with no effect on
+                                   results */
+    int32_t g2p_ctas_per_sm;    /* resident G2P CTAs per SM: 0 (the library default: 4 for one scene,
+                                   3 for a batch), 3 (the 80-register build) or 4 (the 64-register
+                                   build); a tuning knob with no effect on results */
     pm_grip grips[PM_MAX_GRIPS];
     pm_collider colliders[PM_MAX_COLLIDERS];
 } pm_params;
@@ -206,8 +212,9 @@ int pm_read_status(const void *ws, size_t ws_bytes, int64_t n, int32_t n_grid, p
  * reference gets these from PyTorch autograd through substep()
  * (anisompm.py:593-803); here the caller records each forward substep of a
  * checkpoint segment into a tape slot and then runs pm_substep_adjoint from
- * the last slot to the first.  Not supported (PM_ERR_ARG): f_clamp,
- * colliders, interface particles. */
+ * the last slot to the first.  Every part of the substep is differentiated:
+ * grips, gravity, grid damping, damage_every, f_clamp, grid colliders (the
+ * tape then needs PM_TAPE_COLLIDERS) and interface particles. */
 
 /* Adjoints of the mutable state, same plane layout as pm_particles. */
 typedef struct pm_state_adj {
@@ -226,9 +233,15 @@ typedef struct pm_param_adj {
 
 /* Tape for `slots` recorded substeps of n particles on an n_grid^3 grid:
  * per slot 24 bytes per grid node and 124 bytes per particle, plus three
- * shared adjoint grids (48 bytes per node).  Zeroed once by pm_tape_init. */
-int pm_tape_size(int64_t n, int32_t n_grid, int32_t slots, size_t *bytes);
-int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32_t slots, void *stream);
+ * shared adjoint grids (48 bytes per node).  flags: PM_TAPE_COLLIDERS when the
+ * recorded substeps have grid colliders (each slot then also keeps the grid
+ * velocity before the colliders, 16 bytes per node); pm_substep_record and
+ * pm_substep_adjoint derive the layout from their pm_params and reject a
+ * tape sized without it.  Zeroed once by pm_tape_init. */
+#define PM_TAPE_COLLIDERS 1
+int pm_tape_size(int64_t n, int32_t n_grid, int32_t slots, int32_t flags, size_t *bytes);
+int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32_t slots, int32_t flags,
+                 void *stream);
 
 /* pm_substep that also records the substep's grid state into tape slot
  * `slot`.  out == NULL: the particle state P advances in place as in

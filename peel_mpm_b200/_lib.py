@@ -48,7 +48,7 @@ class pm_params(C.Structure):
         ("use_f_clamp", C.c_int32), ("record_stress", C.c_int32),
         ("f_clamp_lo", C.c_double), ("f_clamp_hi", C.c_double),
         ("n_grips", C.c_int32), ("n_colliders", C.c_int32), ("p2g_ctas_per_sm", C.c_int32),
-        ("grid_ctas_per_sm", C.c_int32),
+        ("grid_ctas_per_sm", C.c_int32), ("stress_ctas_per_sm", C.c_int32), ("g2p_ctas_per_sm", C.c_int32),
         ("grips", pm_grip * PM_MAX_GRIPS), ("colliders", pm_collider * PM_MAX_COLLIDERS),
     ]
 
@@ -151,8 +151,8 @@ def load():
         "pm_batch_workspace_release": (C.c_int, [vp]),
         "pm_batch_substep": (C.c_int, [i32, vp, vp, C.POINTER(pm_particles), vp, sz, vp, vp]),
         "pm_batch_read_status": (C.c_int, [vp, sz, i32, vp, vp, C.POINTER(pm_status_info), vp]),
-        "pm_tape_size": (C.c_int, [i64, i32, i32, C.POINTER(sz)]),
-        "pm_tape_init": (C.c_int, [vp, sz, i64, i32, i32, vp]),
+        "pm_tape_size": (C.c_int, [i64, i32, i32, i32, C.POINTER(sz)]),
+        "pm_tape_init": (C.c_int, [vp, sz, i64, i32, i32, i32, vp]),
         "pm_substep_record": (C.c_int, [C.POINTER(pm_params), C.POINTER(pm_particles), C.POINTER(pm_particles), vp,
                                         sz, C.POINTER(pm_clock), vp, sz, i32, i32, vp]),
         "pm_render_workspace_size": (C.c_int, [i64, i32, i32, i32, C.POINTER(sz)]),
@@ -170,7 +170,7 @@ def load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.pm_abi_version() != 1:
+    if lib.pm_abi_version() != 2:
         raise ImportError("libpeelmpm.so ABI version mismatch; rebuild it")
     _lib = lib
     return lib
@@ -235,8 +235,11 @@ def batch_workspace_layout(ns, grids) -> pm_batch_layout:
     return lay
 
 
-def tape_size(n: int, n_grid: int, slots: int) -> int:
+PM_TAPE_COLLIDERS = 1
+
+
+def tape_size(n: int, n_grid: int, slots: int, flags: int = 0) -> int:
     lib = load()
     out = C.c_size_t(0)
-    check(lib.pm_tape_size(int(n), int(n_grid), int(slots), C.byref(out)), "pm_tape_size")
+    check(lib.pm_tape_size(int(n), int(n_grid), int(slots), int(flags), C.byref(out)), "pm_tape_size")
     return int(out.value)

@@ -184,6 +184,8 @@ class AnisoMPM:
         self.use_graphs = True
         self.p2g_ctas_per_sm = 0  # launch knobs (0 = library defaults; autotune.tune sets them); results
         self.grid_ctas_per_sm = 0  # do not depend on them
+        self.stress_ctas_per_sm = 0
+        self.g2p_ctas_per_sm = 0
         self._S = None            # float32 planes (N_PLANES, stride)
         self._allow = None        # bool (N)
         self._imask = None        # bool (N)
@@ -430,6 +432,7 @@ class AnisoMPM:
         key = (self.n_grid, self.grid_lim, self.dt, self._gravity_host, self.grid_damp,
                None if self.f_clamp is None else tuple(float(v) for v in self.f_clamp), self.damage_every,
                bool(self.record_stress), int(self.p2g_ctas_per_sm), int(self.grid_ctas_per_sm),
+               int(self.stress_ctas_per_sm), int(self.g2p_ctas_per_sm),
                tuple((g.velocity, g.ramp) for g in grips),
                tuple((c.kind, c.mode, c.friction, c.radius, tuple(c.normal)) for c in self.colliders))
         if key == self._params_key:
@@ -447,6 +450,8 @@ class AnisoMPM:
         p.record_stress = int(bool(self.record_stress))
         p.p2g_ctas_per_sm = int(self.p2g_ctas_per_sm)
         p.grid_ctas_per_sm = int(self.grid_ctas_per_sm)
+        p.stress_ctas_per_sm = int(self.stress_ctas_per_sm)
+        p.g2p_ctas_per_sm = int(self.g2p_ctas_per_sm)
         p.n_grips = len(grips)
         for i, g in enumerate(grips):
             for a in range(3):

@@ -46,12 +46,18 @@ class BatchedAnisoMPM:
         self.use_graphs = use_graphs
         self.p2g_ctas_per_sm = 0  # launch knobs for the whole batch (0 = library defaults)
         self.grid_ctas_per_sm = 0
+        self.stress_ctas_per_sm = 0
+        self.g2p_ctas_per_sm = 0
         self._lib = _lib.load()
         self._graphs = {}
         self._ws = None
         self._pack()
 
     # ------------------------------------------------------------------ packing
+    def _knobs(self):
+        return (int(self.p2g_ctas_per_sm), int(self.grid_ctas_per_sm), int(self.stress_ctas_per_sm),
+                int(self.g2p_ctas_per_sm))
+
     def _pack(self):
         sims, dev = self.sims, self.device
         self.ns = [s.n for s in sims]
@@ -142,12 +148,14 @@ class BatchedAnisoMPM:
             self._tag_keys = tag_keys
             self._P = None
         prms = [s._build_params(gs) for s, gs in zip(self.sims, grips_all)]
-        keys = tuple(s._params_key for s in self.sims) + (int(self.p2g_ctas_per_sm), int(self.grid_ctas_per_sm))
+        keys = tuple(s._params_key for s in self.sims) + self._knobs()
         if keys != self._params_keys or not self._ws_ready:
             arr = (_lib.pm_params * len(prms))(*prms)
             for k in range(len(prms)):
                 arr[k].p2g_ctas_per_sm = int(self.p2g_ctas_per_sm)
                 arr[k].grid_ctas_per_sm = int(self.grid_ctas_per_sm)
+                arr[k].stress_ctas_per_sm = int(self.stress_ctas_per_sm)
+                arr[k].g2p_ctas_per_sm = int(self.g2p_ctas_per_sm)
             st = torch.cuda.current_stream(self.device).cuda_stream
             if not self._ws_ready:
                 _lib.check(self._lib.pm_batch_workspace_init(self._ws.data_ptr(), self._ws_bytes, len(prms),
@@ -226,8 +234,7 @@ class BatchedAnisoMPM:
             # keep the pinned source and device table alive until the copy and kernels ran
             self._eager_keep = (host, table)
         else:
-            key = (n_sub, id(P), self._ws.data_ptr(), self._S.data_ptr(), int(self.p2g_ctas_per_sm),
-                   int(self.grid_ctas_per_sm))
+            key = (n_sub, id(P), self._ws.data_ptr(), self._S.data_ptr()) + self._knobs()
             entry = self._graphs.get(key)
             if entry is None:
                 table = torch.empty(host.numel(), dtype=torch.uint8, device=self.device)

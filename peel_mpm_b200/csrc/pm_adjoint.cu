@@ -25,8 +25,10 @@
 //                   stress, damage and eigen-split adjoints.
 // Non-smooth operations take the branch the forward took (relu, max and clamp
 // pass the adjoint where the forward passed the value; base cells are
-// piecewise constant).  Unsupported in the adjoint (rejected by the host):
-// f_clamp, colliders and interface particles.
+// piecewise constant).  The strain limit (f_clamp) is differentiated as a
+// function of the singular values (f_clamp_adj), grid colliders from the
+// recorded pre-collider grid velocity (resolve_adj), and the directional
+// stress at interface particles by dir_adjoint.
 #include "pm_kernels.cuh"
 
 namespace pm {
@@ -43,6 +45,8 @@ struct TapeHead {
     double time;
     unsigned n_work;    // non-empty sub-blocks of the substep's sort
     unsigned pad;
+    float col_origin[PM_MAX_COLLIDERS][3];   // the substep's collider origins and velocities
+    float col_vel[PM_MAX_COLLIDERS][3];
 };
 
 // Control block of one adjoint substep: the bounds of the scatter's
@@ -152,6 +156,19 @@ __device__ __forceinline__ void g2p_tail_adj(const pm_params &prm, const float x
     for (int k = 0; k < 9; ++k) Ct[k] = a.Cb[k] + dt * FbFt[k];
 }
 
+// The F that G2P updated: with the strain limit, the limited F rebuilt from
+// the taped V and S as the forward built it.
+__device__ __forceinline__ void g2p_input_F(const pm_params &prm, const float *__restrict__ tpol, long long rs,
+                                            long long p, float F[9]) {
+    if (!prm.use_f_clamp) return;
+    float V[9], S[3];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) V[k] = tpol[(9 + k) * rs + p];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) S[k] = tpol[(18 + k) * rs + p];
+    f_clamp_F(F, V, S, (float)prm.f_clamp_lo, (float)prm.f_clamp_hi, F);
+}
+
 // ---------------------------------------------------------------- k_adj_pre
 // Adjoint of v' = sum w v_i, C' = K sum w v_i dpos^T and lap' = sum L gd_i has
 // the form of a P2G scatter: node i receives w (vt + K Ct dpos) and
@@ -162,7 +179,8 @@ constexpr int kAdjCW = 30;   // expanded cubic w and w'' per particle (5 per axi
 
 __global__ void __launch_bounds__(256) k_adj_pre(const pm_params prm, const Parts pre, const Parts post,
                                                  const pm_state_adj ain, const int *__restrict__ iperm,
-                                                 float4 *__restrict__ pay, AdjCtrl *actl) {
+                                                 float4 *__restrict__ pay, AdjCtrl *actl,
+                                                 const float *__restrict__ tpol, long long rs) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= pre.n) return;
     const long long ps = pre.ps;
@@ -178,6 +196,7 @@ __global__ void __launch_bounds__(256) k_adj_pre(const pm_params prm, const Part
     }
 #pragma unroll
     for (int k = 0; k < 9; ++k) F[k] = pre.F[k * ps + p];
+    g2p_input_F(prm, tpol, rs, p, F);
     AdjIn a;
     load_adj(ain, p, a);
     float vt[3], Ct[9];
@@ -425,45 +444,50 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
                 morton_decode(lcell[ja], cq);
                 if (sl < 3) {
                     const int ox = sl;
-                    float acc3[3][3][3];
+                    // packed pairs: components (0, 1) of every node, component 2 alone
+                    float2 acc01[3][3];
+                    float acc2[3][3];
 #pragma unroll
                     for (int i2 = 0; i2 < 3; ++i2)
 #pragma unroll
-                        for (int j = 0; j < 3; ++j)
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) acc3[i2][j][c] = 0.0f;
-                    for (int j = ja; j < jb; ++j) {
-                        if (!regular[j]) continue;
+                        for (int j = 0; j < 3; ++j) {
+                            acc01[i2][j] = make_float2(0.0f, 0.0f);
+                            acc2[i2][j] = 0.0f;
+                        }
+                    // a cell's particles share their base cell: all regular or all not
+                    const int jend = regular[ja] ? jb : ja;
+                    for (int j = ja; j < jend; ++j) {
                         const int t = j + (j >> 5);
                         const float fx0 = sp[0][t], fx1 = sp[1][t], fx2 = sp[2][t];
                         float wx[3], wy[3], wz[3];
                         qw(fx0, wx); qw(fx1, wy); qw(fx2, wz);
                         const float dxo = ((float)ox - fx0) * dx;
-                        float base[3], ay[3], az[3];
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            base[c] = sp[3 + c][t] + sp[6 + 3 * c][t] * dxo;
-                            ay[c] = sp[7 + 3 * c][t];
-                            az[c] = sp[8 + 3 * c][t];
-                        }
+                        const float2 base01 = fma2(make_float2(sp[6][t], sp[9][t]), bc2(dxo),
+                                                   make_float2(sp[3][t], sp[4][t]));
+                        const float base2 = sp[5][t] + sp[12][t] * dxo;
+                        const float2 ay01 = make_float2(sp[7][t], sp[10][t]), az01 = make_float2(sp[8][t], sp[11][t]);
+                        const float ay2 = sp[13][t], az2 = sp[14][t];
                         const float wxs = ox == 0 ? wx[0] : (ox == 1 ? wx[1] : wx[2]);
-                        float bz3[3][3];
+                        // w (base + a_y dy + a_z dz) = wxy [wz (base + a_z dz)] + [wxy a_y dy] wz
+                        float2 bz01[3], wz2[3];
+                        float bz2[3];
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
                             const float dz = ((float)oz - fx2) * dx;
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) bz3[oz][c] = base[c] + az[c] * dz;
+                            wz2[oz] = bc2(wz[oz]);
+                            bz01[oz] = mul2(wz2[oz], fma2(az01, bc2(dz), base01));
+                            bz2[oz] = wz[oz] * (base2 + az2 * dz);
                         }
 #pragma unroll
                         for (int oy = 0; oy < 3; ++oy) {
-                            const float dy = ((float)oy - fx1) * dx;
                             const float wxy = wxs * wy[oy];
-                            const float ady[3] = {ay[0] * dy, ay[1] * dy, ay[2] * dy};
+                            const float wdy = wxy * (((float)oy - fx1) * dx);
+                            const float2 w2 = bc2(wxy), ady01 = mul2(bc2(wdy), ay01);
+                            const float ady2 = wdy * ay2;
 #pragma unroll
                             for (int oz = 0; oz < 3; ++oz) {
-                                const float wk = wxy * wz[oz];
-#pragma unroll
-                                for (int c = 0; c < 3; ++c) acc3[oy][oz][c] += wk * (bz3[oz][c] + ady[c]);
+                                acc01[oy][oz] = fma2(ady01, wz2[oz], fma2(w2, bz01[oz], acc01[oy][oz]));
+                                acc2[oy][oz] = fmaf(ady2, wz[oz], fmaf(wxy, bz2[oz], acc2[oy][oz]));
                             }
                         }
                     }
@@ -473,34 +497,37 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
 #pragma unroll
                         for (int oz = 0; oz < 3; ++oz) {
                             const int sidx = nx * kAQSX + (cq[1] + oy) * kAQSY + cq[2] + oz;
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) plane_add(&qlo[c][sidx], &qhi[c][sidx], acc3[oy][oz][c], smom);
+                            plane_add(&qlo[0][sidx], &qhi[0][sidx], acc01[oy][oz].x, smom);
+                            plane_add(&qlo[1][sidx], &qhi[1][sidx], acc01[oy][oz].y, smom);
+                            plane_add(&qlo[2][sidx], &qhi[2][sidx], acc2[oy][oz], smom);
                         }
                 } else {
                     const int nxs = sl - 3;
-                    float al[5][5];
+                    // packed pairs of z-neighbours: nodes (0, 1), (2, 3) of a row, node 4 alone
+                    float2 al01[5], al23[5];
+                    float al4[5];
 #pragma unroll
-                    for (int i2 = 0; i2 < 5; ++i2)
-#pragma unroll
-                        for (int j = 0; j < 5; ++j) al[i2][j] = 0.0f;
-                    for (int j = ja; j < jb; ++j) {
-                        if (!regular[j]) continue;
+                    for (int i2 = 0; i2 < 5; ++i2) {
+                        al01[i2] = al23[i2] = make_float2(0.0f, 0.0f);
+                        al4[i2] = 0.0f;
+                    }
+                    const int jend = regular[ja] ? jb : ja;
+                    for (int j = ja; j < jend; ++j) {
                         const int t = j + (j >> 5);
                         const float lb = sp[16][t];
                         const float ax = lb * cw[15 + nxs][t], bx2 = lb * cw[nxs][t];   // lb w''x, lb wx
-                        float ez[5], e2z[5];
-#pragma unroll
-                        for (int k = 0; k < 5; ++k) {
-                            ez[k] = cw[10 + k][t];
-                            e2z[k] = cw[25 + k][t];
-                        }
+                        const float2 ez01 = make_float2(cw[10][t], cw[11][t]), ez23 = make_float2(cw[12][t], cw[13][t]);
+                        const float2 e2z01 = make_float2(cw[25][t], cw[26][t]), e2z23 = make_float2(cw[27][t], cw[28][t]);
+                        const float ez4 = cw[14][t], e2z4 = cw[29][t];
 #pragma unroll
                         for (int ny = 0; ny < 5; ++ny) {
                             const float wy = cw[5 + ny][t], w2y = cw[20 + ny][t];
                             const float t1 = ax * wy + bx2 * w2y;   // (w''x wy + wx w''y) lb
                             const float t2 = bx2 * wy;              // wx wy lb
-#pragma unroll
-                            for (int nz = 0; nz < 5; ++nz) al[ny][nz] += t1 * ez[nz] + t2 * e2z[nz];
+                            const float2 t12 = bc2(t1), t22 = bc2(t2);
+                            al01[ny] = fma2(t22, e2z01, fma2(t12, ez01, al01[ny]));
+                            al23[ny] = fma2(t22, e2z23, fma2(t12, ez23, al23[ny]));
+                            al4[ny] = fmaf(t2, e2z4, fmaf(t1, ez4, al4[ny]));
                         }
                     }
                     const int nx = cq[0] + nxs;
@@ -510,7 +537,9 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
                         for (int nz = 0; nz < 5; ++nz)
                         {
                             const int sidx = nx * kACSX + (cq[1] + ny) * kACSY + cq[2] + nz;
-                            plane_add(&clo[sidx], &chi[sidx], al[ny][nz], slap);
+                            const float a = nz == 0 ? al01[ny].x : nz == 1 ? al01[ny].y : nz == 2 ? al23[ny].x
+                                          : nz == 3 ? al23[ny].y : al4[ny];
+                            plane_add(&clo[sidx], &chi[sidx], a, slap);
                         }
                 }
             }
@@ -568,6 +597,48 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
     }
 }
 
+// Adjoint of resolve() (the reference's _resolve, anisompm.py:811-825) at
+// input velocity v: vb holds the adjoint of the output on entry and of the
+// input on return.  Sticky: the output is the collider velocity, a constant.
+// Slip: torch's subgradient conventions, clamp passing where its input lies
+// inside the bounds inclusive (vn <= 0 for the inward part, scale >= 0 for
+// the friction factor) and the norm passing nothing at zero.
+__device__ __forceinline__ void resolve_adj(const float v[3], const float vc[3], const float nn[3], bool sticky,
+                                            float fr, float vb[3]) {
+    if (sticky) {
+        vb[0] = vb[1] = vb[2] = 0.0f;
+        return;
+    }
+    const float r[3] = {v[0] - vc[0], v[1] - vc[1], v[2] - vc[2]};
+    const float vn = r[0] * nn[0] + r[1] * nn[1] + r[2] * nn[2];
+    const float inward = vn < 0.0f ? vn : 0.0f;
+    const float t[3] = {r[0] - vn * nn[0], r[1] - vn * nn[1], r[2] - vn * nn[2]};
+    const float keepb = vb[0] * nn[0] + vb[1] * nn[1] + vb[2] * nn[2];
+    float tb[3] = {vb[0], vb[1], vb[2]};
+    float inwardb = -keepb;
+    if (fr > 0.0f) {
+        const float vtm = sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        const float den = vtm + 1e-9f;
+        const float sraw = 1.0f + fr * inward / den;
+        const float sc = sraw < 0.0f ? 0.0f : sraw;
+        const float scb = tb[0] * t[0] + tb[1] * t[1] + tb[2] * t[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) tb[a] *= sc;
+        if (sraw >= 0.0f) {
+            inwardb += scb * fr / den;
+            const float vtmb = -scb * fr * inward / (den * den);
+            if (vtm > 0.0f) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) tb[a] += vtmb * t[a] / vtm;
+            }
+        }
+    }
+    float vnb = keepb - (tb[0] * nn[0] + tb[1] * nn[1] + tb[2] * nn[2]);
+    if (vn <= 0.0f) vnb += inwardb;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vb[a] = tb[a] + vnb * nn[a];
+}
+
 // ---------------------------------------------------------------- k_adj_grid
 // Grid-update adjoint over the recorded active blocks.  Forward (active node,
 // m > 1e-12): v = (mv / m + dt g) * damp; gd = sum wd / sum w when sum w >
@@ -575,6 +646,7 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
 // clears acc.
 __global__ void __launch_bounds__(256) k_adj_grid(const pm_params prm, const int *__restrict__ blocks,
                                                   const TapeHead *head, const float4 *__restrict__ gvel,
+                                                  const float4 *__restrict__ vpre,
                                                   const float *__restrict__ ggd, const float *__restrict__ gsw,
                                                   long long *__restrict__ acc, const AdjCtrl *actl,
                                                   float4 *__restrict__ A, float4 *__restrict__ B,
@@ -583,7 +655,7 @@ __global__ void __launch_bounds__(256) k_adj_grid(const pm_params prm, const int
     const long long nact = min((long long)head->n_active, n_blocks);
     const long long items = nact * 64;
     const int ng = prm.n_grid, nbs = (ng + kBlockEdge - 1) / kBlockEdge;
-    const float dt = (float)prm.dt, damp = (float)prm.grid_damp;
+    const float dt = (float)prm.dt, damp = (float)prm.grid_damp, dx = (float)prm.dx;
     const float dg[3] = {damp * dt * (float)prm.gravity[0], damp * dt * (float)prm.gravity[1],
                          damp * dt * (float)prm.gravity[2]};
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
@@ -600,14 +672,38 @@ __global__ void __launch_bounds__(256) k_adj_grid(const pm_params prm, const int
         an[1] = make_longlong2(0, 0);
         const float4 ab = make_float4(from_fix(a01.x, umom), from_fix(a01.y, umom), from_fix(a23.x, umom),
                                       from_fix(a23.y, ulap));
-        const float4 gv = gvel[node];
+        float4 gv = gvel[node];
         float4 ao = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (gv.w > 1e-12f) {
+            float vb[3] = {ab.x, ab.y, ab.z};
+            if (vpre && prm.n_colliders > 0) {
+                // colliders (anisompm.py:737-746): rerun them from the recorded
+                // pre-collider velocity, keeping each one's input, then walk
+                // them back
+                const float4 vp = vpre[node];
+                const float pos[3] = {(float)ix * dx, (float)iy * dx, (float)iz * dx};
+                float vs[PM_MAX_COLLIDERS][3], nrm[PM_MAX_COLLIDERS][3];
+                unsigned hit = 0u;
+                float v[3] = {vp.x, vp.y, vp.z};
+                for (int c = 0; c < prm.n_colliders; ++c) {
+                    vs[c][0] = v[0]; vs[c][1] = v[1]; vs[c][2] = v[2];
+                    if (collider_hit(prm.colliders[c], head->col_origin[c], pos, nrm[c])) {
+                        hit |= 1u << c;
+                        resolve(v, head->col_vel[c], nrm[c], prm.colliders[c].mode == 1,
+                                (float)prm.colliders[c].friction);
+                    }
+                }
+                for (int c = prm.n_colliders - 1; c >= 0; --c)
+                    if (hit & (1u << c))
+                        resolve_adj(vs[c], head->col_vel[c], nrm[c], prm.colliders[c].mode == 1,
+                                    (float)prm.colliders[c].friction, vb);
+                gv.x = vp.x; gv.y = vp.y; gv.z = vp.z;   // the velocity the mass and momentum made
+            }
             const float im = 1.0f / gv.w;
-            const float u0 = damp * ab.x, u1 = damp * ab.y, u2 = damp * ab.z;
+            const float u0 = damp * vb[0], u1 = damp * vb[1], u2 = damp * vb[2];
             ao.x = u0 * im; ao.y = u1 * im; ao.z = u2 * im;
             // mv / m = v / damp - dt g:  mbar = -damp vbar . (mv/m) / m
-            ao.w = -(ab.x * (gv.x - dg[0]) + ab.y * (gv.y - dg[1]) + ab.z * (gv.z - dg[2])) * im;
+            ao.w = -(vb[0] * (gv.x - dg[0]) + vb[1] * (gv.y - dg[1]) + vb[2] * (gv.z - dg[2])) * im;
         }
         A[node] = ao;
         const float sw = gsw[node], gd = ggd[node];
@@ -625,7 +721,9 @@ __global__ void __launch_bounds__(256) k_adj_grid(const pm_params prm, const int
 // driving geometry (Cauchy stress eigensystem, sigma+, A, M) is not kept: it
 // is needed only where the history drive is active, and is recomputed there.
 struct Cons {
-    float F[9], V[9], S[3], R[9], lamC[3];
+    float F[9], V[9], S[3], Sc[3], R[9], lamC[3];   // F: after the strain limit; S before it, Sc after
+    bool fclamp, iface;
+    float n0[3];   // interface normal (iface)
     float J, Jraw, tdev[9], tv;
     bool dmg;
     float phi, drive, Dh0, Dh1, d0, lap, arg, cc, u, dn, d1, g, vdeg, res, sc, zeta, l0;
@@ -684,11 +782,14 @@ __device__ __forceinline__ void damage_geom(const float R[9], const float V[9], 
 }
 
 
-// Forward constitutive update without f_clamp and interface particles, as
-// the forward kernel computes it, keeping the intermediates.  The polar
+// Forward constitutive update without interface particles, as the forward
+// kernel computes it (the strain limit included), keeping the intermediates.  The polar
 // decomposition (R, V, S) and, on damage steps, phi come from the tape that
 // the recorded forward wrote (pol[k * rs + p]: R 0..8, V 9..17, S 18..20,
 // phi 21), so neither eigensolve is repeated here.
+// EXT: the strain limit and interface particles are compiled in (a kernel
+// without them keeps fewer registers live).
+template <bool EXT>
 __device__ __forceinline__ void cons_forward(const pm_params &prm, const Parts &P, long long p, bool do_damage,
                                              Cons &c, float tau[9], const float *__restrict__ pol, long long rs) {
     const long long ps = P.ps;
@@ -703,7 +804,11 @@ __device__ __forceinline__ void cons_forward(const pm_params &prm, const Parts &
         c.S[i] = pol[(18 + i) * rs + p];
         c.lamC[i] = c.S[i] > sqrtf(1e-12f) ? 1.0f : 0.0f;   // 0 where S = sqrt(max(lamC, 1e-12)) clamped
     }
-    c.Jraw = c.S[0] * c.S[1] * c.S[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) c.Sc[i] = c.S[i];
+    c.fclamp = EXT && prm.use_f_clamp != 0;
+    if (c.fclamp) f_clamp_F(c.F, c.V, c.Sc, (float)prm.f_clamp_lo, (float)prm.f_clamp_hi, c.F);
+    c.Jraw = c.Sc[0] * c.Sc[1] * c.Sc[2];
     c.J = c.Jraw < 1e-6f ? 1e-6f : c.Jraw;
     const float mu = P.mu[p], lam = P.lam[p];
     {
@@ -742,6 +847,114 @@ __device__ __forceinline__ void cons_forward(const pm_params &prm, const Parts &
     c.vdeg = (c.J >= 1.0f) ? c.g : 1.0f;
 #pragma unroll
     for (int k = 0; k < 9; ++k) tau[k] = c.g * c.tdev[k] + ((k % 4 == 0) ? c.vdeg * c.tv : 0.0f);
+    c.iface = EXT && P.interface_mask && P.interface_mask[p];
+    if (c.iface) {
+        c.n0[0] = P.n_interface[p];
+        c.n0[1] = P.n_interface[ps + p];
+        c.n0[2] = P.n_interface[2 * ps + p];
+    }
+}
+
+// Adjoint of the directional (delamination) stress at an interface particle
+// (directional_kirchhoff, anisompm.py:190-227 via 697-703): tau = Q tc Q +
+// gI P tc P + g (P tc Q + Q tc P) with tc = tdev + tv I, P = m m^T, Q = I - P,
+// m = F n0 / (|F n0| + 1e-9) and gI = g where m^T tc m > 0, else 1.  Given
+// taub: the adjoints of g (gb), tdev, tv and the direct part of F (Fb, added).
+__device__ __forceinline__ void dir_adjoint(const Cons &c, const float taub[9], float &gb, float tdevb[9],
+                                            float &tvb, float Fb[9]) {
+    float tc[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) tc[k] = c.tdev[k] + ((k % 4 == 0) ? c.tv : 0.0f);
+    float u[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) u[i] = c.F[3 * i] * c.n0[0] + c.F[3 * i + 1] * c.n0[1] + c.F[3 * i + 2] * c.n0[2];
+    const float un = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const float mn = un + 1e-9f;
+    const float m[3] = {u[0] / mn, u[1] / mn, u[2] / mn};
+    float Pm[9], Qm[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            Pm[3 * i + j] = m[i] * m[j];
+            Qm[3 * i + j] = ((i == j) ? 1.0f : 0.0f) - Pm[3 * i + j];
+        }
+    float snn = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) snn += m[i] * tc[3 * i + j] * m[j];
+    const bool tens = snn > 0.0f;
+    const float gI = tens ? c.g : 1.0f;
+    // pieces of the forward, for the adjoint of g
+    float T1[9], perp[9], shs[9], X[9];
+    mm3(Pm, tc, T1);                        // P tc
+    mm3(T1, Pm, perp);                      // P tc P
+    mm3(T1, Qm, shs);                       // P tc Q
+    mm3(Qm, tc, T1);                        // Q tc
+    mm3(T1, Pm, X);                         // Q tc P
+    gb = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gb += taub[k] * (shs[k] + X[k] + (tens ? perp[k] : 0.0f));
+    // tcb = Q taub Q + gI P taub P + g (P taub Q + Q taub P)
+    float PT[9], QT[9], A1[9], A2[9], A3[9], A4[9];
+    mm3(Pm, taub, PT);
+    mm3(Qm, taub, QT);
+    mm3(QT, Qm, A1);
+    mm3(PT, Pm, A2);
+    mm3(PT, Qm, A3);
+    mm3(QT, Pm, A4);
+    float trc = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const float tcb = A1[k] + gI * A2[k] + c.g * (A3[k] + A4[k]);
+        tdevb[k] = tcb;
+        if (k % 4 == 0) trc += tcb;
+    }
+    tvb = trc;
+    // Pbar, Qbar from the four products (P, Q symmetric; Xbar of each piece:
+    // par taub, perp gI taub, both shears g taub)
+    float Pb[9], Qb[9];
+    {
+        float tcP[9], tcQ[9], tcT[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) tcT[3 * i + j] = tc[3 * j + i];
+        mm3(tcT, Pm, tcP);                  // tc^T P
+        mm3(tcT, Qm, tcQ);                  // tc^T Q
+        float PtcT[9], QtcT[9];
+        mm3(Pm, tcT, PtcT);                 // P tc^T
+        mm3(Qm, tcT, QtcT);                 // Q tc^T
+        float B1[9], B2[9], B3[9], B4[9], B5[9], B6[9], B7[9], B8[9];
+        mm3(taub, PtcT, B1);                // perp: Xb P tc^T
+        mm3(tcP, taub, B2);                 //       tc^T P Xb
+        mm3(taub, QtcT, B3);                // sh1 = P tc Q: Pb += Xb Q tc^T
+        mm3(tcP, taub, B4);                 //               Qb += tc^T P Xb
+        mm3(taub, PtcT, B5);                // sh2 = Q tc P: Qb += Xb P tc^T
+        mm3(tcQ, taub, B6);                 //               Pb += tc^T Q Xb
+        mm3(taub, QtcT, B7);                // par = Q tc Q: Qb += Xb Q tc^T
+        mm3(tcQ, taub, B8);                 //               Qb += tc^T Q Xb
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            Pb[k] = gI * (B1[k] + B2[k]) + c.g * (B3[k] + B6[k]);
+            Qb[k] = c.g * (B4[k] + B5[k]) + B7[k] + B8[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Pb[k] -= Qb[k];   // Q = I - P
+    float mb[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        mb[i] = (Pb[3 * i] + Pb[i]) * m[0] + (Pb[3 * i + 1] + Pb[3 + i]) * m[1] + (Pb[3 * i + 2] + Pb[6 + i]) * m[2];
+    const float mbu = mb[0] * u[0] + mb[1] * u[1] + mb[2] * u[2];
+    const float cu = un > 0.0f ? mbu / (un * mn * mn) : 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float ub = mb[i] / mn - cu * u[i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Fb[3 * i + j] += ub * c.n0[j];
+    }
 }
 
 // Adjoint of the eigen split sp = Q diag(relu(e)) Q^T of the symmetric sig:
@@ -787,23 +1000,32 @@ __device__ __forceinline__ void eigsplit_adj(const float ev[3], const float Q[9]
     mmt3(T, Q, sgb);
 }
 
+// Fb: the adjoint of the pre-substep F; with the strain limit, the adjoint
+// of the limited F (direct terms only) and, apart, the polar rotation's
+// contribution to the pre-substep F (Fp) and the adjoint of the limited
+// singular values (Scb), which f_clamp_adj combines.
 struct ConsAdj {
-    float Fb[9], mub, lamb, scb, A0b[9], d0b, lapb, Dh0b;
+    float Fb[9], Fp[9], Scb[3], mub, lamb, scb, A0b[9], d0b, lapb, Dh0b;
 };
 
 // Reverse of cons_forward given taubar, the adjoint of the updated damage d1
 // and of the updated history D_hist1.
 __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, const float lam, const float taub[9],
                                              float d1b, float Dh1b, const Parts &P, long long p, ConsAdj &o) {
-    const float trt = taub[0] + taub[4] + taub[8];
-    float gb = 0.0f;
+    float gb = 0.0f, tdevb[9], tvb, Fbd[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) gb += taub[k] * c.tdev[k];
-    if (c.J >= 1.0f) gb += c.tv * trt;
-    float tdevb[9];
+    for (int k = 0; k < 9; ++k) Fbd[k] = 0.0f;
+    if (c.iface) {
+        dir_adjoint(c, taub, gb, tdevb, tvb, Fbd);
+    } else {   // tau = g tdev + vdeg tv I
+        const float trt = taub[0] + taub[4] + taub[8];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) tdevb[k] = c.g * taub[k];
-    float tvb = c.vdeg * trt;
+        for (int k = 0; k < 9; ++k) gb += taub[k] * c.tdev[k];
+        if (c.J >= 1.0f) gb += c.tv * trt;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) tdevb[k] = c.g * taub[k];
+        tvb = c.vdeg * trt;
+    }
     d1b += gb * (-2.0f * (1.0f - c.d1) * (1.0f - c.res));
     float Jb = 0.0f, Rb[9];
 #pragma unroll
@@ -925,19 +1147,22 @@ __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, cons
             TtFmR[3 * i + j] = tdevb[i] * FmR[j] + tdevb[3 + i] * FmR[3 + j] + tdevb[6 + i] * FmR[6 + j];
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        o.Fb[k] = (2.0f * mu) * (TF[k] + TtFmR[k]);
+        o.Fb[k] = (2.0f * mu) * (TF[k] + TtFmR[k]) + Fbd[k];
         Rb[k] += -(2.0f * mu) * TF[k];
     }
     // J = max(S0 S1 S2, 1e-6); S = sqrt(max(lamC, 1e-12))
     float Sb[3] = {0.0f, 0.0f, 0.0f};
     if (c.Jraw > 1e-6f) {
-        Sb[0] = Jb * c.S[1] * c.S[2];
-        Sb[1] = Jb * c.S[0] * c.S[2];
-        Sb[2] = Jb * c.S[0] * c.S[1];
+        Sb[0] = Jb * c.Sc[1] * c.Sc[2];
+        Sb[1] = Jb * c.Sc[0] * c.Sc[2];
+        Sb[2] = Jb * c.Sc[0] * c.Sc[1];
     }
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 3; ++i) {
         if (c.lamC[i] == 0.0f) Sb[i] = 0.0f;
+        o.Scb[i] = Sb[i];
+        if (c.fclamp) Sb[i] = 0.0f;   // through the limited values: f_clamp_adj
+    }
     // polar F = R U: Fbar += R V (G + diag(Sbar)) V^T with
     // G_ij = (B_ij - B_ji) / (S_i + S_j), B = V^T R^T Rbar V
     float RtRb[9], T[9], Bm[9];
@@ -969,7 +1194,52 @@ __device__ __forceinline__ void cons_adjoint(const Cons &c, const float mu, cons
     mm3(RV, G, RVG);
     mmt3(RVG, c.V, Fp);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) o.Fb[k] += Fp[k];
+    for (int k = 0; k < 9; ++k) {
+        o.Fp[k] = Fp[k];
+        if (!c.fclamp) o.Fb[k] += Fp[k];
+    }
+}
+
+// Adjoint of the strain limit F -> Fc = U g(S) V^T (anisompm.py:622-636 with
+// U = R V, S the singular values before the limit, g = clamp(., lo, hi)),
+// given Fcb (the adjoint of Fc) and Scb (of g(S)): returns U G V^T with
+// X = U^T Fcb V, G_ii = g'(S_i) (X_ii + Scb_i) and, off the diagonal, the
+// divided differences of a singular-value function:
+// G_ij = a (X_ij + X_ji)/2 + b (X_ij - X_ji)/2, a = (g_i - g_j)/(S_i - S_j)
+// (the mean of g' at equal values), b = (g_i + g_j)/(S_i + S_j).  g' passes
+// on [lo, hi] inclusive, as torch's clamp does.
+__device__ __forceinline__ void f_clamp_adj(const Cons &c, float lo, float hi, const float Fcb[9],
+                                            const float Scb[3], float out[9]) {
+    float U[9], T[9], X[9], G[9], g[3], gp[3];
+    mm3(c.R, c.V, U);
+    mm3(Fcb, c.V, T);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) X[3 * i + j] = U[i] * T[j] + U[3 + i] * T[3 + j] + U[6 + i] * T[6 + j];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        g[i] = c.Sc[i];
+        gp[i] = (c.S[i] >= lo && c.S[i] <= hi) ? 1.0f : 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            if (i == j) {
+                G[3 * i + i] = c.lamC[i] != 0.0f ? gp[i] * (X[3 * i + i] + Scb[i]) : 0.0f;
+            } else {
+                const float ds = c.S[i] - c.S[j];
+                const float a = fabsf(ds) > 1e-6f * fmaxf(c.S[i], c.S[j]) ? (g[i] - g[j]) / ds : 0.5f * (gp[i] + gp[j]);
+                const float den = fmaxf(c.S[i] + c.S[j], 1e-6f);
+                const float b = (g[i] + g[j]) / den;
+                const float xs = 0.5f * (X[3 * i + j] + X[3 * j + i]), xa = 0.5f * (X[3 * i + j] - X[3 * j + i]);
+                G[3 * i + j] = a * xs + b * xa;
+            }
+        }
+    float UG[9];
+    mm3(U, G, UG);
+    mmt3(UG, c.V, out);
 }
 
 constexpr int kAQ = 512;    // staged quadratic nodes per CTA ({v, m} and {mvbar, mbar}: 32 B each)
@@ -1103,6 +1373,7 @@ __device__ __forceinline__ void adj_gather(const float xp[3], float inv_dx, floa
 // the gather state live.  The output adjoint of F is written in two parts:
 // (I + dt C')^T Fbar' before the gathers, the constitutive part added at the
 // end (same thread, same address).
+template <bool EXT>
 __global__ void __launch_bounds__(128, 4) k_adj_particle(const pm_params prm, const Parts pre, const Parts post,
                                                          const pm_state_adj ain, const pm_state_adj aout,
                                                          const pm_param_adj grads, const TapeHead *head,
@@ -1180,6 +1451,7 @@ __global__ void __launch_bounds__(128, 4) k_adj_particle(const pm_params prm, co
         for (int k = 0; k < 3; ++k) vpost[k] = post.v[k * ps + p];
 #pragma unroll
         for (int k = 0; k < 9; ++k) F[k] = pre.F[k * ps + p];
+        if (EXT) g2p_input_F(prm, tpol, taff_stride, p, F);
         AdjIn a;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -1260,11 +1532,23 @@ __global__ void __launch_bounds__(128, 4) k_adj_particle(const pm_params prm, co
     for (int k = 0; k < 9; ++k) taub[k] = coeff * affb[k];
     Cons c;
     float tau[9];
-    cons_forward(prm, pre, p, do_damage, c, tau, tpol, taff_stride);
+    cons_forward<EXT>(prm, pre, p, do_damage, c, tau, tpol, taff_stride);
     ConsAdj o;
     cons_adjoint(c, pre.mu[p], pre.lam[p], taub, d1b, ain.D_hist[p], pre, p, o);
+    if (c.fclamp) {
+        // the G2P part above and the stress's direct part are adjoints of the
+        // limited F: through the limit to the pre-substep F, plus the polar
+        // rotation's part
+        float Fcb[9], F0b[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) aout.F[k * os + p] += o.Fb[k];
+        for (int k = 0; k < 9; ++k) Fcb[k] = aout.F[k * os + p] + o.Fb[k];
+        f_clamp_adj(c, (float)prm.f_clamp_lo, (float)prm.f_clamp_hi, Fcb, o.Scb, F0b);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) aout.F[k * os + p] = F0b[k] + o.Fp[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) aout.F[k * os + p] += o.Fb[k];
+    }
     aout.d[p] = o.d0b;
     aout.lap[p] = o.lapb;
     aout.D_hist[p] = o.Dh0b;
@@ -1293,6 +1577,13 @@ __global__ void k_tape_head(const Ctrl *ctrl, TapeHead *head, long long n) {
         head->time = ctrl->time;
         head->n_work = (unsigned)min((long long)ctrl->n_work, n);
     }
+    if (threadIdx.x < PM_MAX_COLLIDERS) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            head->col_origin[threadIdx.x][a] = ctrl->col_origin[threadIdx.x][a];
+            head->col_vel[threadIdx.x][a] = ctrl->col_vel[threadIdx.x][a];
+        }
+    }
 }
 
 }  // namespace
@@ -1310,7 +1601,7 @@ void prepare_adjoint() {
 }
 
 // ------------------------------------------------------------------ tape layout
-TapeLayout make_tape_layout(long long n, int ng, int slots) {
+TapeLayout make_tape_layout(long long n, int ng, int slots, int flags) {
     TapeLayout T;
     const size_t A = 256;
     const long long G = (long long)ng * ng * ng;
@@ -1329,6 +1620,7 @@ TapeLayout make_tape_layout(long long n, int ng, int slots) {
     T.vel = s;     s = align_up(s + 16 * (size_t)G, A);
     T.gd = s;      s = align_up(s + 4 * (size_t)G, A);
     T.sw = s;      s = align_up(s + 4 * (size_t)G, A);
+    T.vpre = s;    s = align_up(s + ((flags & PM_TAPE_COLLIDERS) ? 16 * (size_t)G : 0), A);   // pre-collider v
     T.blocks = s;  s = align_up(s + 4 * (size_t)nb, A);
     T.keys = s;    s = align_up(s + 4 * (size_t)np, A);
     T.iperm = s;   s = align_up(s + 4 * (size_t)np, A);
@@ -1340,6 +1632,7 @@ TapeLayout make_tape_layout(long long n, int ng, int slots) {
     T.total = o + s * (size_t)(slots > 0 ? slots : 1);
     T.n_blocks = nb;
     T.slots = slots;
+    T.flags = flags;
     return T;
 }
 
@@ -1348,6 +1641,7 @@ void record_redirect(const TapeLayout &T, void *tape, int slot, WS &w) {
     w.g_vel = (float4 *)(b + T.vel);
     w.g_gd = (float *)(b + T.gd);
     w.g_sw = (float *)(b + T.sw);
+    w.g_vpre = (T.flags & PM_TAPE_COLLIDERS) ? (float4 *)(b + T.vpre) : nullptr;
     w.block_list = (int *)(b + T.blocks);
     w.inv_perm = (int *)(b + T.iperm);   // the substep's sort stays on the tape for the adjoint
     w.work = (int *)(b + T.work);
@@ -1384,7 +1678,8 @@ void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, c
     if (n <= 0) return;
     prepare_adjoint();
     cudaMemsetAsync(actl, 0, sizeof(AdjCtrl), s);
-    k_adj_pre<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prm, pre, post, ain, (const int *)(b + T.iperm), apay, actl);
+    k_adj_pre<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(prm, pre, post, ain, (const int *)(b + T.iperm), apay, actl,
+                                                          (const float *)(b + T.pol), T.aff_stride);
     k_adj_bounds<<<1, kBoundSlots, 0, s>>>(actl);
     {
         static int slots_dev[64] = {0};
@@ -1401,11 +1696,17 @@ void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, c
     }
     const long long max_items = T.n_blocks * 64;
     const int gb = (int)std::max<long long>(1, std::min<long long>((max_items + 255) / 256, 148LL * 8));
-    k_adj_grid<<<gb, 256, 0, s>>>(prm, blocks, h, gvel, ggd, gsw, acc, actl, Aq, Bc, T.n_blocks);
+    const float4 *vpre = (T.flags & PM_TAPE_COLLIDERS) ? (const float4 *)(b + T.vpre) : nullptr;
+    k_adj_grid<<<gb, 256, 0, s>>>(prm, blocks, h, gvel, vpre, ggd, gsw, acc, actl, Aq, Bc, T.n_blocks);
     const float *taff = (const float *)(b + T.aff);
     const float *tpol = (const float *)(b + T.pol);
-    k_adj_particle<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(prm, pre, post, ain, aout, grads, h, gvel, Aq, Bc,
-                                                               taff, tpol, T.aff_stride);
+    const unsigned pb = (unsigned)((n + 127) / 128);
+    if (prm.use_f_clamp || pre.interface_mask)
+        k_adj_particle<true><<<pb, 128, 0, s>>>(prm, pre, post, ain, aout, grads, h, gvel, Aq, Bc, taff, tpol,
+                                                T.aff_stride);
+    else
+        k_adj_particle<false><<<pb, 128, 0, s>>>(prm, pre, post, ain, aout, grads, h, gvel, Aq, Bc, taff, tpol,
+                                                 T.aff_stride);
 }
 
 }  // namespace pm

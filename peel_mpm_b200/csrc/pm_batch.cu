@@ -111,7 +111,7 @@ pm::BatchScenes scenes_of(void *ws, const BatchPlan &bp) {
 std::mutex g_mu;
 struct WsRecord {
     uint64_t sig;
-    int p2g_ctas, grid_ctas;   // launch knobs, from the stored parameters of scene 0
+    int p2g_ctas, grid_ctas, stress_ctas, g2p_ctas;   // launch knobs, from the stored parameters of scene 0
 };
 std::unordered_map<uintptr_t, WsRecord> g_sig;
 
@@ -119,7 +119,7 @@ std::unordered_map<uintptr_t, WsRecord> g_sig;
 WsRecord recorded_knobs(const void *ws) {
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_sig.find((uintptr_t)ws);
-    return it == g_sig.end() ? WsRecord{0, 0, 0} : it->second;
+    return it == g_sig.end() ? WsRecord{0, 0, 0, 0, 0} : it->second;
 }
 
 
@@ -213,7 +213,8 @@ int pm_batch_workspace_init(void *ws, size_t ws_bytes, int32_t n_scenes, const i
     if ((rc = upload_tables(ws, bp, prms, s))) return rc;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        g_sig[(uintptr_t)ws] = WsRecord{bp.sig, prms[0].p2g_ctas_per_sm, prms[0].grid_ctas_per_sm};
+        g_sig[(uintptr_t)ws] = WsRecord{bp.sig, prms[0].p2g_ctas_per_sm, prms[0].grid_ctas_per_sm,
+                                        prms[0].stress_ctas_per_sm, prms[0].g2p_ctas_per_sm};
     }
     return pm::api_cuda_check("pm_batch_workspace_init");
 }
@@ -235,6 +236,8 @@ int pm_batch_set_params(void *ws, size_t ws_bytes, int32_t n_scenes, const int64
         std::lock_guard<std::mutex> lk(g_mu);
         g_sig[(uintptr_t)ws].p2g_ctas = prms[0].p2g_ctas_per_sm;
         g_sig[(uintptr_t)ws].grid_ctas = prms[0].grid_ctas_per_sm;
+        g_sig[(uintptr_t)ws].stress_ctas = prms[0].stress_ctas_per_sm;
+        g_sig[(uintptr_t)ws].g2p_ctas = prms[0].g2p_ctas_per_sm;
     }
     return PM_OK;
 }
@@ -257,10 +260,10 @@ int pm_batch_substep(int32_t n_scenes, const int64_t *n, const int32_t *n_grid, 
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, bp.n_total, s, w.inv_perm, true);
         const WsRecord knobs = recorded_knobs(ws);
-        pm::launch_p2g(sc, parts, w, s, knobs.p2g_ctas);
+        pm::launch_p2g(sc, parts, w, s, knobs.p2g_ctas, knobs.stress_ctas);
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s, knobs.grid_ctas);
-        pm::launch_g2p(sc, parts, w, s, bp.n_ctas);
+        pm::launch_g2p(sc, parts, w, s, bp.n_ctas, knobs.g2p_ctas);
     }
     return pm::api_cuda_check("pm_batch_substep");
 }

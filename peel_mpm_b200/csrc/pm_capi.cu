@@ -47,6 +47,10 @@ int check_params(const pm_params *prm) {
     if (prm->p2g_ctas_per_sm < 0 || prm->p2g_ctas_per_sm > 8) return fail(PM_ERR_ARG, "p2g_ctas_per_sm must be in [0, 8]");
     if (prm->grid_ctas_per_sm < 0 || prm->grid_ctas_per_sm > 64)
         return fail(PM_ERR_ARG, "grid_ctas_per_sm must be in [0, 64]");
+    if (prm->stress_ctas_per_sm != 0 && prm->stress_ctas_per_sm != 3 && prm->stress_ctas_per_sm != 4)
+        return fail(PM_ERR_ARG, "stress_ctas_per_sm must be 0, 3 or 4");
+    if (prm->g2p_ctas_per_sm != 0 && prm->g2p_ctas_per_sm != 3 && prm->g2p_ctas_per_sm != 4)
+        return fail(PM_ERR_ARG, "g2p_ctas_per_sm must be 0, 3 or 4");
     if (!(prm->dx > 0.0) || !(prm->inv_dx > 0.0)) return fail(PM_ERR_ARG, "dx must be positive");
     return PM_OK;
 }
@@ -185,7 +189,7 @@ int pm_p2g(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
-    pm::launch_p2g(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream, prm->p2g_ctas_per_sm);
+    pm::launch_p2g(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream, prm->p2g_ctas_per_sm, prm->stress_ctas_per_sm);
     pm::launch_compact(w, (cudaStream_t)stream);
     return cuda_check("pm_p2g");
 }
@@ -204,7 +208,7 @@ int pm_g2p(const pm_params *prm, const pm_particles *P, void *ws, size_t ws_byte
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
-    pm::launch_g2p(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream);
+    pm::launch_g2p(pm::PlainScenes{*prm}, pm::make_parts(P), w, (cudaStream_t)stream, -1, prm->g2p_ctas_per_sm);
     return cuda_check("pm_g2p");
 }
 
@@ -224,10 +228,10 @@ static int substep_common(const pm_params *prm, const pm_particles *P, void *ws,
         const pm::PlainScenes sc{*prm};
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, P->n, s, w.inv_perm, true);
-        pm::launch_p2g(sc, parts, w, s, prm->p2g_ctas_per_sm);
+        pm::launch_p2g(sc, parts, w, s, prm->p2g_ctas_per_sm, prm->stress_ctas_per_sm);
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s, prm->grid_ctas_per_sm);
-        pm::launch_g2p(sc, parts, w, s);
+        pm::launch_g2p(sc, parts, w, s, -1, prm->g2p_ctas_per_sm);
     }
     return cuda_check("pm_substep");
 }
@@ -245,35 +249,34 @@ int pm_substep_dev_clock(const pm_params *prm, const pm_particles *P, void *ws, 
 }
 
 // ------------------------------------------------------------------ adjoint
-static int check_adjoint_params(const pm_params *prm, const pm_particles *P) {
-    if (prm->use_f_clamp) return fail(PM_ERR_ARG, "the adjoint does not support f_clamp");
-    if (prm->n_colliders > 0) return fail(PM_ERR_ARG, "the adjoint does not support colliders");
-    if (P && P->interface_mask) return fail(PM_ERR_ARG, "the adjoint does not support interface particles");
-    return PM_OK;
-}
-
-static int get_tape(void *tape, size_t bytes, long long n, int ng, int slots, int slot, pm::TapeLayout *T) {
+static int get_tape(void *tape, size_t bytes, long long n, int ng, int slots, int flags, int slot,
+                    pm::TapeLayout *T) {
     if (!tape) return fail(PM_ERR_WORKSPACE, "tape is NULL");
     if (((uintptr_t)tape & 255) != 0) return fail(PM_ERR_WORKSPACE, "tape must be 256-byte aligned");
     if (slots < 1 || slot < 0 || slot >= slots) return fail(PM_ERR_ARG, "bad tape slot");
-    *T = pm::make_tape_layout(n, ng, slots);
-    if (bytes < T->total) return fail(PM_ERR_WORKSPACE, "tape too small for (n, n_grid, slots)");
+    *T = pm::make_tape_layout(n, ng, slots, flags);
+    if (bytes < T->total) return fail(PM_ERR_WORKSPACE, "tape too small for (n, n_grid, slots, flags)");
     return PM_OK;
 }
 
-int pm_tape_size(int64_t n, int32_t n_grid, int32_t slots, size_t *bytes) {
+static int tape_flags(const pm_params *prm) { return prm->n_colliders > 0 ? PM_TAPE_COLLIDERS : 0; }
+
+int pm_tape_size(int64_t n, int32_t n_grid, int32_t slots, int32_t flags, size_t *bytes) {
     if (!bytes) return fail(PM_ERR_ARG, "bytes is NULL");
     if (n < 0 || n_grid < 4 || n_grid > 1024 || slots < 1) return fail(PM_ERR_ARG, "bad n, n_grid or slots");
-    *bytes = pm::make_tape_layout(n, n_grid, slots).total;
+    if (flags & ~PM_TAPE_COLLIDERS) return fail(PM_ERR_ARG, "unknown tape flags");
+    *bytes = pm::make_tape_layout(n, n_grid, slots, flags).total;
     return PM_OK;
 }
 
-int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32_t slots, void *stream) {
+int pm_tape_init(void *tape, size_t tape_bytes, int64_t n, int32_t n_grid, int32_t slots, int32_t flags,
+                 void *stream) {
     int rc;
     if ((rc = check_device())) return rc;
     if (n < 0 || n_grid < 4 || n_grid > 1024) return fail(PM_ERR_ARG, "bad n or n_grid");
+    if (flags & ~PM_TAPE_COLLIDERS) return fail(PM_ERR_ARG, "unknown tape flags");
     pm::TapeLayout T;
-    if ((rc = get_tape(tape, tape_bytes, n, n_grid, slots, 0, &T))) return rc;
+    if ((rc = get_tape(tape, tape_bytes, n, n_grid, slots, flags, 0, &T))) return rc;
     if (cudaMemsetAsync(tape, 0, T.total, (cudaStream_t)stream) != cudaSuccess) return cuda_check("pm_tape_init");
     return cuda_check("pm_tape_init");
 }
@@ -282,7 +285,6 @@ int pm_substep_record(const pm_params *prm, const pm_particles *P, const pm_part
                       const pm_clock *clk, void *tape, size_t tape_bytes, int32_t slots, int32_t slot, void *stream) {
     int rc;
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(P, true))) return rc;
-    if ((rc = check_adjoint_params(prm, P))) return rc;
     if (!clk) return fail(PM_ERR_ARG, "clock is NULL");
     if (out) {
         if (out->n != P->n || out->plane_stride != P->plane_stride)
@@ -295,7 +297,7 @@ int pm_substep_record(const pm_params *prm, const pm_particles *P, const pm_part
     pm::WS w;
     if ((rc = get_ws(ws, ws_bytes, P->n, prm->n_grid, &w))) return rc;
     pm::TapeLayout T;
-    if ((rc = get_tape(tape, tape_bytes, P->n, prm->n_grid, slots, slot, &T))) return rc;
+    if ((rc = get_tape(tape, tape_bytes, P->n, prm->n_grid, slots, tape_flags(prm), slot, &T))) return rc;
     pm::record_redirect(T, tape, slot, w);
     const pm::Parts parts = out ? pm::make_parts_out(P, out) : pm::make_parts(P);
     cudaStream_t s = (cudaStream_t)stream;
@@ -304,10 +306,10 @@ int pm_substep_record(const pm_params *prm, const pm_particles *P, const pm_part
         const pm::PlainScenes sc{*prm};
         pm::launch_keys(sc, w, parts, s);
         pm::launch_sort(w, P->n, s, w.inv_perm, true);
-        pm::launch_p2g(sc, parts, w, s, prm->p2g_ctas_per_sm);
+        pm::launch_p2g(sc, parts, w, s, prm->p2g_ctas_per_sm, prm->stress_ctas_per_sm);
         pm::launch_compact(w, s);
         pm::launch_grid(sc, w, s, prm->grid_ctas_per_sm);
-        pm::launch_g2p(sc, parts, w, s);
+        pm::launch_g2p(sc, parts, w, s, -1, prm->g2p_ctas_per_sm);
     }
     pm::launch_tape_head(T, tape, slot, w, P->n, s);
     return cuda_check("pm_substep_record");
@@ -328,13 +330,12 @@ int pm_substep_adjoint(const pm_params *prm, const pm_particles *pre, const pm_p
     if ((rc = check_device()) || (rc = check_params(prm)) || (rc = check_particles(pre, true)) ||
         (rc = check_particles(post, true)))
         return rc;
-    if ((rc = check_adjoint_params(prm, pre))) return rc;
     if (pre->n != post->n) return fail(PM_ERR_ARG, "pre and post differ in n");
     if ((rc = check_adj(adj_in, pre->n)) || (rc = check_adj(adj_out, pre->n))) return rc;
     if (adj_in->x == adj_out->x) return fail(PM_ERR_ARG, "adj_in and adj_out must be distinct");
     if (!grads || (grads->A0 && grads->plane_stride < pre->n)) return fail(PM_ERR_ARG, "bad parameter gradients");
     pm::TapeLayout T;
-    if ((rc = get_tape(tape, tape_bytes, pre->n, prm->n_grid, slots, slot, &T))) return rc;
+    if ((rc = get_tape(tape, tape_bytes, pre->n, prm->n_grid, slots, tape_flags(prm), slot, &T))) return rc;
     pm::launch_adjoint(*prm, pm::make_parts(pre), pm::make_parts(post), *adj_in, *adj_out, *grads, T, tape, slot,
                        (cudaStream_t)stream);
     return cuda_check("pm_substep_adjoint");

@@ -142,6 +142,7 @@ struct WS {
     float4 *g_vel;      // {v.x, v.y, v.z, unused}
     float *g_gd;        // normalised damage field
     float *g_sw;        // cubic weight sums (recorded for the adjoint; NULL otherwise)
+    float4 *g_vpre;     // grid velocity before the colliders (recorded for the adjoint; NULL otherwise)
     float *tape_aff;    // APIC affine term, 9 planes (recorded for the adjoint; NULL otherwise)
     float *tape_pol;    // polar R, V, S and phi, 22 planes (recorded for the adjoint; NULL otherwise)
     long long tape_aff_stride;
@@ -171,6 +172,7 @@ inline WS make_ws(void *base, const Layout &L) {
     w.g_vel = (float4 *)(b + L.g_vel);
     w.g_gd = (float *)(b + L.g_gd);
     w.g_sw = nullptr;
+    w.g_vpre = nullptr;
     w.tape_aff = nullptr;
     w.tape_pol = nullptr;
     w.tape_aff_stride = 0;
@@ -606,6 +608,71 @@ __device__ __forceinline__ void stress_eig_polar(const float Ucols[9], const flo
         const float s2 = sig[6] * q0 + sig[7] * q1 + sig[8] * q2;
         ev[j] = q0 * s0 + q1 * s1 + q2 * s2;
     }
+}
+
+// The strain limit f_clamp (anisompm.py:622-636): Sc = clamp(S, lo, hi) and
+// F <- F V diag(Sc / max(S, 1e-12)) V^T, every product rounded as the
+// reference's matmuls round it.  S is replaced by Sc.
+__device__ __forceinline__ void f_clamp_F(const float F0[9], const float V[9], float S[3], float lo, float hi,
+                                          float Fc[9]) {
+    float D[9], corr[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float sc = S[i] < lo ? lo : S[i];
+        sc = sc > hi ? hi : sc;
+        const float ratio = sc / (S[i] < 1e-12f ? 1e-12f : S[i]);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) D[3 * r + i] = V[3 * r + i] * ratio;
+        S[i] = sc;
+    }
+    mmt3_rn(D, V, corr);   // V diag(Sc/S) V^T
+    mm3_rn(F0, corr, Fc);
+}
+
+// _resolve (anisompm.py:811-825) for one node
+__device__ __forceinline__ void resolve(float v[3], const float vc[3], const float nn[3], bool sticky, float fr) {
+    if (sticky) {
+        v[0] = vc[0]; v[1] = vc[1]; v[2] = vc[2];
+        return;
+    }
+    // every op rounded separately, as the reference's tensor ops round them
+    const float r0 = __fsub_rn(v[0], vc[0]), r1 = __fsub_rn(v[1], vc[1]), r2 = __fsub_rn(v[2], vc[2]);
+    const float vn = dot3_rn(r0, nn[0], r1, nn[1], r2, nn[2]);
+    const float inward = vn < 0.0f ? vn : 0.0f;
+    float t0 = __fsub_rn(r0, __fmul_rn(vn, nn[0])), t1 = __fsub_rn(r1, __fmul_rn(vn, nn[1])),
+          t2 = __fsub_rn(r2, __fmul_rn(vn, nn[2]));
+    if (fr > 0.0f) {
+        const float vtm = sqrtf(dot3_rn(t0, t0, t1, t1, t2, t2));
+        float sc = __fadd_rn(1.0f, __fdiv_rn(__fmul_rn(fr, inward), __fadd_rn(vtm, 1e-9f)));
+        sc = sc < 0.0f ? 0.0f : sc;
+        t0 = __fmul_rn(t0, sc); t1 = __fmul_rn(t1, sc); t2 = __fmul_rn(t2, sc);
+    }
+    const float keep = __fsub_rn(vn, inward);
+    v[0] = __fadd_rn(__fadd_rn(vc[0], t0), __fmul_rn(keep, nn[0]));
+    v[1] = __fadd_rn(__fadd_rn(vc[1], t1), __fmul_rn(keep, nn[1]));
+    v[2] = __fadd_rn(__fadd_rn(vc[2], t2), __fmul_rn(keep, nn[2]));
+}
+
+// Whether grid node position `pos` lies inside collider `col` (origin o at
+// this substep), and its outward normal there: halfspace_collider
+// (anisompm.py:847-867) tests (pos - o) . n < 0 with the normalised normal;
+// sphere_collider (828-844) tests |pos - o| < radius, normal (pos - o) /
+// (|pos - o| + 1e-9).  Each op rounded separately as the reference's tensor
+// ops round them.
+__device__ __forceinline__ bool collider_hit(const pm_collider &col, const float o[3], const float pos[3],
+                                             float nn[3]) {
+    if (col.kind == 0) {
+        nn[0] = (float)col.normal[0]; nn[1] = (float)col.normal[1]; nn[2] = (float)col.normal[2];
+        const float sd = dot3_rn(__fsub_rn(pos[0], o[0]), nn[0], __fsub_rn(pos[1], o[1]), nn[1],
+                                 __fsub_rn(pos[2], o[2]), nn[2]);
+        return sd < 0.0f;
+    }
+    const float r0 = pos[0] - o[0], r1 = pos[1] - o[1], r2 = pos[2] - o[2];
+    const float dist = sqrtf(dot3_rn(r0, r0, r1, r1, r2, r2));
+    if (!(dist < (float)col.radius)) return false;
+    const float den = dist + 1e-9f;
+    nn[0] = r0 / den; nn[1] = r1 / den; nn[2] = r2 / den;
+    return true;
 }
 
 // ------------------------------------------------------- cell-aggregated scatter

@@ -86,30 +86,6 @@ void launch_set_clock_dev(const pm_params &prm, const WS &w, const pm_clock *dev
 }
 
 // ------------------------------------------------------------ grid update
-// _resolve (anisompm.py:811-825) for one node
-__device__ __forceinline__ void resolve(float v[3], const float vc[3], const float nn[3], bool sticky, float fr) {
-    if (sticky) {
-        v[0] = vc[0]; v[1] = vc[1]; v[2] = vc[2];
-        return;
-    }
-    // every op rounded separately, as the reference's tensor ops round them
-    const float r0 = __fsub_rn(v[0], vc[0]), r1 = __fsub_rn(v[1], vc[1]), r2 = __fsub_rn(v[2], vc[2]);
-    const float vn = dot3_rn(r0, nn[0], r1, nn[1], r2, nn[2]);
-    const float inward = vn < 0.0f ? vn : 0.0f;
-    float t0 = __fsub_rn(r0, __fmul_rn(vn, nn[0])), t1 = __fsub_rn(r1, __fmul_rn(vn, nn[1])),
-          t2 = __fsub_rn(r2, __fmul_rn(vn, nn[2]));
-    if (fr > 0.0f) {
-        const float vtm = sqrtf(dot3_rn(t0, t0, t1, t1, t2, t2));
-        float sc = __fadd_rn(1.0f, __fdiv_rn(__fmul_rn(fr, inward), __fadd_rn(vtm, 1e-9f)));
-        sc = sc < 0.0f ? 0.0f : sc;
-        t0 = __fmul_rn(t0, sc); t1 = __fmul_rn(t1, sc); t2 = __fmul_rn(t2, sc);
-    }
-    const float keep = __fsub_rn(vn, inward);
-    v[0] = __fadd_rn(__fadd_rn(vc[0], t0), __fmul_rn(keep, nn[0]));
-    v[1] = __fadd_rn(__fadd_rn(vc[1], t1), __fmul_rn(keep, nn[1]));
-    v[2] = __fadd_rn(__fadd_rn(vc[2], t2), __fmul_rn(keep, nn[2]));
-}
-
 // One thread per z-row of 4 nodes of an active 4^3 block: the row's scene,
 // parameters and node address are resolved once and its 4 nodes' loads are
 // independent.  Reads and clears the P2G accumulators, writes grid velocity
@@ -178,26 +154,14 @@ __global__ void __launch_bounds__(256) k_grid(const SC sc, const WS w) {
                 v[0] *= damp; v[1] *= damp; v[2] *= damp;
             }
             if (!active) v[0] = v[1] = v[2] = 0.0f;
+            if (w.g_vpre && ncol > 0) w.g_vpre[node] = make_float4(v[0], v[1], v[2], 0.0f);   // for the adjoint
             if (active && ncol > 0) {
                 const float pos[3] = {(float)ix * dx, (float)iy * dx, (float)(iz0 + k) * dx};
                 for (int c = 0; c < ncol; ++c) {
                     const pm_collider col = prm.colliders[c];
-                    const float *o = ctrl->col_origin[c];
-                    const float *vc = ctrl->col_vel[c];
-                    if (col.kind == 0) {   // halfspace_collider (847-867)
-                        const float nn[3] = {(float)col.normal[0], (float)col.normal[1], (float)col.normal[2]};
-                        const float sd = dot3_rn(__fsub_rn(pos[0], o[0]), nn[0], __fsub_rn(pos[1], o[1]), nn[1],
-                                                 __fsub_rn(pos[2], o[2]), nn[2]);
-                        if (sd < 0.0f) resolve(v, vc, nn, col.mode == 1, (float)col.friction);
-                    } else {               // sphere_collider (828-844)
-                        const float r0 = pos[0] - o[0], r1 = pos[1] - o[1], r2 = pos[2] - o[2];
-                        const float dist = sqrtf(dot3_rn(r0, r0, r1, r1, r2, r2));
-                        if (dist < (float)col.radius) {
-                            const float den = dist + 1e-9f;
-                            const float nn[3] = {r0 / den, r1 / den, r2 / den};
-                            resolve(v, vc, nn, col.mode == 1, (float)col.friction);
-                        }
-                    }
+                    float nn[3];
+                    if (collider_hit(col, ctrl->col_origin[c], pos, nn))
+                        resolve(v, ctrl->col_vel[c], nn, col.mode == 1, (float)col.friction);
                 }
             }
             w.g_vel[node] = make_float4(v[0], v[1], v[2], mom[k].w);   // .w: node mass (read by the adjoint)
@@ -409,8 +373,10 @@ __device__ __forceinline__ void g2p_particle(const pm_params &prm, const Parts &
     P.lapo[p] = lap;
 }
 
-template <class SC>
-__global__ void __launch_bounds__(kG2PThreads, SC::batched ? 3 : 4) k_g2p(const SC scn, const Parts P, const WS w) {
+// MINB: resident CTAs per SM the registers are budgeted for (3: 80 registers;
+// 4: 64 registers with a few spills), a tunable.
+template <class SC, int MINB>
+__global__ void __launch_bounds__(kG2PThreads, MINB) k_g2p(const SC scn, const Parts P, const WS w) {
     __shared__ float4 sq[kGTQ];
     __shared__ float sc[kGTC];
     __shared__ int s_box[6];
@@ -487,13 +453,19 @@ __global__ void __launch_bounds__(kG2PThreads, SC::batched ? 3 : 4) k_g2p(const 
 // n_ctas: CTAs over all scenes (each scene's particles start a new CTA); the
 // plain form derives it from P.n.
 template <class SC>
-void launch_g2p(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, long long n_ctas) {
+void launch_g2p(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, long long n_ctas, int ctas_per_sm) {
     const long long blocks = n_ctas >= 0 ? n_ctas : (P.n + kG2PThreads - 1) / kG2PThreads;
     if (blocks <= 0) return;
-    k_g2p<SC><<<(unsigned)blocks, kG2PThreads, 0, s>>>(sc, P, w);
+    // 0: the default build (4 per SM for one scene; 3 for a batch, whose scene
+    // lookups need more registers)
+    const int minb = ctas_per_sm > 0 ? ctas_per_sm : (SC::batched ? 3 : 4);
+    if (minb >= 4)
+        k_g2p<SC, 4><<<(unsigned)blocks, kG2PThreads, 0, s>>>(sc, P, w);
+    else
+        k_g2p<SC, 3><<<(unsigned)blocks, kG2PThreads, 0, s>>>(sc, P, w);
 }
-template void launch_g2p<PlainScenes>(const PlainScenes &, const Parts &, const WS &, cudaStream_t, long long);
-template void launch_g2p<BatchScenes>(const BatchScenes &, const Parts &, const WS &, cudaStream_t, long long);
+template void launch_g2p<PlainScenes>(const PlainScenes &, const Parts &, const WS &, cudaStream_t, long long, int);
+template void launch_g2p<BatchScenes>(const BatchScenes &, const Parts &, const WS &, cudaStream_t, long long, int);
 
 // ---------------------------------------------------------------- sym_eig
 __global__ void __launch_bounds__(256) k_sym_eig(const float *__restrict__ A, long long n, int sweeps,

@@ -17,10 +17,12 @@ void prepare_sort();
 void prepare_adjoint();
 void launch_keys_only(const float *x, long long n, long long ps, int ng, float inv_dx, bool blocked, const WS &w,
                       cudaStream_t s);
-template <class SC> void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int ctas_per_sm = 0);
+template <class SC>
+void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int ctas_per_sm = 0, int stress_ctas = 0);
 template <class SC> void launch_grid(const SC &sc, const WS &w, cudaStream_t s, int ctas_per_sm = 0);
 void launch_grid_sums(const WS &w, long long n_nodes, float *mom, float *dmg, cudaStream_t s);
-template <class SC> void launch_g2p(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, long long n_ctas = -1);
+template <class SC>
+void launch_g2p(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, long long n_ctas = -1, int ctas_per_sm = 0);
 void launch_set_clock(const pm_params &prm, const WS &w, const pm_clock &clk, cudaStream_t s);
 void launch_set_clock_dev(const pm_params &prm, const WS &w, const pm_clock *dev, int row, cudaStream_t s);
 void launch_set_clock_batch(const BatchScenes &sc, const WS &w, const pm_clock *dev, cudaStream_t s);
@@ -36,12 +38,12 @@ void launch_sym_eig(const float *A, long long n, int sweeps, float *ev, float *V
 // work list), the particles' APIC affine term and their polar decomposition
 // (R, V, S) and damage drive phi.
 struct TapeLayout {
-    size_t head, actl, acc, adj_q, adj_c, apay, slot0, vel, gd, sw, blocks, keys, iperm, work, aff, pol, slot_bytes,
-        total;
+    size_t head, actl, acc, adj_q, adj_c, apay, slot0, vel, gd, sw, vpre, blocks, keys, iperm, work, aff, pol,
+        slot_bytes, total;
     long long n_blocks, aff_stride;
-    int slots;
+    int slots, flags;
 };
-TapeLayout make_tape_layout(long long n, int ng, int slots);
+TapeLayout make_tape_layout(long long n, int ng, int slots, int flags);
 void record_redirect(const TapeLayout &T, void *tape, int slot, WS &w);
 void launch_tape_head(const TapeLayout &T, void *tape, int slot, const WS &w, long long n, cudaStream_t s);
 void launch_adjoint(const pm_params &prm, const Parts &pre, const Parts &post, const pm_state_adj &ain,

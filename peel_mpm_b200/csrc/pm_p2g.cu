@@ -105,19 +105,7 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
         for (int k = 0; k < 3; ++k) rec[(18 + k) * rs + p] = S[k];
     }
     if (prm.use_f_clamp) {                                           // (622-636)
-        const float lo = (float)prm.f_clamp_lo, hi = (float)prm.f_clamp_hi;
-        float D[9], corr[9];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            float sc = S[i] < lo ? lo : S[i];
-            sc = sc > hi ? hi : sc;
-            const float ratio = sc / clamp_min(S[i], 1e-12f);
-#pragma unroll
-            for (int r = 0; r < 3; ++r) D[3 * r + i] = V[3 * r + i] * ratio;
-            S[i] = sc;
-        }
-        mmt3_rn(D, V, corr);                                         // V diag(Sc/S) V^T
-        mm3_rn(F, corr, F);
+        f_clamp_F(F, V, S, (float)prm.f_clamp_lo, (float)prm.f_clamp_hi, F);
 #pragma unroll
         for (int k = 0; k < 9; ++k) P.Fo[k * ps + p] = F[k];
     }
@@ -263,8 +251,10 @@ __device__ __forceinline__ void constitutive(const pm_params &prm, const Parts &
 //   {fx | x, m} {m v, d} {affine 0..3} {affine 4..7} {affine 8, regular, 0, 0}
 // with fx = X - floor(X - 0.5) per axis for particles whose stencil needs no
 // clamping (regular, base cell in [1, n_grid-4]) and the position x otherwise.
-template <class SC>
-__global__ void __launch_bounds__(256, 3) k_stress(const SC sc, const Parts P, const WS w) {
+// MINB: resident CTAs per SM the registers are budgeted for (3: 80 registers;
+// 4: 64 registers with a few spills), a tunable.
+template <class SC, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_stress(const SC sc, const Parts P, const WS w) {
     // particle order: the state reads and writes are coalesced; the payload
     // goes to the particle's sorted position
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -855,12 +845,15 @@ void prepare_p2g() {
 // kernel with as many CTAs as fit (3 per SM); 4 = the 64-register kernel at 4
 // per SM; 1..3 = the 80-register kernel capped at that many per SM.
 template <class SC>
-void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int ctas_per_sm) {
+void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int ctas_per_sm, int stress_ctas) {
     if (P.n <= 0) return;
     prepare_p2g();
     const int lb = (int)std::min<long long>((P.n + 255) / 256, 148LL * 8);
     k_subblocks<<<lb, 256, 0, s>>>(w.sorted_keys, P.n, w.work, w.ctrl);
-    k_stress<SC><<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(sc, P, w);
+    if (stress_ctas == 4)
+        k_stress<SC, 4><<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(sc, P, w);
+    else
+        k_stress<SC, 3><<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(sc, P, w);
     k_bounds<<<sc.count(), kBoundSlots, 0, s>>>(w.ctrl);
     static int slots_dev[64][2] = {{0}};
     int dev = 0;
@@ -883,7 +876,7 @@ void launch_p2g(const SC &sc, const Parts &P, const WS &w, cudaStream_t s, int c
     else
         k_p2g_tiles<SC, 3><<<blocks, kP2GThreads, kP2GSmem, s>>>(sc, w, P.n);
 }
-template void launch_p2g<PlainScenes>(const PlainScenes &, const Parts &, const WS &, cudaStream_t, int);
-template void launch_p2g<BatchScenes>(const BatchScenes &, const Parts &, const WS &, cudaStream_t, int);
+template void launch_p2g<PlainScenes>(const PlainScenes &, const Parts &, const WS &, cudaStream_t, int, int);
+template void launch_p2g<BatchScenes>(const BatchScenes &, const Parts &, const WS &, cudaStream_t, int, int);
 
 }  // namespace pm

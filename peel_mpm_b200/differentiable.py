@@ -19,9 +19,12 @@ gradients with respect to Young's modulus and fiber directions follow by
 composition.  The reference obtains the same gradients by PyTorch autograd
 through its substep (anisompm.py:593-803).
 
-Not differentiable here (the C ABI rejects them): f_clamp, colliders and
-interface particles.  Grips, damping, gravity and damage_every are supported;
-gripped particles have zero velocity adjoint (their velocity is prescribed).
+Everything the substep does is differentiated: grips (gripped particles
+have zero velocity adjoint, their velocity is prescribed), gravity, grid
+damping, damage_every, the strain limit f_clamp (through the singular values
+it limits), grid colliders (each collider's resolve rule, walked back from the
+recorded pre-collider grid velocity) and the directional stress at interface
+particles.
 """
 from __future__ import annotations
 
@@ -71,6 +74,10 @@ def _particles_at(sim: AnisoMPM, P, state: torch.Tensor):
     return Q
 
 
+def _tape_flags(sim: AnisoMPM) -> int:
+    return _lib.PM_TAPE_COLLIDERS if sim.colliders else 0
+
+
 class _Recorder:
     """Tape and per-substep states of one checkpoint segment."""
 
@@ -84,11 +91,12 @@ class _Recorder:
         self.prm = sim._build_params(grips)
         sim._ensure_ws()
         P = sim._particles()
-        self.tape_bytes = _lib.tape_size(n, sim.n_grid, slots)
+        flags = _tape_flags(sim)
+        self.tape_bytes = _lib.tape_size(n, sim.n_grid, slots, flags)
         self.tape = torch.empty(self.tape_bytes, dtype=torch.uint8, device=dev)
         self.stream = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(lib.pm_tape_init(self.tape.data_ptr(), self.tape_bytes, n, sim.n_grid, slots, self.stream),
-                   "pm_tape_init")
+        _lib.check(lib.pm_tape_init(self.tape.data_ptr(), self.tape_bytes, n, sim.n_grid, slots, flags,
+                                    self.stream), "pm_tape_init")
         self.states = torch.empty((slots + 1, _MUTABLE, stride), device=dev, dtype=torch.float32)
         self.descr = [_particles_at(sim, P, self.states[j]) for j in range(slots + 1)]
 
@@ -114,8 +122,6 @@ class _Rollout(torch.autograd.Function):
             sim.sigma_c.copy_(sigma_c)
             sim.A0.copy_(A0)
             sim.v.copy_(v0)
-        if sim.colliders or sim.f_clamp is not None or sim._iface_used:
-            raise NotImplementedError("the adjoint does not support colliders, f_clamp or interface particles")
         step0 = sim._step
         checkpoints = []
         want_grad = any(ctx.needs_input_grad[:5])
@@ -181,7 +187,7 @@ class _Rollout(torch.autograd.Function):
 def segment_bytes(sim: AnisoMPM, k: int) -> int:
     """Device bytes of a k-substep recording segment: the tape (grid and
     particle records of every substep) and the k + 1 particle states."""
-    return _lib.tape_size(sim.n, sim.n_grid, k) + (k + 1) * _MUTABLE * sim._S.stride(0) * 4
+    return _lib.tape_size(sim.n, sim.n_grid, k, _tape_flags(sim)) + (k + 1) * _MUTABLE * sim._S.stride(0) * 4
 
 
 def auto_segment(sim: AnisoMPM, n_steps: int, memory_fraction: float = 0.5) -> int:
@@ -245,16 +251,15 @@ def substep_vjp(sim: AnisoMPM, time: float, bars: dict):
     grips, calls = sim._descriptors()
     if calls:
         raise NotImplementedError("the adjoint needs grip_bc descriptors, not callables")
-    if sim.colliders or sim.f_clamp is not None or sim._iface_used:
-        raise NotImplementedError("the adjoint does not support colliders, f_clamp or interface particles")
     sim._grip_tags(grips)
     prm = sim._build_params(grips)
     sim._ensure_ws()
     P = sim._particles()
     st = torch.cuda.current_stream(dev).cuda_stream
-    tape_bytes = _lib.tape_size(n, sim.n_grid, 1)
+    flags = _tape_flags(sim)
+    tape_bytes = _lib.tape_size(n, sim.n_grid, 1, flags)
     tape = torch.empty(tape_bytes, dtype=torch.uint8, device=dev)
-    _lib.check(lib.pm_tape_init(tape.data_ptr(), tape_bytes, n, sim.n_grid, 1, st), "pm_tape_init")
+    _lib.check(lib.pm_tape_init(tape.data_ptr(), tape_bytes, n, sim.n_grid, 1, flags, st), "pm_tape_init")
     states = torch.empty((2, _MUTABLE, stride), device=dev, dtype=torch.float32)
     states[0].copy_(sim._S[:_MUTABLE])
     pre, post = _particles_at(sim, P, states[0]), _particles_at(sim, P, states[1])

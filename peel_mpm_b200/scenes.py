@@ -267,6 +267,38 @@ def knobs_drop(seed: int = 0) -> Scene:
         ])
 
 
+def colliders_drop(seed: int = 0) -> Scene:
+    """knobs_drop without f_clamp (grid damping, damage_every=2 and the three
+    colliders: slip half-space with friction, sticky and slip spheres), with
+    the half-space's origin at 9.43 dx instead of 9.4 dx.  knobs_drop's plane
+    passes exactly through the grid nodes (14, 8, z), which float32 and float64
+    then classify by rounding; here every node is at least 0.03 dx from it."""
+    sc = knobs_drop(seed)
+    dx = 1.0 / sc.n_grid
+    hs = sc.colliders[0]
+    sc.colliders[0] = ColliderSpec(hs.kind, (0.0, 9.43 * dx, 0.0), hs.velocity, normal=hs.normal, mode=hs.mode,
+                                   friction=hs.friction)
+    sc.name, sc.f_clamp = "colliders_drop", None
+    return sc
+
+
+def limit_drop(seed: int = 0) -> Scene:
+    """colliders_drop with knobs_drop's strain limit f_clamp = (0.6, 1.6),
+    which the first singular values reach after about 55 substeps."""
+    sc = colliders_drop(seed)
+    sc.name, sc.f_clamp = "limit_drop", (0.6, 1.6)
+    return sc
+
+
+def clamp_drop(seed: int = 0) -> Scene:
+    """colliders_drop with a tight strain limit, f_clamp = (0.9, 1.02): about
+    a hundred particles have a singular value beyond a bound at each substep
+    after the first ten."""
+    sc = colliders_drop(seed)
+    sc.name, sc.f_clamp = "clamp_drop", (0.9, 1.02)
+    return sc
+
+
 def interface_peel(seed: int = 0) -> Scene:
     """Two-layer slab whose interface band carries set_normal_isolation
     normals (directional delamination stress, anisompm.py:190-227, 697-703);

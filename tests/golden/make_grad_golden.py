@@ -110,16 +110,24 @@ def run(mod, sc, n_steps, E, fib, sig, v0):
 
 
 # one-substep cases: (scene, forward substeps before the differentiated one)
-ONESTEP = {"tiny_bar": (5, 25, 38)}
+ONESTEP = {"tiny_bar": (5, 25, 38), "colliders_drop": (20,), "limit_drop": (57,), "clamp_drop": (14,),
+           "interface_peel": (15,)}
+COMPACT = ("colliders_drop", "limit_drop", "clamp_drop", "interface_peel")
+ONESTEP_SCENES = {"tiny_bar": scenes.tiny_bar, "colliders_drop": scenes.colliders_drop,
+                  "limit_drop": scenes.limit_drop, "clamp_drop": scenes.clamp_drop,
+                  "interface_peel": scenes.interface_peel}
 STATE = ("x", "v", "F", "C", "d", "lap", "D_hist")
 PARAMS = ("mu", "lam", "sigma_c", "A0")
 
 
-def onestep(mod, name, factory, pre_steps, out, meta, tag):
+def onestep(mod, name, factory, pre_steps, out, meta, tag, compact=False):
     """Adjoint of one substep from a state with damage under way: random
     adjoints of the post-substep state, gradients of their inner product with
     the post state with respect to the pre state and the per-particle
-    parameters."""
+    parameters.  compact: the pre state is rounded to float32 before the
+    substep (the GPU path starts from float32 values) and the arrays are
+    saved in float32, without the adjoints, which the test draws again from
+    the same seed (numpy's default_rng(7), normal, in STATE order)."""
     sc = factory()
     dt = torch.float64
     sim = mod.AnisoMPM(n_grid=sc.n_grid, grid_lim=sc.grid_lim, dt=sc.dt, gravity=tuple(sc.gravity),
@@ -132,7 +140,9 @@ def onestep(mod, name, factory, pre_steps, out, meta, tag):
     leaves = {}
     for k in STATE + PARAMS:
         t = getattr(sim, k).detach().clone()
-        out[f"{tag}/pre_{k}"] = t.numpy()
+        if compact:
+            t = t.to(torch.float32).to(dt)
+        out[f"{tag}/pre_{k}"] = t.numpy().astype(np.float32) if compact else t.numpy()
         leaves[k] = t.requires_grad_(True)
         setattr(sim, k, leaves[k] * 1.0)
     step = sim._step
@@ -142,14 +152,17 @@ def onestep(mod, name, factory, pre_steps, out, meta, tag):
     for k in STATE:
         post = getattr(sim, k)
         w = torch.tensor(rng.normal(size=tuple(post.shape)), dtype=dt)
-        out[f"{tag}/bar_{k}"] = w.numpy()
-        out[f"{tag}/post_{k}"] = post.detach().numpy()
+        if not compact:
+            out[f"{tag}/bar_{k}"] = w.numpy()
+        out[f"{tag}/post_{k}"] = post.detach().numpy().astype(np.float32 if compact else np.float64)
         total = total + (w * post).sum()
     total.backward()
     for k in STATE + PARAMS:
         g = leaves[k].grad
-        out[f"{tag}/grad_{k}"] = (torch.zeros_like(leaves[k]) if g is None else g).numpy()
-    meta[tag] = {"pre_steps": pre_steps, "step": step, "time": pre_steps * sc.dt, "n": sc.n}
+        g = (torch.zeros_like(leaves[k]) if g is None else g).numpy()
+        out[f"{tag}/grad_{k}"] = g.astype(np.float32) if compact else g
+    meta[tag] = {"pre_steps": pre_steps, "step": step, "time": pre_steps * sc.dt, "n": sc.n,
+                 "bars": "seed 7" if compact else "saved"}
     print(tag, {k: float(np.linalg.norm(out[f"{tag}/grad_{k}"])) for k in STATE + PARAMS}, flush=True)
 
 
@@ -158,6 +171,8 @@ def main():
     ap.add_argument("--ref", default=os.environ.get("PEELMPM_REFERENCE_SRC"),
                     help="the reference's anisompm_py/src directory (default: $PEELMPM_REFERENCE_SRC)")
     ap.add_argument("--out", default=os.path.join(HERE, "reference_grads.npz"))
+    ap.add_argument("--only", nargs="*", default=None,
+                    help="compute only these one-substep cases and merge them into --out")
     args = ap.parse_args()
     if not args.ref:
         ap.error("give --ref or set PEELMPM_REFERENCE_SRC")
@@ -167,6 +182,8 @@ def main():
     torch.set_num_threads(os.cpu_count() or 1)
     out, meta = {}, {}
     for name, (factory, n_steps) in CASES.items():
+        if args.only:
+            break
         sc = factory()
         n = sc.n
         E0 = torch.tensor(sc.E, dtype=torch.float64)
@@ -190,8 +207,17 @@ def main():
                                                                    ("sigma_c", sig.grad), ("v0", v0.grad))}}
         print(name, meta[name], flush=True)
     for name, pres in ONESTEP.items():
+        if args.only and name not in args.only:
+            continue
         for pre in pres:
-            onestep(mod, name, CASES[name][0], pre, out, meta, f"one_{name}_{pre}")
+            onestep(mod, name, ONESTEP_SCENES[name], pre, out, meta, f"one_{name}_{pre}", compact=name in COMPACT)
+    if args.only and os.path.exists(args.out):   # merge into the existing file (cases computed now replace theirs)
+        old = np.load(args.out)
+        keep = [k for k in old.files if k.split("/")[0] not in {f"one_{n}_{p}" for n in args.only
+                                                                 for p in ONESTEP.get(n, ())}]
+        out = {**{k: old[k] for k in keep}, **out}
+        with open(args.out.replace(".npz", ".json")) as f:
+            meta = {**json.load(f), **meta}
     np.savez_compressed(args.out, **out)
     with open(args.out.replace(".npz", ".json"), "w") as f:
         json.dump(meta, f, indent=1)

@@ -32,7 +32,7 @@ def test_struct_layouts_match_binding():
 
 
 def test_abi_version():
-    assert _lib.load().pm_abi_version() == 1
+    assert _lib.load().pm_abi_version() == 2
 
 
 @pytest.mark.parametrize("n,ng", [(0, 4), (1, 8), (16384, 64), (1 << 20, 128), (8_847_360, 256), (1000, 96)])

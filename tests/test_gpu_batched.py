@@ -126,7 +126,12 @@ def test_autotuned_knobs_keep_results_bit_for_bit():
     b = BatchedAnisoMPM([make_gpu_sim(sc) for sc in scs])
     k = autotune.tune(a, substeps=2, reps=1, force=True)
     assert k["p2g_ctas_per_sm"] in autotune.P2G_CANDIDATES and k["grid_ctas_per_sm"] in autotune.GRID_CANDIDATES
-    assert (a.p2g_ctas_per_sm, a.grid_ctas_per_sm) == (k["p2g_ctas_per_sm"], k["grid_ctas_per_sm"])
+    assert k["stress_ctas_per_sm"] in autotune.STRESS_CANDIDATES and k["g2p_ctas_per_sm"] in autotune.G2P_CANDIDATES
+    for name in autotune.KNOBS:
+        assert getattr(a, name) == k[name], name
+        assert set(autotune._CACHE[autotune.bucket(a)]["ms"][name]) == set(autotune.__dict__[
+            {"p2g_ctas_per_sm": "P2G_CANDIDATES", "grid_ctas_per_sm": "GRID_CANDIDATES",
+             "stress_ctas_per_sm": "STRESS_CANDIDATES", "g2p_ctas_per_sm": "G2P_CANDIDATES"}[name]])
     assert autotune.bucket(a) in autotune._CACHE
     a.run_frame(5, 0.0)
     b.run_frame(5, 0.0)
@@ -136,11 +141,12 @@ def test_autotuned_knobs_keep_results_bit_for_bit():
             assert np.array_equal(v, gpu_state(sa)[f]), f
 
 
-@pytest.mark.parametrize("p2g,grid", [(1, 0), (2, 4), (0, 32)])
-def test_plain_launch_knobs_keep_results_bit_for_bit(p2g, grid):
+@pytest.mark.parametrize("p2g,grid,stress,g2p", [(1, 0, 4, 3), (2, 4, 3, 4), (0, 32, 4, 4)])
+def test_plain_launch_knobs_keep_results_bit_for_bit(p2g, grid, stress, g2p):
     sc = scenes.knobs_drop()
     a, b = make_gpu_sim(sc), make_gpu_sim(sc)
     a.p2g_ctas_per_sm, a.grid_ctas_per_sm = p2g, grid
+    a.stress_ctas_per_sm, a.g2p_ctas_per_sm = stress, g2p
     a.run_frame(6, 0.0)
     b.run_frame(6, 0.0)
     torch.cuda.synchronize()
