@@ -720,7 +720,9 @@ __device__ __forceinline__ void cw5_2(float fx, float e[5]) {
 // per particle, so a chunk of 256 particles keeps |hi| under 2^31).  Both
 // adds are fire-and-forget (no returned value, no carry chain) and
 // unconditional (a branch per add costs more than adding a zero); the pair
-// is folded into an int64 tile after every chunk, exactly.
+// is folded into an int64 tile, exactly, before either plane can overflow:
+// after every chunk in the adjoint scatter, after every fourth chunk in the
+// forward P2G (whose adds per particle are below 0.42 of 2^kFixBits).
 constexpr int kSplitBits = 24;
 __device__ __forceinline__ void plane_add(unsigned *lo, int *hi, float v, float scale) {
     const long long q = to_fix(v, scale);

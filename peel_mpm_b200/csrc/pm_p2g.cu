@@ -555,7 +555,8 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                             bz * kSortBlock + (int)(oct & 1u) * kSubEdge};   // first cell of the sub-block
 
         long long item_n = 0;                               // particles of the sub-block
-        for (long long sub = a;; sub += kSub) {
+        int chunk = 0;
+        for (long long sub = a;; sub += kSub, ++chunk) {
             // ---------------- the chunk's payload (written by k_stress in sorted
             // order) into shared memory: coalesced float4 loads
             const long long i = sub + tid;
@@ -736,58 +737,66 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
             }
             __syncthreads();
             const bool last = cnt < kSub;                       // uniform: the last chunk of the sub-block
-            // ---------------- fold the chunk planes into the int64 sums; after
-            // the last chunk, flush those with one atomic per nonzero node
-            // component.
-            for (int li = tid; li < kQN; li += kP2GThreads) {
-                const int tx = li / (kQE * kQE), ty = (li / kQE) % kQE, tz = li % kQE;
-                const int sidx = tx * kQSX + ty * kQSY + tz;
-                long long q[4];
+            // the planes take up to four chunks (1,024 particles) before they
+            // must be folded: one add per node is below 0.42 (the largest
+            // quadratic weight) of 2^46 units per particle, so the high plane
+            // stays under 1024 * 0.42 * 2^22 < 2^31; a node takes at most one
+            // add per covering cell and chunk, fewer than 2^7 adds of 24 bits
+            // into the unsigned low plane
+            if (last || (chunk & 3) == 3) {
+                // ---------------- fold the chunk planes into the int64 sums; after
+                // the last chunk, flush those with one atomic per nonzero node
+                // component.
+                for (int li = tid; li < kQN; li += kP2GThreads) {
+                    const int tx = li / (kQE * kQE), ty = (li / kQE) % kQE, tz = li % kQE;
+                    const int sidx = tx * kQSX + ty * kQSY + tz;
+                    long long q[4];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    const unsigned lo = qlo[c][sidx];
-                    const int hi = qhi[c][sidx];
-                    q[c] = qt[c * kQN + li];
-                    if ((lo | (unsigned)hi) != 0u) {
-                        qlo[c][sidx] = 0u;
-                        qhi[c][sidx] = 0;
-                        q[c] += plane_value(lo, hi);
+                    for (int c = 0; c < 4; ++c) {
+                        const unsigned lo = qlo[c][sidx];
+                        const int hi = qhi[c][sidx];
+                        q[c] = qt[c * kQN + li];
+                        if ((lo | (unsigned)hi) != 0u) {
+                            qlo[c][sidx] = 0u;
+                            qhi[c][sidx] = 0;
+                            q[c] += plane_value(lo, hi);
+                        }
+                    }
+                    // the running sums are kept between chunks and cleared after the
+                    // last one whatever their value (a partial that the last chunk
+                    // cancels exactly must not leak into the CTA's next sub-block)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) qt[c * kQN + li] = last ? 0 : q[c];
+                    if (last && (q[0] | q[1] | q[2] | q[3]) != 0) {
+                        long long *g = g_mom + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            if (q[c]) atomicAdd((unsigned long long *)(g + c), (unsigned long long)q[c]);
                     }
                 }
-                // the running sums are kept between chunks and cleared after the
-                // last one whatever their value (a partial that the last chunk
-                // cancels exactly must not leak into the CTA's next sub-block)
+                for (int li = tid; li < kCN; li += kP2GThreads) {
+                    const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
+                    const int sidx = tx * kCSX + ty * kCSY + tz;
+                    long long q[2];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) qt[c * kQN + li] = last ? 0 : q[c];
-                if (last && (q[0] | q[1] | q[2] | q[3]) != 0) {
-                    long long *g = g_mom + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
-#pragma unroll
-                    for (int c = 0; c < 4; ++c)
-                        if (q[c]) atomicAdd((unsigned long long *)(g + c), (unsigned long long)q[c]);
-                }
-            }
-            for (int li = tid; li < kCN; li += kP2GThreads) {
-                const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
-                const int sidx = tx * kCSX + ty * kCSY + tz;
-                long long q[2];
-#pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const unsigned lo = clo[c][sidx];
-                    const int hi = chi[c][sidx];
-                    q[c] = ct[c * kCN + li];
-                    if ((lo | (unsigned)hi) != 0u) {
-                        clo[c][sidx] = 0u;
-                        chi[c][sidx] = 0;
-                        q[c] += plane_value(lo, hi);
+                    for (int c = 0; c < 2; ++c) {
+                        const unsigned lo = clo[c][sidx];
+                        const int hi = chi[c][sidx];
+                        q[c] = ct[c * kCN + li];
+                        if ((lo | (unsigned)hi) != 0u) {
+                            clo[c][sidx] = 0u;
+                            chi[c][sidx] = 0;
+                            q[c] += plane_value(lo, hi);
+                        }
                     }
-                }
-                ct[li] = last ? 0 : q[0];
-                ct[kCN + li] = last ? 0 : q[1];
-                if (last && (q[0] | q[1]) != 0) {
-                    long long *g = g_dmg + 2 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
-                                                (org[2] - 1 + tz));
-                    if (q[0]) atomicAdd((unsigned long long *)g, (unsigned long long)q[0]);
-                    if (q[1]) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q[1]);
+                    ct[li] = last ? 0 : q[0];
+                    ct[kCN + li] = last ? 0 : q[1];
+                    if (last && (q[0] | q[1]) != 0) {
+                        long long *g = g_dmg + 2 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
+                                                    (org[2] - 1 + tz));
+                        if (q[0]) atomicAdd((unsigned long long *)g, (unsigned long long)q[0]);
+                        if (q[1]) atomicAdd((unsigned long long *)(g + 1), (unsigned long long)q[1]);
+                    }
                 }
             }
             if (last) break;
