@@ -75,16 +75,16 @@ BYTES_PER_PARTICLE = 216 + 73
 BYTES_PER_NODE = 80
 # Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) and
 # warp instructions (smsp__inst_executed.sum) of the substep's kernels on this
-# workload, from one ncu capture of `bench.py --form plain` (the command and
-# the figures are in profiles/p2g_g2p_1m_kernels.md); used for the roofline's
+# workload, from one ncu capture per kernel of `bench.py --form plain` (the
+# command and the figures sit with the profile summaries); used for the roofline's
 # `traffic` and its issue-bound floor (warp instructions / (4 schedulers x
 # SMs x SM clock)).
 NCU_KERNELS = {
     "k_subblocks": {"dram_bytes": 4203264, "warp_inst": 1975877},
-    "k_stress": {"dram_bytes": 195187200 + 62620928, "warp_inst": 39989452},
+    "k_stress": {"dram_bytes": 195174912 + 62206208, "warp_inst": 39083888},
     "k_bounds": {"dram_bytes": 4864, "warp_inst": 172},
-    "k_p2g_tiles": {"dram_bytes": 96168192 + 2324992, "warp_inst": 76360593},
-    "k_g2p": {"dram_bytes": 54701056 + 45764352, "warp_inst": 56582144},
+    "k_p2g_tiles": {"dram_bytes": 96181760 + 5001984, "warp_inst": 56973418},
+    "k_g2p": {"dram_bytes": 54698240 + 46928640, "warp_inst": 53436416},
 }
 P2G_KERNELS = ("k_subblocks", "k_stress", "k_bounds", "k_p2g_tiles")
 
