@@ -117,3 +117,19 @@ def test_batch_argument_errors_without_device():
                                        C.byref(out)) == _lib.PM_ERR_ARG
     assert lib.pm_batch_workspace_size(1, None, g1, C.byref(out)) == _lib.PM_ERR_ARG
     assert lib.pm_batch_workspace_size(1, n1, g1, C.byref(out)) == _lib.PM_OK and out.value > 0
+
+
+def test_tape_size_grows_by_the_pre_collider_grid_per_slot():
+    """With PM_TAPE_COLLIDERS every slot also keeps the grid velocity before
+    the colliders (16 bytes per node); unknown flag bits are rejected."""
+    lib = _lib.load()
+    src = open(os.path.join(ROOT, "include", "peelmpm.h")).read()
+    assert re.search(r"#define PM_TAPE_COLLIDERS 1\b", src) and _lib.PM_TAPE_COLLIDERS == 1
+    n, ng = 100_000, 64
+    for slots in (1, 3):
+        plain = _lib.tape_size(n, ng, slots, 0)
+        col = _lib.tape_size(n, ng, slots, _lib.PM_TAPE_COLLIDERS)
+        assert col - plain == slots * 16 * ng ** 3
+    out = C.c_size_t(0)
+    assert lib.pm_tape_size(n, ng, 1, 2, C.byref(out)) == _lib.PM_ERR_ARG
+
