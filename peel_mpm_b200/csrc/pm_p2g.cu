@@ -11,21 +11,22 @@
 //
 // k_p2g_tiles, persistent CTAs taking work items from a list of the
 // non-empty 4^3-cell sub-blocks of the sort (the cells of a sub-block are a
-// contiguous run of the Morton-ordered sort).  A work item owns two
-// shared-memory tiles: the quadratic momentum tile (nodes [4s, 4s+6)^3,
-// {mv, m}) and the cubic damage tile (nodes [4s-1, 4s+7)^3, {sum w d,
-// sum w}).  Chunks of 256 particles stage their payload in shared memory,
-// then one work item per (cell, x-slab): all particles of a cell share their
-// quadratic base, so an item sums the cell's contributions to 9 quadratic
-// nodes (3 slabs) or 25 cubic nodes (5 slabs; a cell's cubic stencils span
-// 5^3 nodes) in float registers (packed pairs: sm_100's FFMA2 issues two
-// FMAs per instruction), in the sorted order, and adds each node once.  Tiles and the global grid accumulate int64 fixed point (units from
-// the control block's bounds): integer addition is associative, so the grid
-// sums, and with them the whole substep, are the same bits whatever order the
-// atomics run in.  The tiles are flushed with one atomic per touched node and
-// component, marking the touched 4^3 grid blocks.  Particles whose stencil
-// needs the reference's edge clamping (base cell outside [1, n_grid-4])
-// scatter directly to the global grid instead.
+// contiguous run of the Morton-ordered sort).  A work item covers the
+// quadratic nodes [4s, 4s+6)^3 ({mv, m}) and the cubic nodes [4s-1, 4s+7)^3
+// ({sum w d, sum w}).  Chunks of 256 particles stage their payload in shared
+// memory, then one work item per (cell, x-slab): all particles of a cell
+// share their quadratic base, so an item sums the cell's contributions to 9
+// quadratic nodes (3 slabs) or 25 cubic nodes (5 slabs; a cell's cubic
+// stencils span 5^3 nodes) in float registers (packed pairs: sm_100's FFMA2
+// issues two FMAs per instruction), in the sorted order, and adds each node
+// once as exact fixed point (units from the control block's bounds) into two
+// 32-bit shared planes per component.  Every fourth chunk and after the last
+// one the planes go to the global int64 grid, one atomic per nonzero node
+// and component; integer addition is associative, so the grid sums, and with
+// them the whole substep, are the same bits whatever order the atomics run
+// in.  The touched 4^3 grid blocks are marked.  Particles whose stencil needs
+// the reference's edge clamping (base cell outside [1, n_grid-4]) scatter
+// directly to the global grid instead.
 //
 // Reference: anisompm.py:601-724 (constitutive, damage, P2G) and 768-776
 // (cubic damage scatter).
@@ -450,8 +451,7 @@ constexpr int kCW = 15;                        // expanded cubic weights per par
 // without bank conflicts.
 constexpr int kQSY = 8, kQSX = 52, kQPl = 312;   // 5*52 + 5*8 + 6 = 306 <= 312
 constexpr int kCSY = 8, kCSX = 68, kCPl = 544;   // 7*68 + 7*8 + 8 = 540 <= 544
-constexpr size_t kP2GSmem = sizeof(long long) * (4 * kQN + 2 * kCN) +
-                            sizeof(unsigned) * 2 * (4 * kQPl + 2 * kCPl) +
+constexpr size_t kP2GSmem = sizeof(unsigned) * 2 * (4 * kQPl + 2 * kCPl) +
                             sizeof(float) * (kPay + kCW) * kPayStride + sizeof(int) * (kSub + 2) + 2 * kSub;
 
 // Folds control block blockIdx.x's bound slots into its three bounds and
@@ -500,9 +500,7 @@ __global__ void __launch_bounds__(256) k_subblocks(const unsigned *__restrict__ 
 template <class SC, int MINB>
 __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, const WS w, long long n) {
     extern __shared__ long long s_raw[];
-    long long *qt = s_raw;                                                // [4][kQN] int64 sub-block sums
-    long long *ct = qt + 4 * kQN;                                         // [2][kCN]
-    unsigned (*qlo)[kQPl] = (unsigned (*)[kQPl])(ct + 2 * kCN);          // [4][kQPl] chunk planes
+    unsigned (*qlo)[kQPl] = (unsigned (*)[kQPl])(s_raw);                 // [4][kQPl] chunk planes
     int (*qhi)[kQPl] = (int (*)[kQPl])(qlo[4]);                         // [4][kQPl]
     unsigned (*clo)[kCPl] = (unsigned (*)[kCPl])(qhi[4]);                // [2][kCPl]
     int (*chi)[kCPl] = (int (*)[kCPl])(clo[2]);                         // [2][kCPl]
@@ -520,8 +518,7 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
     Ctrl *ctrl0 = w.ctrl;
     const unsigned n_work = min(ctrl0->n_work, (unsigned)min(n, (long long)0x7fffffff));
 
-    // tiles and planes start zero; every fold and flush clears what it visits
-    for (int i = tid; i < 4 * kQN + 2 * kCN; i += kP2GThreads) qt[i] = 0;
+    // the planes start zero; every fold clears what it visits
     for (int i = tid; i < 2 * (4 * kQPl + 2 * kCPl); i += kP2GThreads) qlo[0][i] = 0u;
     if (tid < 27) s_bmark[tid] = 0;
     for (;;) {
@@ -744,9 +741,10 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
             // add per covering cell and chunk, fewer than 2^7 adds of 24 bits
             // into the unsigned low plane
             if (last || (chunk & 3) == 3) {
-                // ---------------- fold the chunk planes into the int64 sums; after
-                // the last chunk, flush those with one atomic per nonzero node
-                // component.
+                // ---------------- fold the chunk planes straight into the global
+                // grid, one int64 atomic per nonzero node component, clearing
+                // them.  Integer addition is associative, so a sub-block of more
+                // than four chunks, folded more than once, adds the same total.
                 for (int li = tid; li < kQN; li += kP2GThreads) {
                     const int tx = li / (kQE * kQE), ty = (li / kQE) % kQE, tz = li % kQE;
                     const int sidx = tx * kQSX + ty * kQSY + tz;
@@ -755,19 +753,14 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                     for (int c = 0; c < 4; ++c) {
                         const unsigned lo = qlo[c][sidx];
                         const int hi = qhi[c][sidx];
-                        q[c] = qt[c * kQN + li];
+                        q[c] = 0;
                         if ((lo | (unsigned)hi) != 0u) {
                             qlo[c][sidx] = 0u;
                             qhi[c][sidx] = 0;
-                            q[c] += plane_value(lo, hi);
+                            q[c] = plane_value(lo, hi);
                         }
                     }
-                    // the running sums are kept between chunks and cleared after the
-                    // last one whatever their value (a partial that the last chunk
-                    // cancels exactly must not leak into the CTA's next sub-block)
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) qt[c * kQN + li] = last ? 0 : q[c];
-                    if (last && (q[0] | q[1] | q[2] | q[3]) != 0) {
+                    if ((q[0] | q[1] | q[2] | q[3]) != 0) {
                         long long *g = g_mom + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
 #pragma unroll
                         for (int c = 0; c < 4; ++c)
@@ -782,16 +775,14 @@ __global__ void __launch_bounds__(kP2GThreads, MINB) k_p2g_tiles(const SC sc, co
                     for (int c = 0; c < 2; ++c) {
                         const unsigned lo = clo[c][sidx];
                         const int hi = chi[c][sidx];
-                        q[c] = ct[c * kCN + li];
+                        q[c] = 0;
                         if ((lo | (unsigned)hi) != 0u) {
                             clo[c][sidx] = 0u;
                             chi[c][sidx] = 0;
-                            q[c] += plane_value(lo, hi);
+                            q[c] = plane_value(lo, hi);
                         }
                     }
-                    ct[li] = last ? 0 : q[0];
-                    ct[kCN + li] = last ? 0 : q[1];
-                    if (last && (q[0] | q[1]) != 0) {
+                    if ((q[0] | q[1]) != 0) {
                         long long *g = g_dmg + 2 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
                                                     (org[2] - 1 + tz));
                         if (q[0]) atomicAdd((unsigned long long *)g, (unsigned long long)q[0]);
