@@ -322,7 +322,7 @@ constexpr int kAPayStride = kATh + kATh / 32;
 constexpr int kASub = 4, kAQE = 6, kACE = 8, kAQN = 216, kACN = 512;
 // chunk planes with the forward P2G's conflict-free strides (z 1, y 8, x 52 / 68)
 constexpr int kAQSY = 8, kAQSX = 52, kAQPl = 312, kACSY = 8, kACSX = 68, kACPl = 544;
-constexpr size_t kAdjTileSmem = sizeof(long long) * (3 * kAQN + kACN) + sizeof(unsigned) * 2 * (3 * kAQPl + kACPl) +
+constexpr size_t kAdjTileSmem = sizeof(unsigned) * 2 * (3 * kAQPl + kACPl) +
                                 sizeof(float) * (17 + kAdjCW) * kAPayStride + sizeof(int) * (kATh + 2) + 2 * kATh;
 
 __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, const unsigned *__restrict__ keys,
@@ -330,9 +330,7 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
                                                        const float4 *__restrict__ pay, AdjCtrl *actl,
                                                        long long *__restrict__ acc, long long n) {
     extern __shared__ long long s_adj[];
-    long long *qt = s_adj;                                                 // [3][kAQN]
-    long long *ct = qt + 3 * kAQN;                                         // [kACN]
-    unsigned (*qlo)[kAQPl] = (unsigned (*)[kAQPl])(ct + kACN);            // [3][kAQPl] chunk planes
+    unsigned (*qlo)[kAQPl] = (unsigned (*)[kAQPl])(s_adj);                // [3][kAQPl] chunk planes
     int (*qhi)[kAQPl] = (int (*)[kAQPl])(qlo[3]);                         // [3][kAQPl]
     unsigned *clo = (unsigned *)(qhi[3]);                                 // [kACPl]
     int *chi = (int *)(clo + kACPl);                                      // [kACPl]
@@ -349,7 +347,6 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
     const int nb = sort_blocks_per_axis(ng);
     const float inv_dx = (float)prm.inv_dx, dx = (float)prm.dx;
     const float smom = fix_scale(actl->mom_bound).scale, slap = fix_scale(actl->lap_bound).scale;
-    for (int i = tid; i < 3 * kAQN + kACN; i += kATh) qt[i] = 0;
     for (int i = tid; i < 2 * (3 * kAQPl + kACPl); i += kATh) qlo[0][i] = 0u;
     for (;;) {
         __syncthreads();
@@ -366,6 +363,7 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
         const int org[3] = {bx * kSortBlock + (int)((oct >> 2) & 1u) * kASub,
                             by * kSortBlock + (int)((oct >> 1) & 1u) * kASub,
                             bz * kSortBlock + (int)(oct & 1u) * kASub};
+        int pending = 0;   // chunks with particles since the planes were last folded
         for (long long sub = a;; sub += kATh) {
             const long long i = sub + tid;
             const unsigned key = i < n ? keys[i] : 0xffffffffu;
@@ -545,50 +543,52 @@ __global__ void __launch_bounds__(kATh, 3) k_adj_tiles(const pm_params prm, cons
             }
             __syncthreads();
             const bool last = cnt < kATh;
-            // fold the chunk planes into the int64 sums; flush after the last chunk
-            for (int li = tid; li < kAQN; li += kATh) {
-                const int tx = li / (kAQE * kAQE), ty = (li / kAQE) % kAQE, tz = li % kAQE;
-                const int sidx = tx * kAQSX + ty * kAQSY + tz;
-                long long q[3];
+            pending += cnt > 0 ? 1 : 0;
+            // fold the chunk planes straight into the global grid, one int64
+            // atomic per nonzero node component, after every second chunk with
+            // particles and after the last: one add per particle and node is
+            // below 0.89 of 2^46 units (|w''x wy wz + wx w''y wz + wx wy w''z|
+            // <= 2.67 against the bound's 3), so two chunks keep the high
+            // plane under 512 * 0.89 * 2^22 < 2^31
+            if (pending > 0 && (last || pending == 2)) {
+                pending = 0;
+                for (int li = tid; li < kAQN; li += kATh) {
+                    const int tx = li / (kAQE * kAQE), ty = (li / kAQE) % kAQE, tz = li % kAQE;
+                    const int sidx = tx * kAQSX + ty * kAQSY + tz;
+                    long long q[3];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const unsigned lo = qlo[c][sidx];
-                    const int hi = qhi[c][sidx];
-                    q[c] = qt[c * kAQN + li];
-                    if ((lo | (unsigned)hi) != 0u) {
-                        qlo[c][sidx] = 0u;
-                        qhi[c][sidx] = 0;
-                        q[c] += plane_value(lo, hi);
+                    for (int c = 0; c < 3; ++c) {
+                        const unsigned lo = qlo[c][sidx];
+                        const int hi = qhi[c][sidx];
+                        q[c] = 0;
+                        if ((lo | (unsigned)hi) != 0u) {
+                            qlo[c][sidx] = 0u;
+                            qhi[c][sidx] = 0;
+                            q[c] = plane_value(lo, hi);
+                        }
+                    }
+                    if ((q[0] | q[1] | q[2]) != 0) {
+                        long long *g = acc + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            if (q[c]) atomicAdd((unsigned long long *)(g + c), (unsigned long long)q[c]);
                     }
                 }
-                // cleared after the last chunk whatever the value (a partial that
-                // the last chunk cancels exactly must not leak into the CTA's
-                // next sub-block)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) qt[c * kAQN + li] = last ? 0 : q[c];
-                if (last && (q[0] | q[1] | q[2]) != 0) {
-                    long long *g = acc + 4 * (((long long)(org[0] + tx) * ng + (org[1] + ty)) * ng + (org[2] + tz));
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-                        if (q[c]) atomicAdd((unsigned long long *)(g + c), (unsigned long long)q[c]);
-                }
-            }
-            for (int li = tid; li < kACN; li += kATh) {
-                const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
-                const int sidx = tx * kACSX + ty * kACSY + tz;
-                const unsigned lo = clo[sidx];
-                const int hi = chi[sidx];
-                long long q3 = ct[li];
-                if ((lo | (unsigned)hi) != 0u) {
-                    clo[sidx] = 0u;
-                    chi[sidx] = 0;
-                    q3 += plane_value(lo, hi);
-                }
-                ct[li] = last ? 0 : q3;
-                if (last && q3 != 0) {
-                    long long *g = acc + 4 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
-                                              (org[2] - 1 + tz));
-                    atomicAdd((unsigned long long *)(g + 3), (unsigned long long)q3);
+                for (int li = tid; li < kACN; li += kATh) {
+                    const int tx = li >> 6, ty = (li >> 3) & 7, tz = li & 7;
+                    const int sidx = tx * kACSX + ty * kACSY + tz;
+                    const unsigned lo = clo[sidx];
+                    const int hi = chi[sidx];
+                    if ((lo | (unsigned)hi) != 0u) {
+                        clo[sidx] = 0u;
+                        chi[sidx] = 0;
+                        const long long q3 = plane_value(lo, hi);
+                        if (q3 != 0) {
+                            long long *g = acc + 4 * (((long long)(org[0] - 1 + tx) * ng + (org[1] - 1 + ty)) * ng +
+                                                      (org[2] - 1 + tz));
+                            atomicAdd((unsigned long long *)(g + 3), (unsigned long long)q3);
+                        }
+                    }
                 }
             }
             if (last) break;
